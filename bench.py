@@ -1,0 +1,493 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 fastibs window scan (reference k-mer probes/s).
+
+Workload (default plain_2gbp): a seeded 2 Gbp reference in 10 contigs of
+100-400 Mbp with 0.5% N runs, scanned in 50 kbp windows against one sample of
+~2.2e9 canonical k=25 k-mers (block-divergence copy of the reference plus 10%
+random k-mers). Synthetic data stands in for the reference project's
+plant-genome inputs, which are not available here.
+
+A step is one scan of the whole reference: every window's row. `value` is
+probes/s with the table and the packed reference resident in HBM (CUDA events
+on the launching stream, max over ranks); `e2e` is the same metric through the
+host-buffer C-ABI call ibs_scan_packed (pinned host reference in, rows out,
+copies inside the timed region). With N GPUs every rank scans its own sample
+(weak scaling, no collective on the data path).
+
+--impl reference times the reference's own CPU implementation (CPU-BATCHED:
+`fastibs --cpu --probe=batched` built from its sources into oracle/_ref/) on
+bounded slices of the same workload, on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "gpu-ibs_b200" / "python"))
+
+BYTES_PER_PROBE = 32.0 + 0.375  # one 32-byte bucket sector + 2-bit base + N-mask bit
+METRIC = "ref k-mer probes/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# workload helpers
+# ---------------------------------------------------------------------------
+def valid_positions(lens, k, runs, lo=None, hi=None) -> int:
+    """k-mer start positions whose k bases are ACGT, per contig from its N
+    runs; optionally only positions in [lo, hi) of contig 0 (a slice)."""
+    rc, rs, rl = runs
+    total = 0
+    for c, L in enumerate(lens):
+        L = int(L)
+        a, b = (0, L) if lo is None or c != 0 else (lo, min(hi, L))
+        if lo is not None and c != 0:
+            continue
+        npos = max(0, (b - a) - k + 1)
+        if npos == 0:
+            continue
+        last = a + npos - 1  # last valid start in the slice
+        iv = []
+        sel = rc == c
+        for s, ln in zip(rs[sel].tolist(), rl[sel].tolist()):
+            x, y = max(a, s - k + 1), min(last, s + ln - 1)
+            if x <= y:
+                iv.append((x, y))
+        iv.sort()
+        bad, cur = 0, None
+        for x, y in iv:
+            if cur is None or x > cur[1] + 1:
+                if cur:
+                    bad += cur[1] - cur[0] + 1
+                cur = [x, y]
+            else:
+                cur[1] = max(cur[1], y)
+        if cur:
+            bad += cur[1] - cur[0] + 1
+        total += npos - bad
+    return total
+
+
+def sample_for_rank(w, rank: int):
+    from ibs_b200 import SampleSpec
+    s = w.samples[0]
+    if rank == 0:
+        return s
+    c = s.c
+    return SampleSpec(seed=int(c.seed) + 7919 * rank, k=int(c.k),
+                      class_rate=tuple(c.class_rate)[: c.n_classes],
+                      class_prob=tuple(c.class_prob)[: c.n_classes], block_len=int(c.block_len),
+                      present_frac=float(c.present_frac), random_frac=float(c.random_frac))
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "of measured"
+    return 6650.0, "of fallback"
+
+
+def profiled_traffic(workload: str):
+    """DRAM bytes per scan-kernel launch from the committed ncu summary, if any."""
+    p = REPO / "profiles" / f"scan_spans_{workload}.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("dram_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's own binary on bounded slices
+# ---------------------------------------------------------------------------
+def cache_dir(w) -> Path:
+    root = Path("/dev/shm") if Path("/dev/shm").is_dir() else Path(tempfile.gettempdir())
+    return root / f"ibs_bench_{w.name}"
+
+
+def write_kmc_db(w, dcodes_ptr: int, n: int, d: Path) -> Path:
+    import ibs_b200 as ib
+    prefix = d / "db" / "sample"
+    stamp = d / "db" / "complete"
+    if stamp.exists():
+        return prefix
+    (d / "db").mkdir(parents=True, exist_ok=True)
+    t = time.time()
+    written = ib.kmc_write(str(prefix), dcodes_ptr, n, on_device=True, **w.kmc)
+    stamp.write_text(str(written))
+    log(f"[bench] KMC database of {written} k-mers written in {time.time() - t:.1f} s")
+    return prefix
+
+
+def write_slices(w, d: Path, starts, length: int) -> list[Path]:
+    """FASTA files of slices [s, s+length) of contig 0."""
+    ascii0 = w.ref.contig_ascii(0)
+    out = []
+    for i, s in enumerate(starts):
+        p = d / f"refs_{i}"
+        p.mkdir(parents=True, exist_ok=True)
+        f = p / f"slice{i}_genome.fasta"
+        if not f.exists():
+            seq = ascii0[s:s + length]
+            with open(f, "wb") as fh:
+                fh.write(b">" + w.ref.names[0].encode() + b"\n")
+                for j in range(0, len(seq), 80):
+                    fh.write(seq[j:j + 80] + b"\n")
+        out.append(p)
+    return out
+
+
+def run_reference_scans(dbdir: Path, refdirs: list[Path], W: int, workdir: Path):
+    """Runs the reference CLI once over a folder holding every slice; returns
+    per-slice 'stats' seconds in slice order."""
+    binp = REPO / "oracle" / "_ref" / "fastibs"
+    allrefs = workdir / "allrefs"
+    shutil.rmtree(allrefs, ignore_errors=True)
+    allrefs.mkdir(parents=True)
+    for rd in refdirs:
+        for f in rd.iterdir():
+            os.symlink(f, allrefs / f.name)
+    out = workdir / "out"
+    shutil.rmtree(out, ignore_errors=True)
+    env = dict(os.environ, FASTIBS_THREADS=str(os.cpu_count()), FASTIBS_CPU_BATCH="16")
+    r = subprocess.run([str(binp), str(dbdir), str(allrefs), str(out), str(W), "--cpu", "--probe=batched"],
+                       env=env, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference fastibs failed: {r.stderr[-1500:]}")
+    stats = {}
+    cur = None
+    for line in r.stdout.splitlines():
+        m = re.match(r"Processing reference: (slice\d+)", line)
+        if m:
+            cur = m.group(1)
+        m = re.search(r"Scan phases: setup ([\d.e-]+) s, read ([\d.e-]+) s, window ([\d.e-]+) s, "
+                      r"stats ([\d.e-]+) s", line)
+        if m and cur:
+            stats[cur] = float(m.group(4))
+    return [stats[f"slice{i}"] for i in range(len(refdirs))], r.stdout
+
+
+def cpu_arm(w, runs, steps: int, warmup: int, slice_len: int, dcodes_ptr=None, n_codes=0):
+    """Times the reference CPU-BATCHED scan on steps+warmup slices."""
+    d = cache_dir(w)
+    d.mkdir(parents=True, exist_ok=True)
+    prefix = d / "db" / "sample"
+    if not (d / "db" / "complete").exists():
+        if dcodes_ptr is None:
+            raise RuntimeError("no sample codes to write the KMC database from")
+        write_kmc_db(w, dcodes_ptr, n_codes, d)
+    n = steps + warmup
+    L0 = int(w.ref.lens[0])
+    starts = [(i * slice_len) % max(1, L0 - slice_len) for i in range(n)]
+    refdirs = write_slices(w, d, starts, slice_len)
+    secs, _ = run_reference_scans(prefix.parent, refdirs, w.window, d / "run")
+    probes = [valid_positions(w.ref.lens, w.k, runs, s, s + slice_len) for s in starts]
+    timed = list(range(warmup, n))
+    value = sum(probes[i] for i in timed) / sum(secs[i] for i in timed)
+    return value, secs, probes
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def gpu_arm(args, w, rank: int, world: int, local: int):
+    import torch
+    import ibs_b200 as ib
+
+    torch.cuda.set_device(local)
+    dev = local
+    k, W = w.k, w.window
+    lens = w.ref.lens
+    runs = w.ref.n_runs()
+    probes_per_scan = valid_positions(lens, k, runs)
+    sw, mw = w.ref.packed_words()
+    n_win = ib.window_count(lens, W, k)
+
+    # random-sector ceiling of this GPU (before the big allocations)
+    sector_rate = ib.random_sector_rate(16 << 30) if args.scale >= 0.5 else ib.random_sector_rate(4 << 30)
+
+    # inputs generated on the device
+    t0 = time.time()
+    dseq = torch.empty(sw, dtype=torch.int64, device="cuda")
+    dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
+    w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
+    smp = sample_for_rank(w, rank)
+    bound = smp.codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
+    dcodes = torch.empty(bound, dtype=torch.int64, device="cuda")
+    n_codes = smp.codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), dcodes.data_ptr(), bound)
+    torch.cuda.synchronize()
+    t_gen = time.time() - t0
+    t0 = time.time()
+    table = ib.Table.from_codes(dcodes.data_ptr(), n_codes, k, on_device=True, device=dev)
+    info = table.info()
+    t_build = time.time() - t0
+    log(f"[bench r{rank}] generated {sum(map(int, lens)) / 1e9:.3f} Gbp + {n_codes / 1e9:.3f}e9 k-mers "
+        f"in {t_gen:.1f} s; table {info.n_buckets * 32 / 1e9:.2f} GB (format {info.format}, "
+        f"{info.stash_keys} stashed) in {t_build:.1f} s")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            value, secs, probes = cpu_arm(w, runs, steps=args.cpu_steps, warmup=1,
+                                          slice_len=args.cpu_slice, dcodes_ptr=dcodes.data_ptr(),
+                                          n_codes=n_codes)
+            cpu = {"value": value, "unit": "probes/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"{args.cpu_steps} slices of {args.cpu_slice / 1e6:g} Mbp of {w.ref.names[0]} "
+                             f"(+1 warm-up) against the full {n_codes / 1e9:.2f}e9-k-mer sample database; "
+                             f"fastibs --cpu --probe=batched, FASTIBS_THREADS={os.cpu_count()}, "
+                             f"'stats' phase seconds {', '.join(f'{s:.2f}' for s in secs[1:])}"}
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": "probes/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+    del dcodes
+    torch.cuda.empty_cache()
+
+    ref = ib.Reference(dseq.data_ptr(), dmask.data_ptr(), lens, device=dev, on_device=True)
+    rows_dev = torch.empty(max(n_win, 1) * 6, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+
+    def step():
+        ib.scan_async(table, ref, W, rows_dev.data_ptr(), n_win, stream.cuda_stream)
+
+    # warm-up (allocates the scan plan on the first call)
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ib.launch_count()
+    with Clocks(dev) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    launches = ib.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_step = ms / args.steps
+    total_probes = probes_per_scan * world
+    value = total_probes / (ms_step * 1e-3)
+    rows = rows_dev[: n_win * 6].cpu().numpy().view(ib.WINDOW_DTYPE)
+
+    # e2e: pinned host reference in, rows out, through ibs_scan_packed
+    hseq = dseq.cpu().pin_memory()
+    hmask = dmask.cpu().pin_memory()
+    hrows = torch.empty(max(n_win, 1) * 6, dtype=torch.int32).pin_memory()
+    for _ in range(2):
+        ib.scan_packed(table, hseq.data_ptr(), hmask.data_ptr(), lens, W, hrows.data_ptr())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ib.scan_packed(table, hseq.data_ptr(), hmask.data_ptr(), lens, W, hrows.data_ptr())
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_rows = hrows[: n_win * 6].numpy().view(ib.WINDOW_DTYPE)
+    assert np.array_equal(e2e_rows, rows), "e2e rows differ from the resident scan's"
+    h2d = (sw + mw) * 8 + n_win * 32 + (n_win + 1) * 4
+    d2h = n_win * 24
+
+    peak, peak_kind = measured_peaks()
+    achieved = probes_per_scan / (ms_step * 1e-3) * BYTES_PER_PROBE / 1e9
+    checksum = int(rows["observed_kmers"].astype(np.int64).sum())
+    out = {
+        "metric": METRIC, "value": value, "unit": "probes/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded generator; stands in for plant-genome inputs not available here)",
+        "config": {"workload": w.name, "reference_bp": int(sum(map(int, lens))), "contigs": len(lens),
+                   "sample_kmers": int(n_codes), "k": k, "window": W, "windows": int(n_win),
+                   "probes_per_scan": int(probes_per_scan), "parallelism": f"{world} sample(s), one per GPU",
+                   "l2": f"inputs larger than L2: {info.n_buckets * 32 / 1e9:.1f} GB table, "
+                         f"{(sw + mw) * 8 / 1e9:.2f} GB packed reference"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": profiled_traffic(w.name),
+                     "bytes_per_probe": BYTES_PER_PROBE,
+                     "random_sector_peak": sector_rate * BYTES_PER_PROBE / 1e9,
+                     "random_sector_frac": (probes_per_scan / (ms_step * 1e-3)) / sector_rate,
+                     "note": "achieved = probes/s x (32 B bucket sector + 0.375 B streamed reference); "
+                             "random_sector_peak = live GUPS-style random 32 B reads x the same bytes"},
+        "e2e": {"value": total_probes / e2e_s, "unit": "probes/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3,
+                "call": "ibs_scan_packed (pinned host 2-bit reference -> host rows)"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "extra": {"gbp_x_samples_per_s": sum(map(int, lens)) * world / (ms_step * 1e-3) / 1e9,
+                  "table": {"format": int(info.format), "buckets": int(info.n_buckets),
+                            "fp_bits": int(info.fp_bits), "stash_keys": int(info.stash_keys),
+                            "device_gb": info.device_bytes / 1e9, "build_s": t_build},
+                  "rows_checksum_observed": checksum, "gen_s": t_gen},
+    }
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    table.close()
+    ref.free()
+    return out
+
+
+def reference_arm(args, w):
+    """--impl reference: the reference's CPU-BATCHED scan on bounded slices."""
+    import torch
+    import ibs_b200 as ib
+    binp = REPO / "oracle" / "_ref" / "fastibs"
+    if not binp.exists():
+        return {"impl": "reference", "unavailable": "oracle/_ref/fastibs was not built (the reference "
+                "sources are needed at build time)"}
+    runs = w.ref.n_runs()
+    d = cache_dir(w)
+    codes_ptr, n_codes, keep = None, 0, []
+    if not (d / "db" / "complete").exists():
+        if not torch.cuda.is_available():
+            return {"impl": "reference", "unavailable": "no GPU to generate the sample database"}
+        sw, mw = w.ref.packed_words()
+        dseq = torch.empty(sw, dtype=torch.int64, device="cuda")
+        dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
+        w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
+        bound = w.samples[0].codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
+        dcodes = torch.empty(bound, dtype=torch.int64, device="cuda")
+        n_codes = w.samples[0].codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), dcodes.data_ptr(), bound)
+        codes_ptr = dcodes.data_ptr()
+        keep = [dseq, dmask, dcodes]
+    value, secs, probes = cpu_arm(w, runs, steps=args.steps, warmup=args.warmup,
+                                  slice_len=args.cpu_slice, dcodes_ptr=codes_ptr, n_codes=n_codes)
+    del keep
+    timed = secs[args.warmup:]
+    ms_step = 1e3 * sum(timed) / len(timed)
+    return {
+        "metric": METRIC, "value": value, "unit": "probes/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "impl": "reference",
+        "data": "synthetic (seeded generator; stands in for plant-genome inputs not available here)",
+        "config": {"workload": w.name, "k": w.k, "window": w.window,
+                   "step": f"one {args.cpu_slice / 1e6:g} Mbp slice of {w.ref.names[0]} against the full "
+                           f"sample database"},
+        "cpu_baseline": {"value": value, "unit": "probes/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"{args.steps} timed + {args.warmup} warm-up slices of "
+                                   f"{args.cpu_slice / 1e6:g} Mbp; fastibs --cpu --probe=batched "
+                                   f"(CPU-BATCHED, FASTIBS_THREADS={os.cpu_count()}); probes/s = valid "
+                                   f"positions / 'stats' phase seconds"},
+        "e2e": {"value": value, "unit": "probes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="plain_2gbp")
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (testing)")
+    ap.add_argument("--cpu-slice", type=int, default=50_000_000, help="bases per CPU-baseline slice")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    from ibs_b200 import configs
+    fn = getattr(configs, args.workload)
+    w = fn(scale=args.scale) if args.scale != 1.0 else fn()
+    args.cpu_slice = min(args.cpu_slice, int(w.ref.lens[0]) // 2)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(reference_arm(args, w)), flush=True)
+        return 0
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    out = gpu_arm(args, w, rank, world, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,173 @@
+// Internal declarations of libibs: error plumbing, the handle structs behind
+// the C-ABI, and the device-side table lookup shared by every scan kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ibs.h"
+#include "ibs_core.cuh"
+
+namespace ibs {
+
+// ---- errors ---------------------------------------------------------------
+void set_error(const std::string &msg);
+void clear_error();
+std::atomic<uint64_t> &launch_counter();
+
+// "CUDA error in <what>: <text>", the reference's message shape
+// (src/gpu/EncodeProbe.cu:15-20).
+ibs_status cuda_fail(cudaError_t e, const char *what);
+
+#define IBS_CUDA(call, what)                                  \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess)                                \
+            return ::ibs::cuda_fail(e_, what);                \
+    } while (0)
+
+#define IBS_LAUNCHED() (::ibs::launch_counter().fetch_add(1, std::memory_order_relaxed))
+
+// RAII guard that makes `dev` current and restores the previous device.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+            prev = -1;
+        ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0)
+            cudaSetDevice(prev);
+    }
+};
+
+// ---- device table view ----------------------------------------------------
+struct TableView {
+    TableGeom g;
+    const uint4 *buckets; // 2 x uint4 per bucket
+    const uint64_t *stash;
+};
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ bool stash_lookup(const TableView &t, uint64_t code)
+{
+    if (t.g.stashBuckets == 0)
+        return false;
+    uint64_t b = stash_home(code, t.g.stashBuckets);
+    for (uint64_t i = 0; i < t.g.stashBuckets; ++i) {
+        const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(t.stash + 4 * b);
+        const ulonglong2 a = __ldg(p), c = __ldg(p + 1);
+        if (a.x == code || a.y == code || c.x == code || c.y == code)
+            return true;
+        if (a.x == STASH_EMPTY || a.y == STASH_EMPTY || c.x == STASH_EMPTY || c.y == STASH_EMPTY)
+            return false;
+        b = (b + 1) & (t.g.stashBuckets - 1);
+    }
+    return false;
+}
+
+// One bucket compare, given the bucket's two 16-byte halves. Returns 1 on a
+// hit, 0 on a sure miss, 2 when the bucket overflowed into the stash.
+template <uint32_t FMT>
+__device__ __forceinline__ uint32_t bucket_match(const uint4 &v0, const uint4 &v1, uint64_t fp)
+{
+    if (FMT == FMT_B8X32) {
+        const uint32_t f = (uint32_t)fp;
+        const bool hit = (v0.x == f) | (v0.y == f) | (v0.z == f) | (v0.w == f) | (v1.x == f) |
+                         (v1.y == f) | (v1.z == f) | (v1.w == f);
+        return hit ? 1u : (v1.w == B8_OVERFLOW ? 2u : 0u);
+    } else {
+        const uint32_t qhi = (uint32_t)(fp >> 8), qlo = (uint32_t)(fp & 0xff);
+        const uint32_t cnt = (v1.w >> 16) & 0xff;
+        bool hit = false;
+        hit |= (0 < cnt) & (v0.x == qhi) & ((v1.z & 0xff) == qlo);
+        hit |= (1 < cnt) & (v0.y == qhi) & (((v1.z >> 8) & 0xff) == qlo);
+        hit |= (2 < cnt) & (v0.z == qhi) & (((v1.z >> 16) & 0xff) == qlo);
+        hit |= (3 < cnt) & (v0.w == qhi) & ((v1.z >> 24) == qlo);
+        hit |= (4 < cnt) & (v1.x == qhi) & ((v1.w & 0xff) == qlo);
+        hit |= (5 < cnt) & (v1.y == qhi) & (((v1.w >> 8) & 0xff) == qlo);
+        return hit ? 1u : ((v1.w >> 24) & 1u ? 2u : 0u);
+    }
+}
+
+template <uint32_t FMT>
+__device__ __forceinline__ bool table_lookup(const TableView &t, uint64_t code)
+{
+    const uint64_t h = perm_hash(code, t.g.bits);
+    const uint64_t r = bucket_of(h, t.g);
+    const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);
+    const uint32_t m = bucket_match<FMT>(v0, v1, fp_of(h, t.g));
+    return m == 1u || (m == 2u && stash_lookup(t, code));
+}
+#endif
+
+} // namespace ibs
+
+// ---- handles ----------------------------------------------------------------
+struct ibs_table {
+    int device = 0;
+    ibs::TableGeom geom{};
+    uint4 *buckets = nullptr;
+    uint64_t *stash = nullptr;
+    uint64_t nKeys = 0, stashKeys = 0;
+    double buildSeconds = 0;
+    uint64_t deviceBytes = 0;
+    ibs::TableView view() const { return ibs::TableView{geom, buckets, stash}; }
+};
+
+namespace ibs {
+// Per-window descriptor on the device.
+struct WinDesc {
+    uint64_t base; // packed base offset of the window's first base
+    uint32_t nPos; // k-mer positions
+    int32_t start, end;
+    uint32_t pad;
+};
+
+// Windows, spans and scratch of one (reference, W, k, span length) plan.
+struct ScanPlan {
+    uint32_t W = 0, k = 0, spanLen = 0;
+    uint64_t nWin = 0, nSpans = 0;
+    std::vector<WinDesc> win;     // host copy
+    std::vector<uint32_t> span0;  // host copy, nWin + 1
+    WinDesc *dWin = nullptr;
+    uint32_t *dSpan0 = nullptr;
+    SegStats *dSpans = nullptr;   // scratch: one summary per span
+    void release();
+};
+
+// Build the plan's host arrays for contigs `lens` starting at packed
+// offsets `baseOff`.
+void plan_windows(ScanPlan &p, const std::vector<uint64_t> &lens,
+                  const std::vector<uint64_t> &baseOff, uint32_t W, uint32_t k, uint32_t spanLen);
+
+// Launch the span kernel over spans [s0, s1) and, when fin, the window
+// finalizer over every window of the plan.
+ibs_status launch_scan(const ibs_table *t, const uint64_t *dSeq, const uint64_t *dMask,
+                       const ScanPlan &p, uint64_t s0, uint64_t s1, cudaStream_t st);
+ibs_status launch_finalize(const ScanPlan &p, uint32_t k, ibs_window *dRows, cudaStream_t st);
+ibs_status launch_panel(ibs_table *const *tables, uint32_t nTables, const uint64_t *dSeq,
+                        const uint64_t *dMask, const ScanPlan &p, ibs_window *dRows,
+                        SegStats *dSpans, cudaStream_t st);
+} // namespace ibs
+
+struct ibs_reference {
+    int device = 0;
+    std::vector<uint64_t> lens, baseOff;
+    uint64_t seqWords = 0, maskWords = 0;
+    uint64_t *dSeq = nullptr, *dMask = nullptr;
+    ibs::ScanPlan plan;                 // cached for the last (W, k)
+    ibs_window *dRows = nullptr;        // cached row buffer for ibs_scan
+    uint64_t dRowsCap = 0;
+    ibs::SegStats *dPanelSpans = nullptr; // panel scratch
+    uint64_t dPanelSpansCap = 0;
+    cudaStream_t stream = nullptr;
+};

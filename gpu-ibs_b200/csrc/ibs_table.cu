@@ -1,0 +1,713 @@
+// Device table: KMC 3 decode and the sector-bucket build.
+//
+// ibs_open reads the KMC 3 random-access files with the same layout rules as
+// the reference's KmcRaIndex (src/gpu/KmcRaIndex.hpp:497-708): header fields
+// and version from the end of .kmc_pre, the bin-major prefix LUT with KMC's
+// total+1 guard, and big-endian suffix records followed by counter bytes in
+// .kmc_suf. Records are decoded on the device (prefix from the LUT bucket,
+// suffix bytes to an integer, counters dropped) straight into canonical
+// codes, which the build then hashes into 32-byte buckets.
+#include "ibs_internal.cuh"
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <thread>
+
+namespace ibs {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_error;
+
+void set_error(const std::string &msg) { g_error = msg; }
+void clear_error() { g_error.clear(); }
+
+std::atomic<uint64_t> &launch_counter()
+{
+    static std::atomic<uint64_t> c{0};
+    return c;
+}
+
+ibs_status cuda_fail(cudaError_t e, const char *what)
+{
+    set_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+    cudaGetLastError(); // clear a sticky-free error so the next call starts clean
+    return e == cudaErrorMemoryAllocation ? IBS_ERR_NOMEM : IBS_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// geometry
+// ---------------------------------------------------------------------------
+static uint32_t floor_log2(uint64_t x) { return 63u - (uint32_t)__builtin_clzll(x); }
+
+static uint64_t next_pow2(uint64_t x)
+{
+    uint64_t p = 1;
+    while (p < x)
+        p <<= 1;
+    return p;
+}
+
+static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opts *o)
+{
+    TableGeom g{};
+    g.k = k;
+    g.bits = 2 * k;
+    const double lam = (o && o->keys_per_bucket > 0) ? o->keys_per_bucket : 4.0;
+    const uint64_t space = g.bits >= 64 ? ~0ull : (1ull << g.bits);
+    auto clampN = [&](uint64_t n) {
+        if (n < 1)
+            n = 1;
+        if (g.bits < 64 && n > space)
+            n = space;
+        return n;
+    };
+    const uint64_t n8 = clampN((uint64_t)((double)nKeys / lam) + 1);
+    const uint64_t min8 = g.bits > 31 ? (1ull << (g.bits - 31)) : 1;
+    const uint64_t n6 = clampN((uint64_t)((double)nKeys / (lam * 6.0 / 8.0)) + 1);
+    const uint64_t min6 = g.bits > 40 ? (1ull << (g.bits - 40)) : 1;
+    uint32_t fmt = o ? o->force_format : 0;
+    if (fmt == 0)
+        fmt = (std::max(n8, min8) <= 2 * n8) ? FMT_B8X32 : FMT_B6X40;
+    g.format = fmt;
+    g.nBuckets = fmt == FMT_B8X32 ? std::max(n8, min8) : std::max(n6, min6);
+    g.nBuckets = clampN(g.nBuckets);
+    int fpb = (int)g.bits - (int)floor_log2(g.nBuckets);
+    g.fpBits = (uint32_t)std::max(fpb, 1);
+    g.stashBuckets = 0;
+    return g;
+}
+
+// ---------------------------------------------------------------------------
+// build kernels
+// ---------------------------------------------------------------------------
+__global__ void k_count(const uint64_t *__restrict__ codes, uint64_t n, TableGeom g,
+                        uint32_t *__restrict__ cnt)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t h = perm_hash(codes[i], g.bits);
+        atomicAdd(cnt + bucket_of(h, g), 1u);
+    }
+}
+
+// Marks overflowing buckets, records B6x40 counts, sums the keys that go to
+// the stash and resets the counters for the placement pass.
+__global__ void k_mark(uint32_t *__restrict__ cnt, uint64_t nb, TableGeom g,
+                       uint32_t *__restrict__ words, unsigned long long *__restrict__ overflowKeys)
+{
+    unsigned long long local = 0;
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < nb;
+         r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = cnt[r];
+        if (g.format == FMT_B8X32) {
+            if (c > 8) {
+                words[r * 8 + 7] = B8_OVERFLOW;
+                local += c - 7;
+            }
+        } else {
+            const uint32_t keep = c > 6 ? 6 : c;
+            const uint32_t flags = c > 6 ? 1u : 0u;
+            if (c > 6)
+                local += c - 6;
+            words[r * 8 + 7] = (words[r * 8 + 7] & 0x0000ffffu) | (keep << 16) | (flags << 24);
+        }
+        cnt[r] = 0;
+    }
+    for (int o = 16; o; o >>= 1)
+        local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local)
+        atomicAdd(overflowKeys, local);
+}
+
+__device__ __forceinline__ bool stash_insert(uint64_t *stash, uint64_t stashBuckets, uint64_t code)
+{
+    uint64_t b = stash_home(code, stashBuckets);
+    for (uint64_t i = 0; i < stashBuckets; ++i) {
+        for (int s = 0; s < 4; ++s) {
+            unsigned long long *slot = reinterpret_cast<unsigned long long *>(stash + 4 * b + s);
+            const unsigned long long old = atomicCAS(slot, (unsigned long long)STASH_EMPTY,
+                                                     (unsigned long long)code);
+            if (old == STASH_EMPTY || old == code)
+                return true;
+        }
+        b = (b + 1) & (stashBuckets - 1);
+    }
+    return false;
+}
+
+__global__ void k_place(const uint64_t *__restrict__ codes, uint64_t n, TableGeom g,
+                        uint32_t *__restrict__ cnt, uint32_t *__restrict__ words,
+                        uint64_t *__restrict__ stash, int *__restrict__ err)
+{
+    uint8_t *bytes = reinterpret_cast<uint8_t *>(words);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t code = codes[i];
+        const uint64_t h = perm_hash(code, g.bits);
+        const uint64_t r = bucket_of(h, g);
+        const uint64_t fp = fp_of(h, g);
+        const uint32_t s = atomicAdd(cnt + r, 1u);
+        bool stashed = false;
+        if (g.format == FMT_B8X32) {
+            const uint32_t limit = words[r * 8 + 7] == B8_OVERFLOW ? 7u : 8u;
+            if (s < limit)
+                words[r * 8 + s] = (uint32_t)fp;
+            else
+                stashed = true;
+        } else {
+            if (s < 6) {
+                words[r * 8 + s] = (uint32_t)(fp >> 8);
+                bytes[r * 32 + 24 + s] = (uint8_t)(fp & 0xff);
+            } else
+                stashed = true;
+        }
+        if (stashed && !stash_insert(stash, g.stashBuckets, code))
+            atomicExch(err, 1);
+    }
+}
+
+// Record r of a .kmc_suf chunk -> canonical code. The LUT bucket j holding
+// record r is the last j with lut[j] <= r (empty buckets repeat a value and
+// are skipped by taking the last); j mod 4^p is the prefix.
+__global__ void k_decode(const uint8_t *__restrict__ raw, uint64_t r0, uint64_t nRec,
+                         uint32_t recBytes, uint32_t sufBytes, const uint64_t *__restrict__ lut,
+                         uint64_t lutN, uint64_t prefixMask, uint32_t sufBits,
+                         uint64_t *__restrict__ out)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nRec;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = r0 + i;
+        uint64_t lo = 0, hi = lutN - 1;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(lut + mid) <= r)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const uint8_t *q = raw + i * recBytes;
+        uint64_t suf = 0;
+        for (uint32_t b = 0; b < sufBytes; ++b)
+            suf = (suf << 8) | q[b];
+        const uint64_t prefix = lo & prefixMask;
+        out[r] = sufBits >= 64 ? suf : ((prefix << sufBits) | suf);
+    }
+}
+
+template <uint32_t FMT>
+__global__ void k_probe(TableView t, const uint64_t *__restrict__ codes, uint64_t n,
+                        uint8_t *__restrict__ hits)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        hits[i] = table_lookup<FMT>(t, codes[i]) ? 1 : 0;
+}
+
+static int grid_for(uint64_t n, int threads)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t want = (n + threads - 1) / threads;
+    const uint64_t cap = (uint64_t)sms * 16;
+    return (int)std::max<uint64_t>(1, std::min(want, cap));
+}
+
+// Builds the table from device codes. The caller has set the device.
+static ibs_status build_from_device_codes(ibs_table *t, const uint64_t *dCodes, uint64_t n,
+                                          uint32_t k, const ibs_table_opts *o)
+{
+    t->geom = choose_geometry(n, k, o);
+    t->nKeys = n;
+    TableGeom &g = t->geom;
+    const uint64_t nb = g.nBuckets;
+    IBS_CUDA(cudaMalloc(&t->buckets, nb * 32), "table alloc");
+    t->deviceBytes = nb * 32;
+    IBS_CUDA(cudaMemset(t->buckets, g.format == FMT_B8X32 ? 0xff : 0x00, nb * 32), "table init");
+    uint32_t *cnt = nullptr;
+    unsigned long long *dOverflow = nullptr;
+    int *dErr = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(cnt);
+        cudaFree(dOverflow);
+        cudaFree(dErr);
+    };
+    cudaError_t e = cudaMalloc(&cnt, nb * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dOverflow, 8);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dErr, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemset(cnt, 0, nb * 4);
+    if (e == cudaSuccess)
+        e = cudaMemset(dOverflow, 0, 8);
+    if (e == cudaSuccess)
+        e = cudaMemset(dErr, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        cleanup();
+        return cuda_fail(e, "table build scratch");
+    }
+    uint32_t *words = reinterpret_cast<uint32_t *>(t->buckets);
+    k_count<<<grid_for(n, 256), 256>>>(dCodes, n, g, cnt);
+    IBS_LAUNCHED();
+    k_mark<<<grid_for(nb, 256), 256>>>(cnt, nb, g, words, dOverflow);
+    IBS_LAUNCHED();
+    unsigned long long overflow = 0;
+    e = cudaMemcpy(&overflow, dOverflow, 8, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cleanup();
+        return cuda_fail(e, "table build count");
+    }
+    t->stashKeys = overflow;
+    if (overflow) {
+        g.stashBuckets = next_pow2((overflow * 2 + 3) / 4);
+        e = cudaMalloc(&t->stash, g.stashBuckets * 32);
+        if (e == cudaSuccess)
+            e = cudaMemset(t->stash, 0xff, g.stashBuckets * 32);
+        if (e != cudaSuccess) {
+            cleanup();
+            return cuda_fail(e, "stash alloc");
+        }
+        t->deviceBytes += g.stashBuckets * 32;
+    }
+    k_place<<<grid_for(n, 256), 256>>>(dCodes, n, g, cnt, words, t->stash, dErr);
+    IBS_LAUNCHED();
+    int herr = 0;
+    e = cudaMemcpy(&herr, dErr, sizeof(int), cudaMemcpyDeviceToHost);
+    cleanup();
+    if (e != cudaSuccess)
+        return cuda_fail(e, "table build place");
+    if (herr) {
+        set_error("table build: stash full");
+        return IBS_ERR_CAPACITY;
+    }
+    return IBS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// KMC 3 files (layout as read by src/gpu/KmcRaIndex.hpp:497-708)
+// ---------------------------------------------------------------------------
+struct KmcHeader {
+    uint32_t version = 0, k = 0, mode = 0, counterSize = 0, p = 0, sigLen = 0;
+    uint64_t total = 0, headerOffset = 0, fileBytes = 0;
+};
+
+struct File {
+    FILE *f = nullptr;
+    explicit File(const std::string &path) { f = fopen(path.c_str(), "rb"); }
+    ~File()
+    {
+        if (f)
+            fclose(f);
+    }
+};
+
+static bool read_at(FILE *f, long long off, void *dst, size_t n)
+{
+    if (fseeko(f, off, SEEK_SET) != 0)
+        return false;
+    return fread(dst, 1, n, f) == n;
+}
+
+static uint64_t file_size(FILE *f)
+{
+    fseeko(f, 0, SEEK_END);
+    return (uint64_t)ftello(f);
+}
+
+static ibs_status check_markers(FILE *f, uint64_t size, const char *marker, const std::string &path)
+{
+    char head[4], tail[4];
+    if (size < 8 || !read_at(f, 0, head, 4) || !read_at(f, (long long)size - 4, tail, 4)) {
+        set_error("KMC: short read of markers in " + path);
+        return IBS_ERR_IO;
+    }
+    if (memcmp(head, marker, 4) || memcmp(tail, marker, 4)) {
+        set_error("KMC: bad marker in " + path);
+        return IBS_ERR_FORMAT;
+    }
+    return IBS_OK;
+}
+
+static ibs_status read_kmc_header(FILE *f, const std::string &path, KmcHeader &h)
+{
+    h.fileBytes = file_size(f);
+    ibs_status s = check_markers(f, h.fileBytes, "KMCP", path);
+    if (s != IBS_OK)
+        return s;
+    if (h.fileBytes < 20 || !read_at(f, (long long)h.fileBytes - 12, &h.version, 4)) {
+        set_error("KMC: short read of version in " + path);
+        return IBS_ERR_IO;
+    }
+    if (h.version != 0 && h.version != 0x200) {
+        set_error("KMC: unsupported KMC format version in " + path);
+        return IBS_ERR_FORMAT;
+    }
+    unsigned char off = 0; // only the first byte of header_offset is read, as KMC does
+    if (!read_at(f, (long long)h.fileBytes - 8, &off, 1)) {
+        set_error("KMC: short read of header offset in " + path);
+        return IBS_ERR_IO;
+    }
+    h.headerOffset = off;
+    const long long pos = (long long)h.fileBytes - (long long)(h.headerOffset + 8);
+    if (pos < 4) {
+        set_error("KMC: header offset out of range in " + path);
+        return IBS_ERR_FORMAT;
+    }
+    if (h.version == 0x200) {
+        uint32_t w[5];
+        if (!read_at(f, pos, w, sizeof w) || !read_at(f, pos + 28, &h.total, 8)) {
+            set_error("KMC: short read of header in " + path);
+            return IBS_ERR_IO;
+        }
+        h.k = w[0], h.mode = w[1], h.counterSize = w[2], h.p = w[3], h.sigLen = w[4];
+    } else {
+        uint32_t w[4];
+        if (!read_at(f, pos, w, sizeof w) || !read_at(f, pos + 24, &h.total, 8)) {
+            set_error("KMC: short read of header in " + path);
+            return IBS_ERR_IO;
+        }
+        h.k = w[0], h.mode = w[1], h.counterSize = w[2], h.p = w[3];
+    }
+    if (h.mode != 0) {
+        set_error("KMC: Quake-compatible counters are not supported");
+        return IBS_ERR_UNSUPPORTED;
+    }
+    if (h.k == 0 || h.k > 32) {
+        set_error("KMC: k=" + std::to_string(h.k) + " is not supported (k must be 1..32)");
+        return IBS_ERR_UNSUPPORTED;
+    }
+    if (h.p > h.k || (h.k - h.p) % 4 != 0 || h.k - h.p > 32) {
+        set_error("KMC: unexpected suffix geometry");
+        return IBS_ERR_FORMAT;
+    }
+    return IBS_OK;
+}
+
+// Reads the prefix LUT (bin-major for 0x200) with the guard set to
+// total + 1 as KMC sets it (src/gpu/KmcRaIndex.hpp:564-591).
+static ibs_status read_kmc_lut(FILE *f, const std::string &path, const KmcHeader &h,
+                               std::vector<uint64_t> &lut)
+{
+    uint64_t entries;
+    if (h.version == 0x200) {
+        const uint64_t sigEntries = (1ull << (2 * h.sigLen)) + 1;
+        const uint64_t fixed = sigEntries * 4 + h.headerOffset + 8 + 12;
+        if (h.fileBytes < fixed) {
+            set_error("KMC: .kmc_pre too small in " + path);
+            return IBS_ERR_FORMAT;
+        }
+        const uint64_t lutArea = h.fileBytes - 12 - (sigEntries * 4 + h.headerOffset + 8);
+        entries = (lutArea + 8) / 8;
+    } else {
+        entries = (1ull << (2 * h.p)) + 1;
+    }
+    const uint64_t single = 1ull << (2 * h.p);
+    if (entries < 2 || (entries - 1) % single != 0) {
+        set_error("KMC: LUT size is not a whole number of bins in " + path);
+        return IBS_ERR_FORMAT;
+    }
+    lut.resize(entries);
+    if (!read_at(f, 4, lut.data(), entries * 8)) {
+        set_error("KMC: short read of prefix LUT in " + path);
+        return IBS_ERR_IO;
+    }
+    lut[entries - 1] = h.total + 1;
+    return IBS_OK;
+}
+
+} // namespace ibs
+
+using namespace ibs;
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" const char *ibs_last_error(void) { return ibs::g_error.c_str(); }
+
+extern "C" int ibs_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+extern "C" uint64_t ibs_launch_count(void) { return launch_counter().load(); }
+
+static ibs_status check_device(int dev)
+{
+    const int n = ibs_device_count();
+    if (n == 0) {
+        set_error("no usable CUDA device (the scan has no CPU fallback)");
+        return IBS_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= n) {
+        set_error("device " + std::to_string(dev) + " out of range");
+        return IBS_ERR_ARG;
+    }
+    return IBS_OK;
+}
+
+extern "C" ibs_status ibs_table_from_codes(const uint64_t *codes, uint64_t n, uint32_t k,
+                                           int codes_on_device, const ibs_table_opts *opts,
+                                           ibs_table **out)
+{
+    clear_error();
+    if (!out || (!codes && n) || k == 0 || k > 32) {
+        set_error("ibs_table_from_codes: bad argument");
+        return IBS_ERR_ARG;
+    }
+    *out = nullptr;
+    const int dev = opts ? opts->device : 0;
+    ibs_status s = check_device(dev);
+    if (s != IBS_OK)
+        return s;
+    DeviceGuard guard(dev);
+    const auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<ibs_table> t(new ibs_table);
+    t->device = dev;
+    uint64_t *dCodes = nullptr;
+    const uint64_t *src = codes;
+    if (!codes_on_device && n) {
+        IBS_CUDA(cudaMalloc(&dCodes, n * 8), "codes alloc");
+        cudaError_t e = cudaMemcpy(dCodes, codes, n * 8, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(dCodes);
+            return cuda_fail(e, "codes upload");
+        }
+        src = dCodes;
+    }
+    s = build_from_device_codes(t.get(), src, n, k, opts);
+    cudaFree(dCodes);
+    if (s != IBS_OK) {
+        ibs_close(t.release());
+        return s;
+    }
+    t->buildSeconds =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = t.release();
+    return IBS_OK;
+}
+
+extern "C" ibs_status ibs_open(const char *prefix, const ibs_table_opts *opts, ibs_table **out)
+{
+    clear_error();
+    if (!prefix || !out) {
+        set_error("ibs_open: bad argument");
+        return IBS_ERR_ARG;
+    }
+    *out = nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
+    const std::string pre = std::string(prefix) + ".kmc_pre";
+    const std::string suf = std::string(prefix) + ".kmc_suf";
+    KmcHeader h;
+    std::vector<uint64_t> lut;
+    {
+        File f(pre);
+        if (!f.f) {
+            set_error("KMC: cannot open " + pre);
+            return IBS_ERR_IO;
+        }
+        ibs_status s = read_kmc_header(f.f, pre, h);
+        if (s != IBS_OK)
+            return s;
+        s = read_kmc_lut(f.f, pre, h, lut);
+        if (s != IBS_OK)
+            return s;
+    }
+    File sf(suf);
+    if (!sf.f) {
+        set_error("KMC: cannot open " + suf);
+        return IBS_ERR_IO;
+    }
+    const uint64_t sufSize = file_size(sf.f);
+    {
+        ibs_status s = check_markers(sf.f, sufSize, "KMCS", suf);
+        if (s != IBS_OK)
+            return s;
+    }
+    const uint32_t sufBytes = (h.k - h.p) / 4;
+    const uint32_t recBytes = sufBytes + h.counterSize;
+    if (recBytes == 0 || sufSize - 8 < h.total * (uint64_t)recBytes) {
+        set_error("KMC: suffix file smaller than expected: " + suf);
+        return IBS_ERR_FORMAT;
+    }
+    const int dev = opts ? opts->device : 0;
+    ibs_status s = check_device(dev);
+    if (s != IBS_OK)
+        return s;
+    DeviceGuard guard(dev);
+
+    uint64_t *dCodes = nullptr, *dLut = nullptr;
+    uint8_t *dRaw[2] = {nullptr, nullptr};
+    uint8_t *hRaw[2] = {nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    auto cleanup = [&]() {
+        if (st)
+            cudaStreamSynchronize(st);
+        cudaFree(dCodes);
+        cudaFree(dLut);
+        for (int i = 0; i < 2; i++) {
+            cudaFree(dRaw[i]);
+            cudaFreeHost(hRaw[i]);
+            if (done[i])
+                cudaEventDestroy(done[i]);
+        }
+        if (st)
+            cudaStreamDestroy(st);
+    };
+    const uint64_t total = h.total;
+    const uint64_t chunkRecs = std::max<uint64_t>(1, (256ull << 20) / recBytes);
+    const uint64_t chunkBytes = chunkRecs * recBytes;
+    cudaError_t e = cudaMalloc(&dCodes, std::max<uint64_t>(total, 1) * 8);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dLut, lut.size() * 8);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dLut, lut.data(), lut.size() * 8, cudaMemcpyHostToDevice);
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+        e = cudaMalloc(&dRaw[i], chunkBytes);
+        if (e == cudaSuccess)
+            e = cudaMallocHost(&hRaw[i], chunkBytes);
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cleanup();
+        return cuda_fail(e, "KMC decode buffers");
+    }
+    // Double-buffered: read chunk i into pinned buffer i%2 while chunk i-1
+    // uploads and decodes.
+    if (fseeko(sf.f, 4, SEEK_SET) != 0) {
+        cleanup();
+        set_error("KMC: seek failed in " + suf);
+        return IBS_ERR_IO;
+    }
+    const uint64_t lutN = lut.size() - 1;
+    const uint64_t prefixMask = (1ull << (2 * h.p)) - 1;
+    int slot = 0;
+    for (uint64_t r0 = 0; r0 < total; r0 += chunkRecs, slot ^= 1) {
+        const uint64_t nRec = std::min(chunkRecs, total - r0);
+        e = cudaEventSynchronize(done[slot]);
+        if (e != cudaSuccess)
+            break;
+        if (fread(hRaw[slot], 1, nRec * recBytes, sf.f) != nRec * recBytes) {
+            cleanup();
+            set_error("KMC: short read of suffix records in " + suf);
+            return IBS_ERR_IO;
+        }
+        e = cudaMemcpyAsync(dRaw[slot], hRaw[slot], nRec * recBytes, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess)
+            break;
+        k_decode<<<grid_for(nRec, 256), 256, 0, st>>>(dRaw[slot], r0, nRec, recBytes, sufBytes,
+                                                      dLut, lutN, prefixMask, 2 * (h.k - h.p),
+                                                      dCodes);
+        IBS_LAUNCHED();
+        e = cudaEventRecord(done[slot], st);
+        if (e != cudaSuccess)
+            break;
+    }
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess)
+        e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cleanup();
+        return cuda_fail(e, "KMC decode");
+    }
+    for (int i = 0; i < 2; i++) {
+        cudaFree(dRaw[i]);
+        dRaw[i] = nullptr;
+        cudaFreeHost(hRaw[i]);
+        hRaw[i] = nullptr;
+    }
+    cudaFree(dLut);
+    dLut = nullptr;
+    std::unique_ptr<ibs_table> t(new ibs_table);
+    t->device = dev;
+    s = build_from_device_codes(t.get(), dCodes, total, h.k, opts);
+    cleanup();
+    if (s != IBS_OK) {
+        ibs_close(t.release());
+        return s;
+    }
+    t->buildSeconds =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = t.release();
+    return IBS_OK;
+}
+
+extern "C" ibs_status ibs_table_info_get(const ibs_table *t, ibs_table_info *info)
+{
+    clear_error();
+    if (!t || !info) {
+        set_error("ibs_table_info_get: bad argument");
+        return IBS_ERR_ARG;
+    }
+    memset(info, 0, sizeof *info);
+    info->k = t->geom.k;
+    info->format = t->geom.format;
+    info->fp_bits = t->geom.fpBits;
+    info->n_keys = t->nKeys;
+    info->n_buckets = t->geom.nBuckets;
+    info->stash_keys = t->stashKeys;
+    info->stash_buckets = t->geom.stashBuckets;
+    info->device_bytes = t->deviceBytes;
+    info->build_seconds = t->buildSeconds;
+    return IBS_OK;
+}
+
+extern "C" ibs_status ibs_probe(ibs_table *t, const uint64_t *codes, uint64_t n, uint8_t *hits)
+{
+    clear_error();
+    if (!t || (n && (!codes || !hits))) {
+        set_error("ibs_probe: bad argument");
+        return IBS_ERR_ARG;
+    }
+    if (!n)
+        return IBS_OK;
+    DeviceGuard guard(t->device);
+    uint64_t *dCodes = nullptr;
+    uint8_t *dHits = nullptr;
+    cudaError_t e = cudaMalloc(&dCodes, n * 8);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dHits, n);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dCodes, codes, n * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        if (t->geom.format == FMT_B8X32)
+            k_probe<FMT_B8X32><<<grid_for(n, 256), 256>>>(t->view(), dCodes, n, dHits);
+        else
+            k_probe<FMT_B6X40><<<grid_for(n, 256), 256>>>(t->view(), dCodes, n, dHits);
+        IBS_LAUNCHED();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(hits, dHits, n, cudaMemcpyDeviceToHost);
+    cudaFree(dCodes);
+    cudaFree(dHits);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "probe");
+    return IBS_OK;
+}
+
+extern "C" void ibs_close(ibs_table *t)
+{
+    if (!t)
+        return;
+    {
+        DeviceGuard guard(t->device);
+        cudaFree(t->buckets);
+        cudaFree(t->stash);
+    }
+    delete t;
+}

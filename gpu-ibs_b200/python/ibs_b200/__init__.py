@@ -1,0 +1,407 @@
+"""ctypes binding of the B200 fastibs scan library (libibs.so) and its tools
+library (libibs_tools.so), for tests and benchmarks.
+
+The scan itself runs only on the GPU through libibs.so; there is no Python or
+CPU implementation behind these calls. Loading fails loudly when the built
+libraries are missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parents[2]  # gpu-ibs_b200/
+LIB_DIR = PKG_DIR / "lib"
+
+IBS_OK = 0
+STATUS_NAMES = {
+    0: "OK", 1: "ERR_ARG", 2: "ERR_IO", 3: "ERR_FORMAT", 4: "ERR_CUDA", 5: "ERR_NOMEM",
+    6: "ERR_UNSUPPORTED", 7: "ERR_CAPACITY", 8: "ERR_TIMEOUT", 9: "ERR_STATE",
+}
+
+WINDOW_DTYPE = np.dtype([("start", "<i4"), ("end", "<i4"), ("total_kmers", "<i4"),
+                         ("observed_kmers", "<i4"), ("variations", "<i4"),
+                         ("kmer_distance", "<i4")])
+
+
+class IbsError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _load(name: str) -> C.CDLL:
+    path = LIB_DIR / name
+    if not path.exists():
+        raise ImportError(f"{path} is missing: build it with `make -C {PKG_DIR}` "
+                          "(the scan has no fallback without its CUDA library)")
+    return C.CDLL(str(path))
+
+
+_lib = _load("libibs.so")
+_tools = _load("libibs_tools.so")
+
+u64p = C.POINTER(C.c_uint64)
+u32p = C.POINTER(C.c_uint32)
+vp = C.c_void_p
+
+
+class TableOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("keys_per_bucket", C.c_double),
+                ("force_format", C.c_uint32), ("reserved", C.c_uint32 * 5)]
+
+
+class TableInfo(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("format", C.c_uint32), ("fp_bits", C.c_uint32),
+                ("reserved0", C.c_uint32), ("n_keys", C.c_uint64), ("n_buckets", C.c_uint64),
+                ("stash_keys", C.c_uint64), ("stash_buckets", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("build_seconds", C.c_double)]
+
+
+class SynthRefSpec(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("n_contigs", C.c_uint32), ("reserved0", C.c_uint32),
+                ("lens", u64p), ("n_frac", C.c_double), ("n_run_min", C.c_uint32),
+                ("n_run_max", C.c_uint32), ("lower_frac", C.c_double),
+                ("lower_run_min", C.c_uint32), ("lower_run_max", C.c_uint32)]
+
+
+class SynthSampleSpec(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("k", C.c_uint32), ("n_classes", C.c_uint32),
+                ("block_len", C.c_uint64), ("class_rate", C.c_double * 4),
+                ("class_prob", C.c_double * 4), ("present_frac", C.c_double),
+                ("random_frac", C.c_double), ("n_intro", C.c_uint32), ("reserved0", C.c_uint32),
+                ("intro_contig", u32p), ("intro_start", u64p), ("intro_len", u64p),
+                ("intro_rate", C.c_double)]
+
+
+class KmcSpec(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("p", C.c_uint32), ("sig_len", C.c_uint32),
+                ("n_bins", C.c_uint32), ("counter_size", C.c_uint32), ("version", C.c_uint32),
+                ("min_count", C.c_uint32), ("max_count", C.c_uint32), ("count_seed", C.c_uint64)]
+
+
+def _sig(lib, name, res, args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+_ibs_open = _sig(_lib, "ibs_open", C.c_int, [C.c_char_p, C.POINTER(TableOpts), C.POINTER(vp)])
+_ibs_from_codes = _sig(_lib, "ibs_table_from_codes", C.c_int,
+                       [vp, C.c_uint64, C.c_uint32, C.c_int, C.POINTER(TableOpts), C.POINTER(vp)])
+_ibs_info = _sig(_lib, "ibs_table_info_get", C.c_int, [vp, C.POINTER(TableInfo)])
+_ibs_probe = _sig(_lib, "ibs_probe", C.c_int, [vp, vp, C.c_uint64, vp])
+_ibs_close = _sig(_lib, "ibs_close", None, [vp])
+_ibs_packed_words = _sig(_lib, "ibs_packed_words", None, [vp, C.c_uint32, u64p, u64p])
+_ibs_pack_ascii = _sig(_lib, "ibs_pack_ascii", C.c_int,
+                       [C.POINTER(C.c_char_p), vp, C.c_uint32, vp, vp, C.c_int])
+_ibs_ref_create = _sig(_lib, "ibs_reference_create", C.c_int,
+                       [vp, vp, vp, C.c_uint32, C.c_int, C.POINTER(vp)])
+_ibs_ref_create_dev = _sig(_lib, "ibs_reference_create_device", C.c_int,
+                           [vp, vp, vp, C.c_uint32, C.c_int, C.POINTER(vp)])
+_ibs_ref_free = _sig(_lib, "ibs_reference_free", None, [vp])
+_ibs_window_count = _sig(_lib, "ibs_window_count", C.c_uint64, [vp, C.c_uint32, C.c_uint32, C.c_uint32])
+_ibs_window_bounds = _sig(_lib, "ibs_window_bounds", C.c_int,
+                          [vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint64])
+_ibs_scan = _sig(_lib, "ibs_scan", C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint64])
+_ibs_scan_async = _sig(_lib, "ibs_scan_async", C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint64, vp])
+_ibs_scan_packed = _sig(_lib, "ibs_scan_packed", C.c_int,
+                        [vp, vp, vp, vp, C.c_uint32, C.c_uint32, vp, C.c_uint64])
+_ibs_scan_panel = _sig(_lib, "ibs_scan_panel", C.c_int,
+                       [C.POINTER(vp), C.c_uint32, vp, C.c_uint32, vp, C.c_uint64])
+_ibs_last_error = _sig(_lib, "ibs_last_error", C.c_char_p, [])
+_ibs_device_count = _sig(_lib, "ibs_device_count", C.c_int, [])
+_ibs_launch_count = _sig(_lib, "ibs_launch_count", C.c_uint64, [])
+
+_t_n_runs = _sig(_tools, "ibs_synth_n_runs", C.c_uint64,
+                 [C.POINTER(SynthRefSpec), vp, vp, vp, C.c_uint64])
+_t_reference = _sig(_tools, "ibs_synth_reference", C.c_int, [C.POINTER(SynthRefSpec), vp, vp, C.c_int])
+_t_contig_ascii = _sig(_tools, "ibs_synth_contig_ascii", C.c_int,
+                       [C.POINTER(SynthRefSpec), C.c_uint32, vp])
+_t_write_fasta = _sig(_tools, "ibs_synth_write_fasta", C.c_int,
+                      [C.POINTER(SynthRefSpec), C.c_char_p, C.POINTER(C.c_char_p), C.c_uint32])
+_t_sample_codes = _sig(_tools, "ibs_synth_sample_codes", C.c_int,
+                       [C.POINTER(SynthRefSpec), C.POINTER(SynthSampleSpec), vp, vp, C.c_int, vp,
+                        C.c_uint64, u64p])
+_t_kmc_write = _sig(_tools, "ibs_kmc_write", C.c_int,
+                    [C.c_char_p, C.POINTER(KmcSpec), vp, C.c_uint64, C.c_int, u64p])
+_t_sort_unique = _sig(_tools, "ibs_sort_unique_host", C.c_uint64, [vp, C.c_uint64, C.c_int])
+_t_last_error = _sig(_tools, "ibs_tools_last_error", C.c_char_p, [])
+_t_sector_rate = _sig(_tools, "ibs_random_sector_rate", C.c_int, [C.c_uint64, C.POINTER(C.c_double)])
+
+
+def _check(status: int, tools: bool = False):
+    if status != IBS_OK:
+        msg = (_t_last_error() if tools else _ibs_last_error()) or b""
+        raise IbsError(status, msg.decode(errors="replace"))
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array, a torch tensor, or an int device pointer."""
+    if a is None:
+        return 0
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    raise TypeError(type(a))
+
+
+def device_count() -> int:
+    return _ibs_device_count()
+
+
+def launch_count() -> int:
+    return _ibs_launch_count()
+
+
+def library_paths() -> list[str]:
+    return [str(LIB_DIR / "libibs.so"), str(LIB_DIR / "libibs_tools.so")]
+
+
+# ---------------------------------------------------------------------------
+# tables
+# ---------------------------------------------------------------------------
+class Table:
+    """One sample's device-resident k-mer table (ibs_table)."""
+
+    def __init__(self, handle: int):
+        self._h = handle
+
+    @classmethod
+    def open(cls, kmc_prefix: str, device: int = 0, keys_per_bucket: float = 0.0,
+             force_format: int = 0) -> "Table":
+        opts = TableOpts(device, keys_per_bucket, force_format)
+        h = vp()
+        _check(_ibs_open(str(kmc_prefix).encode(), C.byref(opts), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_codes(cls, codes, n: int, k: int, on_device: bool, device: int = 0,
+                   keys_per_bucket: float = 0.0, force_format: int = 0) -> "Table":
+        opts = TableOpts(device, keys_per_bucket, force_format)
+        h = vp()
+        _check(_ibs_from_codes(_ptr(codes), n, k, int(on_device), C.byref(opts), C.byref(h)))
+        return cls(h.value)
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def info(self) -> TableInfo:
+        i = TableInfo()
+        _check(_ibs_info(self._h, C.byref(i)))
+        return i
+
+    def probe(self, codes: np.ndarray) -> np.ndarray:
+        codes = np.ascontiguousarray(codes, dtype=np.uint64)
+        hits = np.zeros(len(codes), dtype=np.uint8)
+        _check(_ibs_probe(self._h, _ptr(codes), len(codes), _ptr(hits)))
+        return hits
+
+    def close(self):
+        if self._h:
+            _ibs_close(self._h)
+            self._h = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# references
+# ---------------------------------------------------------------------------
+def packed_words(lens) -> tuple[int, int]:
+    lens = np.ascontiguousarray(lens, dtype=np.uint64)
+    sw, mw = C.c_uint64(), C.c_uint64()
+    _ibs_packed_words(_ptr(lens), len(lens), C.byref(sw), C.byref(mw))
+    return sw.value, mw.value
+
+
+def pack_ascii(seqs: list[bytes], threads: int = 0) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    lens = np.array([len(s) for s in seqs], dtype=np.uint64)
+    sw, mw = packed_words(lens)
+    seq = np.zeros(sw, dtype=np.uint64)
+    mask = np.zeros(mw, dtype=np.uint64)
+    arr = (C.c_char_p * max(1, len(seqs)))(*seqs)
+    _check(_ibs_pack_ascii(arr, _ptr(lens), len(seqs), _ptr(seq), _ptr(mask), threads))
+    return seq, mask, lens
+
+
+class Reference:
+    """A device-resident packed reference (ibs_reference)."""
+
+    def __init__(self, seq2bit, nmask, lens, device: int = 0, on_device: bool = False):
+        self.lens = np.ascontiguousarray(lens, dtype=np.uint64)
+        h = vp()
+        fn = _ibs_ref_create_dev if on_device else _ibs_ref_create
+        _check(fn(_ptr(seq2bit), _ptr(nmask), _ptr(self.lens), len(self.lens), device, C.byref(h)))
+        self._h = h.value
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def free(self):
+        if self._h:
+            _ibs_ref_free(self._h)
+            self._h = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def window_count(lens, W: int, k: int) -> int:
+    lens = np.ascontiguousarray(lens, dtype=np.uint64)
+    return _ibs_window_count(_ptr(lens), len(lens), W, k)
+
+
+def window_bounds(lens, W: int, k: int) -> np.ndarray:
+    lens = np.ascontiguousarray(lens, dtype=np.uint64)
+    n = window_count(lens, W, k)
+    rows = np.zeros(n, dtype=WINDOW_DTYPE)
+    _check(_ibs_window_bounds(_ptr(lens), len(lens), W, k, _ptr(rows), n))
+    return rows
+
+
+def scan(table: Table, ref: Reference, W: int) -> np.ndarray:
+    n = window_count(ref.lens, W, table.info().k)
+    rows = np.zeros(max(n, 1), dtype=WINDOW_DTYPE)
+    _check(_ibs_scan(table.handle, ref.handle, W, _ptr(rows), n))
+    return rows[:n]
+
+
+def scan_async(table: Table, ref: Reference, W: int, rows_dev, cap: int, stream: int = 0):
+    _check(_ibs_scan_async(table.handle, ref.handle, W, _ptr(rows_dev), cap, stream))
+
+
+def scan_packed(table: Table, seq2bit, nmask, lens, W: int, rows=None) -> np.ndarray:
+    lens = np.ascontiguousarray(lens, dtype=np.uint64)
+    n = window_count(lens, W, table.info().k)
+    if rows is None:
+        rows = np.zeros(max(n, 1), dtype=WINDOW_DTYPE)
+    _check(_ibs_scan_packed(table.handle, _ptr(seq2bit), _ptr(nmask), _ptr(lens), len(lens), W,
+                            _ptr(rows), n))
+    return rows[:n] if isinstance(rows, np.ndarray) else rows
+
+
+def scan_panel(tables: list[Table], ref: Reference, W: int) -> np.ndarray:
+    k = tables[0].info().k
+    n = window_count(ref.lens, W, k)
+    rows = np.zeros(max(n * len(tables), 1), dtype=WINDOW_DTYPE)
+    arr = (vp * len(tables))(*[t.handle for t in tables])
+    _check(_ibs_scan_panel(arr, len(tables), ref.handle, W, _ptr(rows), n * len(tables)))
+    return rows[: n * len(tables)].reshape(len(tables), n)
+
+
+# ---------------------------------------------------------------------------
+# synthetic inputs and the KMC writer (libibs_tools.so)
+# ---------------------------------------------------------------------------
+class RefSpec:
+    def __init__(self, seed: int, lens, n_frac=0.0, n_run=(50, 500), lower_frac=0.0,
+                 lower_run=(20, 200), names=None):
+        self.lens = np.ascontiguousarray(lens, dtype=np.uint64)
+        self.names = list(names) if names else [f"chr{i + 1}" for i in range(len(self.lens))]
+        self.c = SynthRefSpec(seed, len(self.lens), 0, self.lens.ctypes.data_as(u64p), n_frac,
+                              n_run[0], n_run[1], lower_frac, lower_run[0], lower_run[1])
+
+    def packed_words(self):
+        return packed_words(self.lens)
+
+    def reference_host(self):
+        sw, mw = self.packed_words()
+        seq = np.zeros(sw, dtype=np.uint64)
+        mask = np.zeros(mw, dtype=np.uint64)
+        _check(_t_reference(C.byref(self.c), _ptr(seq), _ptr(mask), 0), tools=True)
+        return seq, mask
+
+    def reference_device(self, seq_dev, mask_dev):
+        _check(_t_reference(C.byref(self.c), _ptr(seq_dev), _ptr(mask_dev), 1), tools=True)
+
+    def contig_ascii(self, c: int) -> bytes:
+        buf = C.create_string_buffer(int(self.lens[c]) + 1)
+        _check(_t_contig_ascii(C.byref(self.c), c, C.addressof(buf)), tools=True)
+        return buf.raw[: int(self.lens[c])]
+
+    def write_fasta(self, path: str, width: int = 80):
+        names = (C.c_char_p * len(self.names))(*[n.encode() for n in self.names])
+        _check(_t_write_fasta(C.byref(self.c), str(path).encode(), names, width), tools=True)
+
+    def n_runs(self):
+        n = _t_n_runs(C.byref(self.c), None, None, None, 0)
+        c = np.zeros(n, np.uint32)
+        s = np.zeros(n, np.uint64)
+        ln = np.zeros(n, np.uint64)
+        _t_n_runs(C.byref(self.c), _ptr(c), _ptr(s), _ptr(ln), n)
+        return c, s, ln
+
+
+class SampleSpec:
+    def __init__(self, seed: int, k: int, class_rate=(0.01,), class_prob=(1.0,),
+                 block_len=1 << 20, present_frac=1.0, random_frac=0.0, intro=(), intro_rate=0.0001):
+        rates = list(class_rate) + [0.0] * (4 - len(class_rate))
+        probs = list(class_prob) + [0.0] * (4 - len(class_prob))
+        self._ic = np.array([i[0] for i in intro] or [0], dtype=np.uint32)
+        self._is = np.array([i[1] for i in intro] or [0], dtype=np.uint64)
+        self._il = np.array([i[2] for i in intro] or [0], dtype=np.uint64)
+        self.k = k
+        self.c = SynthSampleSpec(seed, k, len(class_rate), block_len, (C.c_double * 4)(*rates),
+                                 (C.c_double * 4)(*probs), present_frac, random_frac, len(intro), 0,
+                                 self._ic.ctypes.data_as(u32p), self._is.ctypes.data_as(u64p),
+                                 self._il.ctypes.data_as(u64p), intro_rate)
+
+    def codes_host(self, ref: RefSpec, seq, mask) -> np.ndarray:
+        n = C.c_uint64()
+        _check(_t_sample_codes(C.byref(ref.c), C.byref(self.c), _ptr(seq), _ptr(mask), 0, None, 0,
+                               C.byref(n)), tools=True)
+        out = np.zeros(max(n.value, 1), dtype=np.uint64)
+        _check(_t_sample_codes(C.byref(ref.c), C.byref(self.c), _ptr(seq), _ptr(mask), 0, _ptr(out),
+                               n.value, C.byref(n)), tools=True)
+        return out[: n.value]
+
+    def codes_device_bound(self, ref: RefSpec, seq_dev, mask_dev) -> int:
+        n = C.c_uint64()
+        _check(_t_sample_codes(C.byref(ref.c), C.byref(self.c), _ptr(seq_dev), _ptr(mask_dev), 1, None,
+                               0, C.byref(n)), tools=True)
+        return n.value
+
+    def codes_device(self, ref: RefSpec, seq_dev, mask_dev, out_dev, cap: int) -> int:
+        n = C.c_uint64()
+        _check(_t_sample_codes(C.byref(ref.c), C.byref(self.c), _ptr(seq_dev), _ptr(mask_dev), 1,
+                               _ptr(out_dev), cap, C.byref(n)), tools=True)
+        return n.value
+
+
+def kmc_write(prefix: str, codes, n: int, k: int, p: int, sig_len: int = 9, n_bins: int = 512,
+              counter_size: int = 1, version: int = 0x200, min_count: int = 2, max_count: int = 255,
+              count_seed: int = 7, on_device: bool = False) -> int:
+    spec = KmcSpec(k, p, sig_len, n_bins, counter_size, version, min_count, max_count, count_seed)
+    out = C.c_uint64()
+    _check(_t_kmc_write(str(prefix).encode(), C.byref(spec), _ptr(codes), n, int(on_device),
+                        C.byref(out)), tools=True)
+    return out.value
+
+
+def sort_unique_host(codes: np.ndarray, threads: int = 0) -> np.ndarray:
+    codes = np.ascontiguousarray(codes, dtype=np.uint64)
+    n = _t_sort_unique(_ptr(codes), len(codes), threads)
+    return codes[:n]
+
+
+def random_sector_rate(nbytes: int) -> float:
+    """Random 32-byte sector reads per second over a device buffer of nbytes."""
+    r = C.c_double()
+    _check(_t_sector_rate(nbytes, C.byref(r)), tools=True)
+    return r.value

@@ -1,0 +1,171 @@
+/*
+ * ibs.h -- C-ABI of the B200 fastibs window scan (libibs.so).
+ *
+ * Plain C types only: pointers, sizes and the structs below. The library
+ * owns every device allocation and all pinned staging; the caller owns the
+ * host buffers it passes and the output rows. A handle is used by one host
+ * thread at a time. Every call returns an ibs_status; on failure
+ * ibs_last_error() (thread-local) holds a one-line message. There is no CPU
+ * fallback: without a usable CUDA device the calls return IBS_ERR_CUDA.
+ *
+ * What it replaces in the reference (GPU-IBS), paths relative to its root:
+ *   - the device index (KmcRaIndex load src/gpu/KmcRaIndex.hpp:124-135 +
+ *     DeviceKmerIndex upload src/gpu/DeviceKmerIndex.cu:72-142)  -> ibs_open
+ *   - the streamed encode+probe engine and its statistics consumer
+ *     (EncodeProbeEngine::submit/wait src/gpu/EncodeProbe.cu:941-1022,
+ *     :1144-1154; encodeProbeKernel :152-171; BitStats::run
+ *     src/gpu/EncodeProbeCore.hpp:338-370 via processReferenceGpu
+ *     src/KmerDatabase.hpp:1497-1530)                          -> ibs_scan*
+ *   - the panel engine (encodeProbeMultiKernel src/gpu/EncodeProbe.cu:175-193,
+ *     KmerPanel::scanRoundGpu src/KmerPanel.hpp:400-439)       -> ibs_scan_panel
+ *   - the reference's exceptions "CUDA error in <what>: ..."
+ *     (src/gpu/EncodeProbe.cu:15-20)                           -> ibs_status
+ */
+#ifndef IBS_H
+#define IBS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IBS_ABI_VERSION 1
+
+typedef enum ibs_status {
+    IBS_OK = 0,
+    IBS_ERR_ARG = 1,         /* bad argument (null pointer, W <= k, cap too small) */
+    IBS_ERR_IO = 2,          /* file missing / unreadable / short */
+    IBS_ERR_FORMAT = 3,      /* not a KMC 3 database this library reads */
+    IBS_ERR_CUDA = 4,        /* CUDA runtime error or no usable device */
+    IBS_ERR_NOMEM = 5,       /* device or pinned host allocation failed */
+    IBS_ERR_UNSUPPORTED = 6, /* k > 32, Quake-mode counters, ... */
+    IBS_ERR_CAPACITY = 7,    /* request beyond a fixed capacity */
+    IBS_ERR_TIMEOUT = 8,     /* a bounded device wait gave up */
+    IBS_ERR_STATE = 9        /* handle in the wrong state for the call */
+} ibs_status;
+
+/* One output row: the reference's Window (src/Window.hpp:7-16) minus its id
+ * string, which the caller keeps per contig. */
+typedef struct ibs_window {
+    int32_t start, end, total_kmers, observed_kmers, variations, kmer_distance;
+} ibs_window;
+
+typedef struct ibs_table ibs_table;         /* one sample's device-resident k-mer table */
+typedef struct ibs_reference ibs_reference; /* a device-resident 2-bit packed reference */
+
+/* Table build options; zero-initialise for the defaults. */
+typedef struct ibs_table_opts {
+    int device;             /* CUDA device ordinal (default 0) */
+    double keys_per_bucket; /* target mean keys per 32 B bucket (0 = default 4.0) */
+    uint32_t force_format;  /* 0 = automatic, 1 = B8x32, 2 = B6x40 */
+    uint32_t reserved[5];
+} ibs_table_opts;
+
+typedef struct ibs_table_info {
+    uint32_t k, format, fp_bits, reserved0;
+    uint64_t n_keys;         /* k-mers in the table */
+    uint64_t n_buckets;      /* 32-byte buckets */
+    uint64_t stash_keys;     /* keys that overflowed their bucket */
+    uint64_t stash_buckets;
+    uint64_t device_bytes;   /* bytes resident on the device */
+    double build_seconds;    /* decode + upload + build wall time */
+} ibs_table_info;
+
+/* ---- tables -------------------------------------------------------------
+ * ibs_open: decode <prefix>.kmc_pre / <prefix>.kmc_suf (KMC 3 formats 0 and
+ * 0x200, k <= 32) once and build the device table. Counters are ignored, as
+ * the reference's KmcRaIndex strips them (src/gpu/KmcRaIndex.hpp:596-708).
+ * Replaces KmcRaIndex(prefix) + DeviceKmerIndex(host, dev, shard). */
+ibs_status ibs_open(const char *kmc_prefix, const ibs_table_opts *opts, ibs_table **out);
+
+/* Build a table from canonical codes (host or device pointer; duplicates
+ * allowed). The k-mer set a KMC database lists, without the file. */
+ibs_status ibs_table_from_codes(const uint64_t *codes, uint64_t n, uint32_t k,
+                                int codes_on_device, const ibs_table_opts *opts,
+                                ibs_table **out);
+
+ibs_status ibs_table_info_get(const ibs_table *t, ibs_table_info *info);
+
+/* Membership of n canonical codes (host arrays), one byte per code.
+ * The probe of KmcRaIndex::probe (src/gpu/KmcRaIndex.hpp:227-235). */
+ibs_status ibs_probe(ibs_table *t, const uint64_t *codes, uint64_t n, uint8_t *hits);
+
+void ibs_close(ibs_table *t);
+
+/* ---- references ----------------------------------------------------------
+ * Packed layout (the reference's packWindow convention,
+ * src/gpu/EncodeProbeCore.hpp:157-186, applied per contig): contig c starts
+ * at packed base offset B_c = sum_{c'<c} roundup(len_c', 64); base i of
+ * contig c sits at bits 2((B_c+i)%32) of u64 seq word (B_c+i)/32 (A=0 C=1
+ * G=2 T=3) and bit (B_c+i)%64 of u64 mask word (B_c+i)/64 is set when the
+ * byte is not one of ACGTacgt. ibs_packed_words() gives both array lengths
+ * (including one zero word of tail padding each). */
+void ibs_packed_words(const uint64_t *lens, uint32_t n_contigs, uint64_t *seq_words,
+                      uint64_t *mask_words);
+
+/* Pack ASCII contigs into that layout on the host (the reference's
+ * packWindow, src/gpu/EncodeProbeCore.hpp:157-186). */
+ibs_status ibs_pack_ascii(const char *const *seqs, const uint64_t *lens, uint32_t n_contigs,
+                          uint64_t *seq2bit, uint64_t *nmask, int threads);
+
+/* Upload a packed reference (host pointers) and keep it on the device. */
+ibs_status ibs_reference_create(const uint64_t *seq2bit, const uint64_t *nmask,
+                                const uint64_t *lens, uint32_t n_contigs, int device,
+                                ibs_reference **out);
+/* The same from device pointers (copied device-to-device). */
+ibs_status ibs_reference_create_device(const uint64_t *seq2bit_dev, const uint64_t *nmask_dev,
+                                       const uint64_t *lens, uint32_t n_contigs, int device,
+                                       ibs_reference **out);
+void ibs_reference_free(ibs_reference *r);
+
+/* Windows chunkSequences cuts (src/Utils.hpp:296-327): sum over contigs of
+ * ceil(len / (W - k)). 0 when W <= k. */
+uint64_t ibs_window_count(const uint64_t *lens, uint32_t n_contigs, uint32_t W, uint32_t k);
+
+/* Window starts/ends in output order (host arrays of ibs_window_count). */
+ibs_status ibs_window_bounds(const uint64_t *lens, uint32_t n_contigs, uint32_t W, uint32_t k,
+                             ibs_window *rows, uint64_t cap);
+
+/* ---- scans ---------------------------------------------------------------
+ * Every window of every contig of `ref` against table `t`: rows in contig,
+ * then window order, bit-identical to the reference CPU path's Window
+ * records. W must exceed k (the reference throws, src/Utils.hpp:302-304).
+ *
+ * ibs_scan: rows to host memory; synchronous. */
+ibs_status ibs_scan(ibs_table *t, ibs_reference *ref, uint32_t W, ibs_window *rows,
+                    uint64_t cap);
+
+/* ibs_scan_async: rows to device memory `rows_dev`, enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream); returns once enqueued.
+ * Scratch is allocated (once per reference and W) before the launch. */
+ibs_status ibs_scan_async(ibs_table *t, ibs_reference *ref, uint32_t W, ibs_window *rows_dev,
+                          uint64_t cap, void *stream);
+
+/* ibs_scan_packed: the end-to-end call over HOST buffers in the packed
+ * layout: uploads the reference in pieces overlapped with the scan and
+ * returns the rows in host memory. */
+ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit, const uint64_t *nmask,
+                           const uint64_t *lens, uint32_t n_contigs, uint32_t W,
+                           ibs_window *rows, uint64_t cap);
+
+/* Panel: one pass over `ref` against n tables (all of the same k); rows are
+ * table-major: rows[i * n_windows + w]. Identical to n single scans
+ * (KmerPanel::processReference, src/KmerPanel.hpp:63-234). */
+ibs_status ibs_scan_panel(ibs_table *const *tables, uint32_t n_tables, ibs_reference *ref,
+                          uint32_t W, ibs_window *rows, uint64_t cap);
+
+/* Last error message of this thread ("" when none). */
+const char *ibs_last_error(void);
+
+/* Device count visible to the library (cudaGetDeviceCount; 0 on error). */
+int ibs_device_count(void);
+
+/* Kernel launches made by this process's library calls so far. */
+uint64_t ibs_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IBS_H */

@@ -1,0 +1,46 @@
+"""The associative window-statistics fold the scan kernel uses
+(gpu-ibs_b200/csrc/ibs_core.cuh, compiled for the host) equals the
+reference's sequential loop for every split of a window into segments."""
+import ctypes
+
+import numpy as np
+import pytest
+from hypothesis import given, settings
+from hypothesis import strategies as st
+
+import oracle as orc
+
+
+def fold(shim, valid, hit, cuts, k):
+    valid = np.ascontiguousarray(valid, np.uint8)
+    hit = np.ascontiguousarray(hit, np.uint8)
+    cuts = np.ascontiguousarray(sorted(cuts), np.uint64)
+    out = (ctypes.c_int32 * 4)()
+    shim.fold_segments(valid.ctypes.data_as(ctypes.c_void_p), hit.ctypes.data_as(ctypes.c_void_p),
+                       ctypes.c_uint64(len(valid)), cuts.ctypes.data_as(ctypes.c_void_p),
+                       ctypes.c_uint64(len(cuts)), ctypes.c_int(k), out)
+    return tuple(out)
+
+
+def sequential(valid, hit, k):
+    h = [int(x) for v, x in zip(valid, hit) if v]  # invalid positions are skipped
+    r = orc.stats_from_hits(h, k)
+    return (int(r["total_kmers"]), int(r["observed_kmers"]), int(r["variations"]),
+            int(r["kmer_distance"]))
+
+
+@settings(max_examples=400, deadline=None)
+@given(st.data())
+def test_fold_equals_sequential_loop(native_shim, data):
+    n = data.draw(st.integers(0, 300))
+    k = data.draw(st.sampled_from([4, 15, 25, 31, 32]))
+    valid = data.draw(st.lists(st.booleans(), min_size=n, max_size=n))
+    hit = [v and data.draw(st.booleans()) for v in valid]
+    cuts = data.draw(st.lists(st.integers(0, n), max_size=12))
+    assert fold(native_shim, valid, hit, cuts, k) == sequential(valid, hit, k)
+
+
+@pytest.mark.parametrize("bits", [2, 8, 14, 20])
+def test_table_hash_is_a_bijection(native_shim, bits):
+    native_shim.hash_collisions.restype = ctypes.c_uint64
+    assert native_shim.hash_collisions(ctypes.c_uint32(bits)) == 0
