@@ -113,6 +113,8 @@ _ibs_scan_packed = _sig(_lib, "ibs_scan_packed", C.c_int,
                         [vp, vp, vp, vp, C.c_uint32, C.c_uint32, vp, C.c_uint64])
 _ibs_scan_panel = _sig(_lib, "ibs_scan_panel", C.c_int,
                        [C.POINTER(vp), C.c_uint32, vp, C.c_uint32, vp, C.c_uint64])
+_ibs_scan_noalloc = _sig(_lib, "ibs_scan_noalloc", C.c_int,
+                         [vp, vp, vp, vp, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp])
 _ibs_last_error = _sig(_lib, "ibs_last_error", C.c_char_p, [])
 _ibs_device_count = _sig(_lib, "ibs_device_count", C.c_int, [])
 _ibs_launch_count = _sig(_lib, "ibs_launch_count", C.c_uint64, [])
@@ -295,6 +297,15 @@ def scan_packed(table: Table, seq2bit, nmask, lens, W: int, rows=None) -> np.nda
     _check(_ibs_scan_packed(table.handle, _ptr(seq2bit), _ptr(nmask), _ptr(lens), len(lens), W,
                             _ptr(rows), n))
     return rows[:n] if isinstance(rows, np.ndarray) else rows
+
+
+def scan_noalloc(table: Table, seq2bit_dev, nmask_dev, lens, W: int, rows_dev, cap: int,
+                 stream: int = 0):
+    """ibs_scan_noalloc: the scan with its scratch in the library's fixed
+    device array (no allocation); every pointer but lens is device memory."""
+    lens = np.ascontiguousarray(lens, dtype=np.uint64)
+    _check(_ibs_scan_noalloc(table.handle, _ptr(seq2bit_dev), _ptr(nmask_dev), _ptr(lens), len(lens), W,
+                             _ptr(rows_dev), cap, stream))
 
 
 def scan_panel(tables: list[Table], ref: Reference, W: int) -> np.ndarray:

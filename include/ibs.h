@@ -156,6 +156,30 @@ ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit, const uint64_t
 ibs_status ibs_scan_panel(ibs_table *const *tables, uint32_t n_tables, ibs_reference *ref,
                           uint32_t W, ibs_window *rows, uint64_t cap);
 
+/* ibs_scan_noalloc: the scan of ibs_scan_async without any memory
+ * allocation. No counterpart in the reference. It is for callers that cannot
+ * allocate device memory while they scan: a serving process that gave all
+ * free device memory to its own pool, a host that keeps its allocations
+ * fixed after start-up, or a latency-bound loop in which cudaMalloc (which
+ * may synchronize the device) is not acceptable.
+ *
+ * The caller passes the table, the packed reference in device memory
+ * (seq2bit_dev / nmask_dev in the packed layout above), the contig lengths
+ * in host memory and the row buffer in device memory; the work is enqueued
+ * on `stream` and the call returns. Its scratch (per-contig window table and
+ * one 32-byte summary per 4096-position span) is a fixed device array of
+ * IBS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * the process exits -- enough for about 4 Gbp of reference at W = 50 kbp. A
+ * scan that needs more returns IBS_ERR_CAPACITY before touching the device.
+ * All calls on a device share that array: calls whose work overlaps on the
+ * GPU (different streams, or different host threads without ordering) race;
+ * order them on one stream. The first call on a device looks up the array's
+ * device address; make that first call before any stream capture. */
+#define IBS_NOALLOC_SCRATCH_BYTES (32ull << 20)
+ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev, const uint64_t *nmask_dev,
+                            const uint64_t *lens, uint32_t n_contigs, uint32_t W,
+                            ibs_window *rows_dev, uint64_t cap, void *stream);
+
 /* Last error message of this thread ("" when none). */
 const char *ibs_last_error(void);
 
