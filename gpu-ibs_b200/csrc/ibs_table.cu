@@ -700,6 +700,29 @@ extern "C" ibs_status ibs_probe(ibs_table *t, const uint64_t *codes, uint64_t n,
     return IBS_OK;
 }
 
+extern "C" uint64_t ibs_table_bytes_for(uint64_t n_keys, uint32_t k, const ibs_table_opts *opts)
+{
+    if (k == 0 || k > 32)
+        return 0;
+    return choose_geometry(n_keys, k, opts).nBuckets * 32;
+}
+
+extern "C" ibs_status ibs_device_memory(int device, uint64_t *free_bytes, uint64_t *total_bytes)
+{
+    clear_error();
+    ibs_status s = check_device(device);
+    if (s != IBS_OK)
+        return s;
+    DeviceGuard guard(device);
+    size_t f = 0, t = 0;
+    IBS_CUDA(cudaMemGetInfo(&f, &t), "cudaMemGetInfo");
+    if (free_bytes)
+        *free_bytes = f;
+    if (total_bytes)
+        *total_bytes = t;
+    return IBS_OK;
+}
+
 extern "C" void ibs_close(ibs_table *t)
 {
     if (!t)

@@ -94,6 +94,15 @@ ibs_status ibs_probe(ibs_table *t, const uint64_t *codes, uint64_t n, uint8_t *h
 
 void ibs_close(ibs_table *t);
 
+/* Device bytes a table of n_keys k-mers takes (its buckets; the stash of
+ * overflowing keys adds about 1% more at the default load). Plans residency
+ * the way KmerPanel::imageBytesOf sizes a database (src/KmerPanel.hpp:265-280). */
+uint64_t ibs_table_bytes_for(uint64_t n_keys, uint32_t k, const ibs_table_opts *opts);
+
+/* Free and total memory of a device (cudaMemGetInfo), as the reference's
+ * DeviceKmerIndex::freeMemory (src/gpu/DeviceKmerIndex.cu:354-367). */
+ibs_status ibs_device_memory(int device, uint64_t *free_bytes, uint64_t *total_bytes);
+
 /* ---- references ----------------------------------------------------------
  * Packed layout (the reference's packWindow convention,
  * src/gpu/EncodeProbeCore.hpp:157-186, applied per contig): contig c starts
