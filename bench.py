@@ -95,6 +95,16 @@ def sample_for_rank(w, rank: int):
                       present_frac=float(c.present_frac), random_frac=float(c.random_frac))
 
 
+def max_over_ranks(value: float, dist=None, device=None) -> float:
+    """The largest value over all ranks (every rank calls it, in the same order)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -327,11 +337,8 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
         ev1.synchronize()
     torch.cuda.synchronize()
     launches = ib.launch_count() - launches0
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     ms_step = ms / args.steps
     total_probes = probes_per_scan * world
@@ -350,11 +357,7 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         ib.scan_packed(table, hseq.data_ptr(), hmask.data_ptr(), lens, W, hrows.data_ptr())
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, dist, "cuda")
     e2e_rows = hrows[: n_win * 6].numpy().view(ib.WINDOW_DTYPE)
     assert np.array_equal(e2e_rows, rows), "e2e rows differ from the resident scan's"
     h2d = (sw + mw) * 8 + n_win * 32 + (n_win + 1) * 4
@@ -395,6 +398,223 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
     if cpu is not None:
         out["cpu_baseline"] = cpu
     table.close()
+    ref.free()
+    return out
+
+
+def panel_arm(args, rank: int):
+    """Batched panel: 16 samples of uneven size against one reference, one
+    joint table, the scan replayed as a CUDA graph; compared with the plain
+    path (one table and one scan launch per sample) on the same GPU, and
+    every sample's panel rows checked against its single-sample rows."""
+    import torch
+    import ibs_b200 as ib
+    from ibs_b200 import configs
+    w = configs.panel_4gbp(n_samples=args.panel_samples, scale=args.panel_scale)
+    k, W = w.k, w.window
+    lens = w.ref.lens
+    runs = w.ref.n_runs()
+    positions = valid_positions(lens, k, runs)
+    sw, mw = w.ref.packed_words()
+    n_win = ib.window_count(lens, W, k)
+    dseq = torch.empty(sw, dtype=torch.int64, device="cuda")
+    dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
+    w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
+    ref = ib.Reference(dseq.data_ptr(), dmask.data_ptr(), lens, on_device=True)
+
+    def sample_codes(i):
+        smp = w.samples[i]
+        bound = smp.codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
+        buf = torch.empty(bound, dtype=torch.int64, device="cuda")
+        n = smp.codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), buf.data_ptr(), bound)
+        return buf, n
+
+    # the union's size from a 1/64 hash sample of every sample's k-mers
+    t0 = time.time()
+    sizes, sampled = [], []
+    for i in range(len(w.samples)):
+        buf, n = sample_codes(i)
+        sizes.append(n)
+        v = buf[:n]
+        sel = v[((v * 0x9E3779B97F4A7C15) >> 58) == 0]
+        sampled.append(torch.unique(sel))
+        del buf, v, sel
+        torch.cuda.empty_cache()
+    union_est = int(torch.unique(torch.cat(sampled)).numel() * 64 * 1.02) + (1 << 20)
+    del sampled
+    # plain path: one table and one scan launch per sample (scan time only)
+    stream = torch.cuda.Stream()
+    rows_single = torch.empty(max(n_win, 1) * 6, dtype=torch.int32, device="cuda")
+    singles, plain_ms = [], 0.0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i in range(len(w.samples)):
+        buf, n = sample_codes(i)
+        t = ib.Table.from_codes(buf.data_ptr(), n, k, on_device=True)
+        del buf
+        torch.cuda.empty_cache()
+        ib.scan_async(t, ref, W, rows_single.data_ptr(), n_win, stream.cuda_stream)  # plan + warm
+        stream.synchronize()
+        e0.record(stream)
+        ib.scan_async(t, ref, W, rows_single.data_ptr(), n_win, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        singles.append(rows_single[: n_win * 6].cpu().numpy().view(ib.WINDOW_DTYPE).copy())
+        t.close()
+    # batched: one joint table, graph-replayed scans
+    pt = ib.PanelTable(k, union_est)
+    for i in range(len(w.samples)):
+        buf, n = sample_codes(i)
+        pt.add_codes(buf.data_ptr(), n, on_device=True)
+        del buf
+        torch.cuda.empty_cache()
+    info, ns = pt.info()
+    t_build = time.time() - t0
+    rows = torch.empty(max(n_win * ns, 1) * 6, dtype=torch.int32, device="cuda")
+    for _ in range(args.warmup):
+        pt.scan_async(ref, W, rows.data_ptr(), n_win * ns, stream.cuda_stream)
+    stream.synchronize()
+    launches0 = ib.launch_count()
+    e0.record(stream)
+    for _ in range(args.steps):
+        pt.scan_async(ref, W, rows.data_ptr(), n_win * ns, stream.cuda_stream)
+    e1.record(stream)
+    e1.synchronize()
+    panel_ms = e0.elapsed_time(e1) / args.steps
+    launches = ib.launch_count() - launches0
+    got = rows[: n_win * ns * 6].cpu().numpy().view(ib.WINDOW_DTYPE).reshape(ns, n_win)
+    mismatched = [i for i in range(ns) if not np.array_equal(got[i], singles[i])]
+    assert not mismatched, f"panel rows differ from single-sample rows for samples {mismatched}"
+    probes = positions * ns
+    out = {"workload": w.name, "samples": ns, "sample_kmers": sizes, "k": k, "window": W,
+           "reference_bp": int(sum(map(int, lens))), "positions": int(positions),
+           "union_keys_estimate": union_est, "joint_table_gb": info.device_bytes / 1e9,
+           "build_s": t_build,
+           "batched_probes_per_s": probes / (panel_ms * 1e-3), "batched_ms_per_scan": panel_ms,
+           "plain_probes_per_s": probes / (plain_ms * 1e-3), "plain_ms_all_samples": plain_ms,
+           "speedup_vs_plain": plain_ms / panel_ms, "graph_launches_per_scan": launches / args.steps,
+           "rows_equal_single_sample": True}
+    pt.close()
+    ref.free()
+    return out
+
+
+def served_arm(args, rank: int):
+    """Served scan stream over the 2 Gbp reference and a pool of resident
+    samples: Poisson arrivals, regions log-uniform from 1 Mbp to a whole
+    contig; the batching server against the same server taking one request
+    per launch. Every result is checked against the sample's full-scan rows."""
+    import torch
+    import ibs_b200 as ib
+    from ibs_b200 import configs
+    w = configs.plain_2gbp(scale=args.serve_scale)
+    k, W = w.k, w.window
+    lens = w.ref.lens
+    sw, mw = w.ref.packed_words()
+    dseq = torch.empty(sw, dtype=torch.int64, device="cuda")
+    dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
+    w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
+    ref = ib.Reference(dseq.data_ptr(), dmask.data_ptr(), lens, on_device=True)
+    rng = np.random.default_rng(404)
+    n_samples = args.serve_samples
+    base = w.samples[0].c
+    specs = [ib.SampleSpec(seed=4000 + i, k=k, class_rate=tuple(base.class_rate)[:4],
+                           class_prob=tuple(base.class_prob)[:4], block_len=int(base.block_len),
+                           present_frac=float(np.exp(rng.uniform(np.log(0.05), np.log(0.5)))),
+                           random_frac=0.10) for i in range(n_samples)]
+    full = []
+    win_start = np.concatenate([[0], np.cumsum([ib.window_count(lens[c:c + 1], W, k) for c in range(len(lens))])])
+    t0 = time.time()
+    n_keys = []
+
+    def codes(sp):
+        bound = sp.codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
+        buf = torch.empty(bound, dtype=torch.int64, device="cuda")
+        n = sp.codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), buf.data_ptr(), bound)
+        return buf, n
+
+    rows_dev = torch.empty(int(win_start[-1]) * 6, dtype=torch.int32, device="cuda")
+    for sp in specs:  # every sample's full-scan rows, to check the served results
+        buf, n = codes(sp)
+        n_keys.append(n)
+        t = ib.Table.from_codes(buf.data_ptr(), n, k, on_device=True)
+        ib.scan_async(t, ref, W, rows_dev.data_ptr(), int(win_start[-1]), 0)
+        torch.cuda.synchronize()
+        full.append(rows_dev.cpu().numpy().view(ib.WINDOW_DTYPE).copy())
+        t.close()
+        del buf
+        torch.cuda.empty_cache()
+    del rows_dev
+    torch.cuda.empty_cache()
+    setup_s = time.time() - t0
+
+    def server(mode):
+        srv = ib.Server(ref, W, k, memory_budget=args.serve_budget_gb << 30,
+                        one_request_per_launch=(mode == "serial"))
+        for sp in specs:
+            buf, n = codes(sp)
+            srv.add_codes(buf.data_ptr(), n, on_device=True)
+            del buf
+            torch.cuda.empty_cache()
+        return srv
+    # the request stream
+    reqs = []
+    step = W - k
+    for _ in range(args.serve_requests):
+        s_ = int(rng.integers(0, n_samples))
+        c = int(rng.integers(0, len(lens)))
+        L = int(lens[c])
+        ln = int(np.exp(rng.uniform(np.log(1e6), np.log(max(L, 1e6 + 1)))))
+        nw_c = int(win_start[c + 1] - win_start[c])
+        first = int(rng.integers(0, max(1, (L - ln) // step + 1)))
+        first = min(first, nw_c - 1)
+        cnt = max(1, min(nw_c - first, ln // step))
+        reqs.append((s_, c, first, cnt))
+    gaps = rng.exponential(1.0 / args.serve_rate, len(reqs))
+
+    def run(srv, paced: bool):
+        done = []
+        stats0 = srv.stats()
+        t_start = srv.now()
+        if paced:
+            t_next = time.perf_counter()
+            for req, g in zip(reqs, gaps):
+                t_next += g
+                while time.perf_counter() < t_next:
+                    done += srv.poll(256, timeout_ms=0)
+                    time.sleep(0.0002)
+                srv.submit(*req)
+        else:
+            for req in reqs:
+                srv.submit(*req)
+        while len(done) < len(reqs):
+            done += srv.poll(256, timeout_ms=1000)
+        makespan = srv.now() - t_start
+        st = srv.stats()
+        lat = np.array([r["done_time"] - r["submit_time"] for r in done])
+        for r in done:
+            a = int(win_start[r["contig"]] + r["first_window"])
+            assert np.array_equal(r["rows"], full[r["sample"]][a:a + int(r["n_windows"])]), "served rows differ"
+        probes = st["probes"] - stats0["probes"]
+        return {"requests": len(done), "probes": int(probes), "makespan_s": makespan,
+                "probes_per_s": probes / makespan,
+                "device_probes_per_s": probes / max(1e-9, st["busy_seconds"] - stats0["busy_seconds"]),
+                "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                "latency_max_s": float(lat.max()), "launches": int(st["launches"] - stats0["launches"]),
+                "reloads": int(st["reloads"] - stats0["reloads"]),
+                "reload_bytes": int(st["reload_bytes"] - stats0["reload_bytes"])}
+
+    out = {"workload": f"plain_2gbp reference x {n_samples} resident samples",
+           "sample_kmers": n_keys, "requests": len(reqs), "arrival_rate_per_s": args.serve_rate,
+           "setup_s": setup_s, "budget_gb": args.serve_budget_gb}
+    for mode in ("batched", "serial"):
+        srv = server(mode)
+        out[f"{mode}_poisson"] = run(srv, True)
+        out[f"{mode}_saturated"] = run(srv, False)
+        srv.close()
+    out["saturated_speedup_vs_one_request_per_launch"] = (out["batched_saturated"]["probes_per_s"] /
+                                                         out["serial_saturated"]["probes_per_s"])
+    out["rows_equal_full_scan"] = True
     ref.free()
     return out
 
@@ -455,6 +675,17 @@ def main():
     ap.add_argument("--cpu-slice", type=int, default=50_000_000, help="bases per CPU-baseline slice")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--panel", action="store_true", help="also measure the 16-sample batched panel")
+    ap.add_argument("--panel-only", action="store_true")
+    ap.add_argument("--panel-samples", type=int, default=16)
+    ap.add_argument("--panel-scale", type=float, default=1.0)
+    ap.add_argument("--serve", action="store_true", help="also measure the served request stream")
+    ap.add_argument("--serve-only", action="store_true")
+    ap.add_argument("--serve-samples", type=int, default=16)
+    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-rate", type=float, default=50.0)
+    ap.add_argument("--serve-scale", type=float, default=1.0)
+    ap.add_argument("--serve-budget-gb", type=int, default=120)
     args = ap.parse_args()
 
     from ibs_b200 import configs
@@ -479,7 +710,25 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
+    if args.serve_only:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"served": served_arm(args, rank)}), flush=True)
+        return 0
+    if args.panel_only:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"panel": panel_arm(args, rank)}), flush=True)
+        return 0
     out = gpu_arm(args, w, rank, world, local)
+    if args.panel and world == 1:
+        import torch
+        torch.cuda.empty_cache()
+        out["extra"]["panel"] = panel_arm(args, rank)
+    if args.serve and world == 1:
+        import torch
+        torch.cuda.empty_cache()
+        out["extra"]["served"] = served_arm(args, rank)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

@@ -78,7 +78,7 @@ IBS_HD uint64_t mulhi64(uint64_t a, uint64_t b)
 //   linear probing over buckets, EMPTY = ~0 (never a canonical code: the
 //   all-T k-mer's reverse complement, all-A, is smaller).
 // ---------------------------------------------------------------------------
-enum : uint32_t { FMT_B8X32 = 1, FMT_B6X40 = 2 };
+enum : uint32_t { FMT_B8X32 = 1, FMT_B6X40 = 2, FMT_PANEL = 3, FMT_MZ8 = 4, FMT_AUTO_HASH = 5 };
 constexpr uint32_t B8_EMPTY = 0xffffffffu;
 constexpr uint32_t B8_OVERFLOW = 0xfffffffeu;
 constexpr uint64_t STASH_EMPTY = ~0ull;

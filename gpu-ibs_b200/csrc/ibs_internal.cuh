@@ -11,6 +11,7 @@
 
 #include "../../include/ibs.h"
 #include "ibs_core.cuh"
+#include "mz_core.cuh"
 
 namespace ibs {
 
@@ -30,6 +31,11 @@ ibs_status cuda_fail(cudaError_t e, const char *what);
             return ::ibs::cuda_fail(e_, what);                \
     } while (0)
 
+// Device count check shared by the entry points.
+ibs_status check_device_ordinal(int dev);
+// Decodes a KMC 3 database into canonical codes in device memory (caller frees).
+ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodes, uint64_t *n, uint32_t *k);
+
 #define IBS_LAUNCHED() (::ibs::launch_counter().fetch_add(1, std::memory_order_relaxed))
 
 // RAII guard that makes `dev` current and restores the previous device.
@@ -48,6 +54,9 @@ struct DeviceGuard {
             cudaSetDevice(prev);
     }
 };
+
+// ---- tuning -----------------------------------------------------------------
+const ibs_tuning &tuning();
 
 // ---- device table view ----------------------------------------------------
 struct TableView {
@@ -101,6 +110,14 @@ __device__ __forceinline__ uint32_t bucket_match(const uint4 &v0, const uint4 &v
 template <uint32_t FMT>
 __device__ __forceinline__ bool table_lookup(const TableView &t, uint64_t code)
 {
+    if (FMT == FMT_MZ8) {
+        uint64_t r;
+        uint32_t slot;
+        mz::locate(code, t.g, r, slot);
+        const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);
+        const uint32_t m = bucket_match<FMT_B8X32>(v0, v1, slot);
+        return m == 1u || (m == 2u && stash_lookup(t, code));
+    }
     const uint64_t h = perm_hash(code, t.g.bits);
     const uint64_t r = bucket_of(h, t.g);
     const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);

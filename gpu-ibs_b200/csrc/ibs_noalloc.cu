@@ -280,6 +280,11 @@ extern "C" ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev
         set_error("ibs_scan_noalloc: bad argument");
         return IBS_ERR_ARG;
     }
+    if (t->geom.format != FMT_B8X32 && t->geom.format != FMT_B6X40) {
+        set_error("ibs_scan_noalloc: scans tables of the hash-bucket formats (1, 2); build the table "
+                  "with force_format 1, 2 or 5");
+        return IBS_ERR_UNSUPPORTED;
+    }
     const uint32_t k = t->geom.k;
     if (W <= k) {
         set_error("window size " + std::to_string(W) + " must be larger than k (" +

@@ -1,0 +1,733 @@
+// Panel scan: one reference pass against up to 16 samples through ONE joint
+// table whose slots carry a sample-membership mask.
+//
+// The reference's panel mode encodes each batch once and probes every
+// resident database separately (encodeProbeMultiKernel + MultiBsProbe,
+// src/gpu/EncodeProbe.cu:82-108, :175-193; MAX_DBS = 16,
+// src/gpu/EncodeProbeCore.hpp:291), so a position costs one index search
+// per sample. Here the samples' k-mer sets are merged into one table: a
+// position costs one random 32-byte bucket load whatever the panel size,
+// and the mask in the matching slot says which samples hold the k-mer.
+// Every sample's rows are still exactly its single-sample rows.
+//
+// Bucket format P5x48 (one 32-byte sector): u32 fingerprints of slots 0-4
+// (words 0-4), u16 sample masks of slots 0-4 (bytes 20-29), slot count
+// (byte 30), flags (byte 31, bit 0 = some key of this bucket is in the
+// stash). The fingerprint is the same quotient of the bijective k-mer hash
+// as in the single-sample table, so it needs nBuckets >= 2^(2k-32).
+// Stash: {code, mask} pairs, two per 32-byte bucket, linear probing.
+#include "ibs_internal.cuh"
+#include "scan_device.cuh"
+
+#include <chrono>
+#include <cstring>
+#include <memory>
+
+namespace ibs {
+namespace panel {
+
+constexpr uint32_t kMaxSamples = IBS_PANEL_MAX_SAMPLES;
+constexpr uint32_t kSlots = 5;
+constexpr uint32_t kSpanLen = 8192;
+constexpr int kNB = 4;
+constexpr uint64_t kStashEmpty = ~0ull;
+
+struct View {
+    TableGeom g;
+    const uint4 *buckets;
+    const ulonglong2 *stash; // {code, mask}
+    uint64_t stashBuckets;   // power of two; two entries each
+};
+
+__device__ __forceinline__ uint32_t stash_mask(const View &t, uint64_t code)
+{
+    uint64_t b = stash_home(code, t.stashBuckets);
+    for (uint64_t i = 0; i < t.stashBuckets; ++i) {
+        const ulonglong2 e0 = __ldg(t.stash + 2 * b), e1 = __ldg(t.stash + 2 * b + 1);
+        if (e0.x == code)
+            return (uint32_t)e0.y;
+        if (e1.x == code)
+            return (uint32_t)e1.y;
+        if (e0.x == kStashEmpty || e1.x == kStashEmpty)
+            return 0;
+        b = (b + 1) & (t.stashBuckets - 1);
+    }
+    return 0;
+}
+
+// Sample mask of a k-mer given its bucket halves and fingerprint; bit 31
+// set = look in the stash.
+__device__ __forceinline__ uint32_t bucket_mask(const uint4 &v0, const uint4 &v1, uint32_t fp)
+{
+    const uint32_t cnt = (v1.w >> 16) & 0xff;
+    uint32_t m = 0;
+    m |= (0 < cnt && v0.x == fp) ? (v1.y & 0xffff) : 0u;
+    m |= (1 < cnt && v0.y == fp) ? (v1.y >> 16) : 0u;
+    m |= (2 < cnt && v0.z == fp) ? (v1.z & 0xffff) : 0u;
+    m |= (3 < cnt && v0.w == fp) ? (v1.z >> 16) : 0u;
+    m |= (4 < cnt && v1.x == fp) ? (v1.w & 0xffff) : 0u;
+    if (!m && ((v1.w >> 24) & 1u))
+        m = 0x80000000u;
+    return m;
+}
+
+__device__ __forceinline__ uint32_t lookup_mask(const View &t, uint64_t code)
+{
+    const uint64_t h = perm_hash(code, t.g.bits);
+    const uint64_t r = bucket_of(h, t.g);
+    const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);
+    uint32_t m = bucket_mask(v0, v1, (uint32_t)fp_of(h, t.g));
+    if (m & 0x80000000u)
+        m = stash_mask(t, code);
+    return m;
+}
+
+// ---- build: phase A finds keys already present and ORs in the sample bit;
+// phase B inserts the rest. Within one sample the keys are unique, so no
+// lookup races with an insert of the same key.
+__global__ void k_find(View t, uint32_t *words, unsigned long long *stashWords, const uint64_t *codes,
+                       uint64_t n, uint32_t bit, uint64_t *pending, unsigned long long *nPending)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t iters = (n + stride - 1) / stride;
+    for (uint64_t it = 0; it < iters; ++it) {
+        const uint64_t i = it * stride + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+        bool miss = false;
+        uint64_t code = 0;
+        if (i < n) {
+            code = codes[i];
+            const uint64_t h = perm_hash(code, t.g.bits);
+            const uint64_t r = bucket_of(h, t.g);
+            const uint32_t fp = (uint32_t)fp_of(h, t.g);
+            uint32_t *w = words + 8 * r;
+            const uint32_t cnt = (w[7] >> 16) & 0xff;
+            int slot = -1;
+            for (uint32_t j = 0; j < cnt && j < kSlots; ++j)
+                if (w[j] == fp)
+                    slot = (int)j;
+            if (slot >= 0) {
+                atomicOr(w + 5 + slot / 2, (1u << bit) << (16 * (slot & 1)));
+            } else if ((w[7] >> 24) & 1u) {
+                // in the stash?
+                uint64_t b = stash_home(code, t.stashBuckets);
+                bool found = false;
+                for (uint64_t s = 0; s < t.stashBuckets && !found; ++s) {
+                    unsigned long long *e = stashWords + 4 * b;
+                    if (e[0] == code) {
+                        atomicOr(e + 1, 1ull << bit);
+                        found = true;
+                    } else if (e[2] == code) {
+                        atomicOr(e + 3, 1ull << bit);
+                        found = true;
+                    } else if (e[0] == kStashEmpty || e[2] == kStashEmpty)
+                        break;
+                    b = (b + 1) & (t.stashBuckets - 1);
+                }
+                miss = !found;
+            } else
+                miss = true;
+        }
+        const uint32_t ballot = __ballot_sync(0xffffffffu, miss);
+        if (!ballot)
+            continue;
+        unsigned long long base = 0;
+        if (lane == 0)
+            base = atomicAdd(nPending, (unsigned long long)__popc(ballot));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (miss)
+            pending[base + __popc(ballot & ((1u << lane) - 1u))] = code;
+    }
+}
+
+__global__ void k_insert(View t, uint32_t *words, unsigned long long *stashWords, const uint64_t *codes,
+                         uint64_t n, uint32_t bit, int *err)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t code = codes[i];
+        const uint64_t h = perm_hash(code, t.g.bits);
+        const uint64_t r = bucket_of(h, t.g);
+        const uint32_t fp = (uint32_t)fp_of(h, t.g);
+        uint32_t *w = words + 8 * r;
+        // claim a slot: bump the count byte while it is below kSlots
+        uint32_t old = w[7], slot = kSlots;
+        for (int tries = 0; tries < 1 << 20; ++tries) {
+            const uint32_t cnt = (old >> 16) & 0xff;
+            if (cnt >= kSlots)
+                break;
+            const uint32_t seen = atomicCAS(w + 7, old, old + (1u << 16));
+            if (seen == old) {
+                slot = cnt;
+                break;
+            }
+            old = seen;
+        }
+        if (slot < kSlots) {
+            w[slot] = fp;
+            atomicOr(w + 5 + slot / 2, (1u << bit) << (16 * (slot & 1)));
+            continue;
+        }
+        atomicOr(w + 7, 1u << 24); // overflow flag
+        uint64_t b = stash_home(code, t.stashBuckets);
+        bool placed = false;
+        for (uint64_t s = 0; s < t.stashBuckets && !placed; ++s) {
+            for (int e = 0; e < 2 && !placed; ++e) {
+                unsigned long long *entry = stashWords + 4 * b + 2 * e;
+                const unsigned long long prev = atomicCAS(entry, kStashEmpty, (unsigned long long)code);
+                if (prev == kStashEmpty || prev == code) {
+                    atomicOr(entry + 1, 1ull << bit);
+                    placed = true;
+                }
+            }
+            b = (b + 1) & (t.stashBuckets - 1);
+        }
+        if (!placed)
+            atomicExch(err, 1);
+    }
+}
+
+// Block statistics of one sample from its valid (V) and hit (H) masks,
+// computed by one lane with bit operations: the gaps between hits are the
+// runs of valid misses, visited one run at a time.
+__device__ __forceinline__ SegStats block_stats_serial(uint32_t V, uint32_t H, int k)
+{
+    SegStats b;
+    b.pad = 0;
+    b.total = __popc(V);
+    b.obs = __popc(H);
+    b.gaps = 0;
+    b.dist = 0;
+    if (H == 0) {
+        b.lead = b.trail = b.total;
+        return b;
+    }
+    const uint32_t first = __ffs(H) - 1;
+    const uint32_t last = 31 - __clz(H);
+    b.lead = __popc(V & ((1u << first) - 1u));
+    b.trail = last == 31 ? 0u : __popc(V >> (last + 1));
+    // valid misses strictly between the first and the last hit
+    const uint64_t inner = ((2ull << last) - 1ull) & ~((2ull << first) - 1ull);
+    uint32_t m = V & ~H & (uint32_t)inner;
+    while (m) {
+        const uint32_t start = __ffs(m) - 1;
+        const uint32_t next = H & ~((2u << start) - 1u); // hits after the run starts (nonzero)
+        const uint32_t j = __ffs(next) - 1;
+        const uint32_t g = __popc(m & ((1u << j) - 1u));
+        b.gaps += 1;
+        b.dist += gap_distance(g, k);
+        m &= ~((1u << j) - 1u);
+    }
+    return b;
+}
+
+template <int NB>
+__global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__restrict__ seq,
+                                                     const uint64_t *__restrict__ mask,
+                                                     const WinDesc *__restrict__ win,
+                                                     const uint32_t *__restrict__ span0, uint32_t nWin,
+                                                     uint64_t nSpans, uint32_t spanLen,
+                                                     uint32_t nSamples,
+                                                     unsigned long long *__restrict__ work,
+                                                     SegStats *__restrict__ out)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t k = t.g.k;
+    const uint64_t kmask = key_mask(2 * k);
+    const uint64_t kbits = (1ull << k) - 1;
+    for (;;) {
+        unsigned long long s = 0;
+        if (lane == 0)
+            s = atomicAdd(work, 1ull);
+        s = __shfl_sync(dev::FULL_MASK, s, 0);
+        if (s >= nSpans)
+            break;
+        uint32_t lo = 0, hi = nWin - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(span0 + mid) <= s)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const uint64_t base = win[lo].base;
+        const uint32_t nPos = win[lo].nPos;
+        const uint32_t p0 = (uint32_t)(s - __ldg(span0 + lo)) * spanLen;
+        const uint32_t p1 = min(p0 + spanLen, nPos);
+        SegStats acc = seg_empty(); // lane j < nSamples: sample j
+        for (uint32_t p = p0; p < p1; p += 32 * NB) {
+            uint4 v0[NB], v1[NB];
+            uint64_t code[NB];
+            uint32_t fp[NB];
+            bool valid[NB];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const uint32_t q = p + 32 * b + lane;
+                const bool inSpan = q < p1;
+                const uint64_t G = base + (inSpan ? q : p0);
+                bool acgt;
+                code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
+                valid[b] = inSpan && acgt;
+                const uint64_t h = perm_hash(code[b], t.g.bits);
+                const uint64_t r = bucket_of(h, t.g);
+                fp[b] = (uint32_t)fp_of(h, t.g);
+                if (valid[b]) {
+                    v0[b] = __ldg(t.buckets + 2 * r);
+                    v1[b] = __ldg(t.buckets + 2 * r + 1);
+                } else {
+                    v0[b] = make_uint4(0, 0, 0, 0);
+                    v1[b] = make_uint4(0, 0, 0, 0);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                uint32_t m = 0;
+                if (valid[b]) {
+                    m = bucket_mask(v0[b], v1[b], fp[b]);
+                    if (m & 0x80000000u)
+                        m = stash_mask(t, code[b]);
+                }
+                const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
+                uint32_t myH = 0;
+                for (uint32_t j = 0; j < nSamples; ++j) {
+                    const uint32_t Hj = __ballot_sync(dev::FULL_MASK, (m >> j) & 1u);
+                    if (lane == j)
+                        myH = Hj;
+                }
+                if (lane < nSamples)
+                    acc = seg_combine(acc, block_stats_serial(V, myH, (int)k), (int)k);
+            }
+        }
+        if (lane < nSamples)
+            out[(uint64_t)lane * nSpans + s] = acc;
+    }
+}
+
+__global__ void k_panel_finalize(const WinDesc *__restrict__ win, const uint32_t *__restrict__ span0,
+                                 uint64_t nWin, uint64_t nSpans, uint32_t nSamples,
+                                 const SegStats *__restrict__ spans, int k, ibs_window *__restrict__ rows)
+{
+    const uint64_t total = nWin * nSamples;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t smp = x / nWin, w = x - smp * nWin;
+        SegStats acc = seg_empty();
+        for (uint32_t s = span0[w]; s < span0[w + 1]; ++s)
+            acc = seg_combine(acc, spans[smp * nSpans + s], k);
+        WindowRow row;
+        row.start = win[w].start;
+        row.end = win[w].end;
+        seg_finish(acc, k, row);
+        ibs_window o;
+        o.start = row.start;
+        o.end = row.end;
+        o.total_kmers = row.total_kmers;
+        o.observed_kmers = row.observed_kmers;
+        o.variations = row.variations;
+        o.kmer_distance = row.kmer_distance;
+        rows[x] = o;
+    }
+}
+
+// Empty stash: every entry {EMPTY, no samples}.
+__global__ void k_stash_init(ulonglong2 *stash, uint64_t entries)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < entries;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        stash[i] = make_ulonglong2(kStashEmpty, 0ull);
+}
+
+__global__ void k_probe_masks(View t, const uint64_t *codes, uint64_t n, uint32_t *masks)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        masks[i] = lookup_mask(t, codes[i]);
+}
+
+int sm_count()
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+int grid_for(uint64_t n)
+{
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 16));
+}
+
+uint64_t next_pow2(uint64_t x)
+{
+    uint64_t p = 1;
+    while (p < x)
+        p <<= 1;
+    return p;
+}
+
+} // namespace panel
+} // namespace ibs
+
+using namespace ibs;
+using namespace ibs::panel;
+
+struct ibs_panel_table {
+    int device = 0;
+    TableGeom geom{};
+    uint4 *buckets = nullptr;
+    ulonglong2 *stash = nullptr;
+    uint64_t stashBuckets = 0;
+    uint32_t nSamples = 0;
+    uint64_t keysAdded = 0; // sum of the samples' key counts
+    uint64_t deviceBytes = 0;
+    double buildSeconds = 0;
+    int *dErr = nullptr;
+    unsigned long long *dCounters = nullptr; // [0] pending count, [1] scan work counter
+    // scan plan and scratch
+    const ibs_reference *planRef = nullptr;
+    std::vector<uint64_t> planLens;
+    ScanPlan plan;
+    SegStats *dSpans = nullptr;
+    uint64_t spansCap = 0;
+    // captured scan graph for (reference, W, rows, stream)
+    cudaGraphExec_t graph = nullptr;
+    const void *graphKey[3] = {nullptr, nullptr, nullptr};
+    uint32_t graphW = 0;
+    View view() const { return View{geom, buckets, stash, stashBuckets}; }
+};
+
+extern "C" ibs_status ibs_panel_table_create(uint32_t k, uint64_t expected_keys,
+                                             const ibs_table_opts *opts, ibs_panel_table **out)
+{
+    clear_error();
+    if (!out || k == 0 || k > 32) {
+        set_error("ibs_panel_table_create: bad argument");
+        return IBS_ERR_ARG;
+    }
+    *out = nullptr;
+    const int dev = opts ? opts->device : 0;
+    ibs_status s = check_device_ordinal(dev);
+    if (s != IBS_OK)
+        return s;
+    DeviceGuard guard(dev);
+    std::unique_ptr<ibs_panel_table> p(new ibs_panel_table);
+    p->device = dev;
+    TableGeom &g = p->geom;
+    g.k = k;
+    g.bits = 2 * k;
+    g.format = 3;
+    const double lam = (opts && opts->keys_per_bucket > 0) ? opts->keys_per_bucket : 3.0;
+    uint64_t nb = (uint64_t)((double)expected_keys / lam) + 1;
+    const uint64_t minN = g.bits > 32 ? (1ull << (g.bits - 32)) : 1;
+    nb = std::max(nb, minN);
+    if (g.bits < 64)
+        nb = std::min<uint64_t>(nb, 1ull << g.bits);
+    g.nBuckets = nb;
+    g.fpBits = (uint32_t)std::max<int>(1, (int)g.bits - (int)(63 - __builtin_clzll(nb)));
+    p->stashBuckets = next_pow2(std::max<uint64_t>(1u << 16, (uint64_t)(expected_keys * 0.06) / 2 + 1));
+    g.stashBuckets = p->stashBuckets;
+    IBS_CUDA(cudaMalloc(&p->buckets, nb * 32), "panel table alloc");
+    IBS_CUDA(cudaMemset(p->buckets, 0, nb * 32), "panel table init");
+    IBS_CUDA(cudaMalloc(&p->stash, p->stashBuckets * 32), "panel stash alloc");
+    k_stash_init<<<grid_for(p->stashBuckets * 2), 256>>>(p->stash, p->stashBuckets * 2);
+    IBS_LAUNCHED();
+    IBS_CUDA(cudaGetLastError(), "panel stash init");
+    IBS_CUDA(cudaMalloc(&p->dErr, sizeof(int)), "panel alloc");
+    IBS_CUDA(cudaMemset(p->dErr, 0, sizeof(int)), "panel alloc");
+    IBS_CUDA(cudaMalloc(&p->dCounters, 16), "panel alloc");
+    p->deviceBytes = nb * 32 + p->stashBuckets * 32;
+    *out = p.release();
+    return IBS_OK;
+}
+
+static ibs_status panel_add_device_codes(ibs_panel_table *p, const uint64_t *dCodes, uint64_t n)
+{
+    if (p->nSamples >= kMaxSamples) {
+        set_error("panel table already holds " + std::to_string(kMaxSamples) + " samples");
+        return IBS_ERR_CAPACITY;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    const uint32_t bit = p->nSamples;
+    if (p->graph) { // the captured scan holds the old sample count
+        cudaGraphExecDestroy(p->graph);
+        p->graph = nullptr;
+    }
+    uint64_t *pending = nullptr;
+    IBS_CUDA(cudaMalloc(&pending, std::max<uint64_t>(n, 1) * 8), "panel pending alloc");
+    std::unique_ptr<uint64_t, cudaError_t (*)(void *)> guard(pending, cudaFree);
+    IBS_CUDA(cudaMemset(p->dCounters, 0, 8), "panel build");
+    View v = p->view();
+    uint32_t *words = reinterpret_cast<uint32_t *>(p->buckets);
+    unsigned long long *stashWords = reinterpret_cast<unsigned long long *>(p->stash);
+    if (n) {
+        k_find<<<grid_for(n), 256>>>(v, words, stashWords, dCodes, n, bit, pending, p->dCounters);
+        IBS_LAUNCHED();
+    }
+    unsigned long long nPend = 0;
+    IBS_CUDA(cudaMemcpy(&nPend, p->dCounters, 8, cudaMemcpyDeviceToHost), "panel build find");
+    if (nPend) {
+        k_insert<<<grid_for(nPend), 256>>>(v, words, stashWords, pending, nPend, bit, p->dErr);
+        IBS_LAUNCHED();
+    }
+    int err = 0;
+    IBS_CUDA(cudaMemcpy(&err, p->dErr, sizeof(int), cudaMemcpyDeviceToHost), "panel build insert");
+    if (err) {
+        set_error("panel table: stash full (raise expected_keys)");
+        return IBS_ERR_CAPACITY;
+    }
+    p->nSamples++;
+    p->keysAdded += n;
+    p->buildSeconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return IBS_OK;
+}
+
+extern "C" ibs_status ibs_panel_table_add_codes(ibs_panel_table *p, const uint64_t *codes, uint64_t n,
+                                                int codes_on_device)
+{
+    clear_error();
+    if (!p || (n && !codes)) {
+        set_error("ibs_panel_table_add_codes: bad argument");
+        return IBS_ERR_ARG;
+    }
+    DeviceGuard guard(p->device);
+    if (codes_on_device)
+        return panel_add_device_codes(p, codes, n);
+    uint64_t *d = nullptr;
+    IBS_CUDA(cudaMalloc(&d, std::max<uint64_t>(n, 1) * 8), "codes alloc");
+    std::unique_ptr<uint64_t, cudaError_t (*)(void *)> guard2(d, cudaFree);
+    IBS_CUDA(cudaMemcpy(d, codes, n * 8, cudaMemcpyHostToDevice), "codes upload");
+    return panel_add_device_codes(p, d, n);
+}
+
+extern "C" ibs_status ibs_panel_table_add_kmc(ibs_panel_table *p, const char *prefix)
+{
+    clear_error();
+    if (!p || !prefix) {
+        set_error("ibs_panel_table_add_kmc: bad argument");
+        return IBS_ERR_ARG;
+    }
+    DeviceGuard guard(p->device);
+    uint64_t *d = nullptr, n = 0;
+    uint32_t k = 0;
+    ibs_status s = decode_kmc(prefix, p->device, &d, &n, &k);
+    if (s != IBS_OK)
+        return s;
+    std::unique_ptr<uint64_t, cudaError_t (*)(void *)> guard2(d, cudaFree);
+    if (k != p->geom.k) {
+        set_error(std::string("panel table: ") + prefix + " has k=" + std::to_string(k) +
+                  " but the panel has k=" + std::to_string(p->geom.k) + "; a panel shares one k");
+        return IBS_ERR_ARG;
+    }
+    return panel_add_device_codes(p, d, n);
+}
+
+extern "C" ibs_status ibs_panel_table_info_get(const ibs_panel_table *p, ibs_table_info *info,
+                                               uint32_t *n_samples)
+{
+    clear_error();
+    if (!p || !info) {
+        set_error("ibs_panel_table_info_get: bad argument");
+        return IBS_ERR_ARG;
+    }
+    memset(info, 0, sizeof *info);
+    info->k = p->geom.k;
+    info->format = p->geom.format;
+    info->fp_bits = p->geom.fpBits;
+    info->n_keys = p->keysAdded;
+    info->n_buckets = p->geom.nBuckets;
+    info->stash_buckets = p->stashBuckets;
+    info->device_bytes = p->deviceBytes;
+    info->build_seconds = p->buildSeconds;
+    if (n_samples)
+        *n_samples = p->nSamples;
+    return IBS_OK;
+}
+
+extern "C" ibs_status ibs_panel_table_probe(ibs_panel_table *p, const uint64_t *codes, uint64_t n,
+                                            uint32_t *masks)
+{
+    clear_error();
+    if (!p || (n && (!codes || !masks))) {
+        set_error("ibs_panel_table_probe: bad argument");
+        return IBS_ERR_ARG;
+    }
+    if (!n)
+        return IBS_OK;
+    DeviceGuard guard(p->device);
+    uint64_t *dc = nullptr;
+    uint32_t *dm = nullptr;
+    IBS_CUDA(cudaMalloc(&dc, n * 8), "probe alloc");
+    std::unique_ptr<uint64_t, cudaError_t (*)(void *)> g1(dc, cudaFree);
+    IBS_CUDA(cudaMalloc(&dm, n * 4), "probe alloc");
+    std::unique_ptr<uint32_t, cudaError_t (*)(void *)> g2(dm, cudaFree);
+    IBS_CUDA(cudaMemcpy(dc, codes, n * 8, cudaMemcpyHostToDevice), "probe upload");
+    k_probe_masks<<<grid_for(n), 256>>>(p->view(), dc, n, dm);
+    IBS_LAUNCHED();
+    IBS_CUDA(cudaMemcpy(masks, dm, n * 4, cudaMemcpyDeviceToHost), "probe download");
+    return IBS_OK;
+}
+
+// Plan and scratch of (reference, W) for the panel scan.
+static ibs_status panel_plan(ibs_panel_table *p, const ibs_reference *ref, uint32_t W)
+{
+    if (p->planRef == ref && p->plan.W == W && p->plan.dWin && p->planLens == ref->lens)
+        return IBS_OK;
+    p->plan.release();
+    plan_windows(p->plan, ref->lens, ref->baseOff, W, p->geom.k, kSpanLen);
+    IBS_CUDA(cudaMalloc(&p->plan.dWin, std::max<uint64_t>(p->plan.nWin, 1) * sizeof(WinDesc)), "plan alloc");
+    IBS_CUDA(cudaMalloc(&p->plan.dSpan0, (p->plan.nWin + 1) * sizeof(uint32_t)), "plan alloc");
+    if (p->plan.nWin)
+        IBS_CUDA(cudaMemcpy(p->plan.dWin, p->plan.win.data(), p->plan.nWin * sizeof(WinDesc),
+                            cudaMemcpyHostToDevice),
+                 "plan upload");
+    IBS_CUDA(cudaMemcpy(p->plan.dSpan0, p->plan.span0.data(), (p->plan.nWin + 1) * sizeof(uint32_t),
+                        cudaMemcpyHostToDevice),
+             "plan upload");
+    const uint64_t need = std::max<uint64_t>(1, p->plan.nSpans * kMaxSamples);
+    if (p->spansCap < need) {
+        cudaFree(p->dSpans);
+        p->dSpans = nullptr;
+        p->spansCap = 0;
+        IBS_CUDA(cudaMalloc(&p->dSpans, need * sizeof(SegStats)), "panel span scratch");
+        p->spansCap = need;
+    }
+    p->planRef = ref;
+    p->planLens = ref->lens;
+    if (p->graph) {
+        cudaGraphExecDestroy(p->graph);
+        p->graph = nullptr;
+    }
+    return IBS_OK;
+}
+
+static ibs_status panel_enqueue(ibs_panel_table *p, const ibs_reference *ref, ibs_window *rowsDev,
+                                cudaStream_t st)
+{
+    const ScanPlan &pl = p->plan;
+    IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
+    if (pl.nSpans) {
+        const int grid = sm_count() * 6;
+        k_panel_spans<kNB><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
+                                                 (uint32_t)pl.nWin, pl.nSpans, pl.spanLen, p->nSamples,
+                                                 p->dCounters + 1, p->dSpans);
+        IBS_LAUNCHED();
+    }
+    if (pl.nWin && p->nSamples) {
+        k_panel_finalize<<<grid_for(pl.nWin * p->nSamples), 256, 0, st>>>(
+            pl.dWin, pl.dSpan0, pl.nWin, pl.nSpans, p->nSamples, p->dSpans, (int)p->geom.k, rowsDev);
+        IBS_LAUNCHED();
+    }
+    IBS_CUDA(cudaGetLastError(), "panel scan launch");
+    return IBS_OK;
+}
+
+extern "C" ibs_status ibs_panel_table_scan_async(ibs_panel_table *p, ibs_reference *ref, uint32_t W,
+                                                 ibs_window *rows_dev, uint64_t cap, void *stream)
+{
+    clear_error();
+    if (!p || !ref || p->device != ref->device) {
+        set_error("ibs_panel_table_scan_async: bad argument");
+        return IBS_ERR_ARG;
+    }
+    if (W <= p->geom.k) {
+        set_error("window size " + std::to_string(W) + " must be larger than k (" +
+                  std::to_string(p->geom.k) + ")");
+        return IBS_ERR_ARG;
+    }
+    const uint64_t nWin = ibs_window_count(ref->lens.data(), (uint32_t)ref->lens.size(), W, p->geom.k);
+    if (nWin * p->nSamples > cap || (nWin && p->nSamples && !rows_dev)) {
+        set_error("ibs_panel_table_scan_async: row capacity too small (samples x windows)");
+        return IBS_ERR_ARG;
+    }
+    DeviceGuard guard(p->device);
+    ibs_status s = panel_plan(p, ref, W);
+    if (s != IBS_OK)
+        return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    // Replay the captured scan when (reference, W, rows, stream) repeat:
+    // the work reset, the span kernel and the finalizer as one graph.
+    const void *key[3] = {ref, rows_dev, stream};
+    if (p->graph && p->graphW == W && !memcmp(key, p->graphKey, sizeof key)) {
+        IBS_CUDA(cudaGraphLaunch(p->graph, st), "panel graph launch");
+        IBS_LAUNCHED();
+        return IBS_OK;
+    }
+    if (p->graph) {
+        cudaGraphExecDestroy(p->graph);
+        p->graph = nullptr;
+    }
+    cudaStream_t cap_st = nullptr;
+    IBS_CUDA(cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking), "capture stream");
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cap_st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        s = panel_enqueue(p, ref, rows_dev, cap_st);
+        e = cudaStreamEndCapture(cap_st, &g);
+    }
+    if (e == cudaSuccess && s == IBS_OK)
+        e = cudaGraphInstantiate(&p->graph, g, 0);
+    if (g)
+        cudaGraphDestroy(g);
+    cudaStreamDestroy(cap_st);
+    if (s != IBS_OK)
+        return s;
+    IBS_CUDA(e, "panel graph capture");
+    memcpy(p->graphKey, key, sizeof key);
+    p->graphW = W;
+    IBS_CUDA(cudaGraphLaunch(p->graph, st), "panel graph launch");
+    return IBS_OK;
+}
+
+extern "C" ibs_status ibs_panel_table_scan(ibs_panel_table *p, ibs_reference *ref, uint32_t W,
+                                           ibs_window *rows, uint64_t cap)
+{
+    clear_error();
+    if (!p || !ref) {
+        set_error("ibs_panel_table_scan: bad argument");
+        return IBS_ERR_ARG;
+    }
+    const uint64_t nWin = ibs_window_count(ref->lens.data(), (uint32_t)ref->lens.size(), W, p->geom.k);
+    const uint64_t need = nWin * p->nSamples;
+    if (need > cap || (need && !rows)) {
+        set_error("ibs_panel_table_scan: row capacity too small (samples x windows)");
+        return IBS_ERR_ARG;
+    }
+    DeviceGuard guard(p->device);
+    ibs_window *d = nullptr;
+    IBS_CUDA(cudaMalloc(&d, std::max<uint64_t>(need, 1) * sizeof(ibs_window)), "row alloc");
+    std::unique_ptr<ibs_window, cudaError_t (*)(void *)> g(d, cudaFree);
+    cudaStream_t st = nullptr;
+    IBS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream create");
+    ibs_status s = ibs_panel_table_scan_async(p, ref, W, d, need, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (s == IBS_OK && e == cudaSuccess && need)
+        e = cudaMemcpy(rows, d, need * sizeof(ibs_window), cudaMemcpyDeviceToHost);
+    // the graph was captured for this call's temporary buffers: drop it
+    if (p->graph && p->graphKey[1] == d) {
+        cudaGraphExecDestroy(p->graph);
+        p->graph = nullptr;
+    }
+    cudaStreamDestroy(st);
+    if (s != IBS_OK)
+        return s;
+    IBS_CUDA(e, "panel scan");
+    return IBS_OK;
+}
+
+extern "C" void ibs_panel_table_close(ibs_panel_table *p)
+{
+    if (!p)
+        return;
+    {
+        DeviceGuard guard(p->device);
+        if (p->graph)
+            cudaGraphExecDestroy(p->graph);
+        p->plan.release();
+        cudaFree(p->dSpans);
+        cudaFree(p->buckets);
+        cudaFree(p->stash);
+        cudaFree(p->dErr);
+        cudaFree(p->dCounters);
+    }
+    delete p;
+}

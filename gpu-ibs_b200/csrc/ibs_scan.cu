@@ -25,8 +25,11 @@
 namespace ibs {
 
 constexpr uint32_t FULL = 0xffffffffu;
-constexpr uint32_t kSpanLen = 4096; // positions per warp task
-constexpr int kNB = 4;              // 32-position blocks in flight per lane
+
+static std::mutex g_tuneMu;
+static ibs_tuning g_tune = {4096, 4, 256, 8, 4.0, 0, {0, 0, 0}};
+
+const ibs_tuning &tuning() { return g_tune; }
 
 // Statistics of one 32-position block from its valid (V) and hit (H) ballots
 // (bit i = position p+i; H is a subset of V). Every lane returns the same
@@ -102,7 +105,7 @@ __device__ __forceinline__ uint32_t window_of_span(const uint32_t *__restrict__ 
 }
 
 template <uint32_t FMT, int NB>
-__global__ void __launch_bounds__(256) k_scan_spans(TableView t, const uint64_t *__restrict__ seq,
+__global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t *__restrict__ seq,
                                                     const uint64_t *__restrict__ mask,
                                                     const WinDesc *__restrict__ win,
                                                     const uint32_t *__restrict__ span0,
@@ -152,6 +155,123 @@ __global__ void __launch_bounds__(256) k_scan_spans(TableView t, const uint64_t 
                 bool hit = false;
                 if (valid[b]) {
                     const uint32_t m = bucket_match<FMT>(v0[b], v1[b], fp[b]);
+                    hit = m == 1u || (m == 2u && stash_lookup(t, code[b]));
+                }
+                const uint32_t V = __ballot_sync(FULL, valid[b]);
+                const uint32_t H = __ballot_sync(FULL, hit);
+                acc = seg_combine(acc, block_stats(V, H, lane, (int)k), (int)k);
+            }
+        }
+        if (lane == 0)
+            out[s] = acc;
+    }
+}
+
+// 16-mer hash at packed base G (its canonical form's 32-bit bijective hash).
+__device__ __forceinline__ uint32_t mmer_hash_at(const uint64_t *__restrict__ seq, uint64_t G)
+{
+    const uint64_t wi = G >> 5;
+    const uint32_t sh = (uint32_t)(G & 31) * 2;
+    const uint64_t x = (__ldg(seq + wi) >> sh) | ((__ldg(seq + wi + 1) << (63 - sh)) << 1);
+    const uint32_t lo = (uint32_t)x; // 16 bases, first at the low bits
+    uint32_t f = __brev(lo);
+    f = ((f >> 1) & 0x55555555u) | ((f & 0x55555555u) << 1); // first base high
+    const uint32_t r = ~lo;
+    return mz::hash16(f < r ? f : r);
+}
+
+// The scan over a minimizer-bucketed table (format MZ8). Each lane hashes the
+// 16-mer starting at its position one block ahead; a k-mer's minimizer is
+// the minimum over the next w lanes' hashes (shuffles across the block
+// boundary), tracked with its leftmost and rightmost offsets so the
+// leftmost-in-the-canonical-k-mer rule holds on either strand. Lanes whose
+// k-mers share a minimizer load the same bucket; the hardware merges them.
+template <int NB>
+__global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64_t *__restrict__ seq,
+                                                       const uint64_t *__restrict__ mask,
+                                                       const WinDesc *__restrict__ win,
+                                                       const uint32_t *__restrict__ span0,
+                                                       uint32_t nWin, uint64_t s0, uint64_t s1,
+                                                       uint32_t spanLen, SegStats *__restrict__ out)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t k = t.g.k;
+    const uint32_t w = mz::w_of(k);
+    const uint64_t kmask = key_mask(2 * k);
+    const uint64_t kbits = (1ull << k) - 1;
+    for (uint64_t s = s0 + warp; s < s1; s += nWarps) {
+        const uint32_t wIdx = window_of_span(span0, nWin, s);
+        const uint64_t base = win[wIdx].base;
+        const uint32_t nPos = win[wIdx].nPos;
+        const uint32_t p0 = (uint32_t)(s - __ldg(span0 + wIdx)) * spanLen;
+        const uint32_t p1 = min(p0 + spanLen, nPos);
+        const uint32_t lastM = nPos - 1 + (w - 1); // last 16-mer start the window's k-mers use
+        SegStats acc = seg_empty();
+        uint32_t hNext = mmer_hash_at(seq, base + min(p0 + lane, lastM));
+        for (uint32_t p = p0; p < p1; p += 32 * NB) {
+            uint32_t hb[NB + 1];
+            hb[0] = hNext;
+#pragma unroll
+            for (int b = 1; b <= NB; ++b)
+                hb[b] = mmer_hash_at(seq, base + min(p + 32 * b + lane, lastM));
+            hNext = hb[NB];
+            uint4 v0[NB], v1[NB];
+            uint64_t code[NB];
+            uint32_t slot[NB];
+            bool valid[NB];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const uint32_t q = p + 32 * b + lane;
+                const bool inSpan = q < p1;
+                const uint64_t G = base + (inSpan ? q : p0);
+                // k-mer and strand
+                const uint64_t wi = G >> 5;
+                const uint32_t sh = (uint32_t)(G & 31) * 2;
+                const uint64_t x = (__ldg(seq + wi) >> sh) | ((__ldg(seq + wi + 1) << (63 - sh)) << 1);
+                const uint64_t mi = G >> 6;
+                const uint32_t ms = (uint32_t)(G & 63);
+                const uint64_t mm = (__ldg(mask + mi) >> ms) | ((__ldg(mask + mi + 1) << (63 - ms)) << 1);
+                uint64_t y = __brevll(x);
+                y = ((y >> 1) & 0x5555555555555555ull) | ((y & 0x5555555555555555ull) << 1);
+                const uint64_t fwd = y >> (64 - 2 * k);
+                const uint64_t rc = ~x & kmask;
+                const bool isFwd = fwd <= rc;
+                code[b] = isFwd ? fwd : rc;
+                valid[b] = inSpan && (mm & kbits) == 0;
+                // minimizer over the w 16-mers starting at q .. q+w-1
+                uint32_t mn = 0xffffffffu, jl = 0, jr = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < 16; ++j) {
+                    if (j < w) {
+                        const uint32_t src = lane + j;
+                        const uint32_t a = __shfl_sync(FULL, hb[b], src & 31);
+                        const uint32_t c = __shfl_sync(FULL, hb[b + 1], src & 31);
+                        const uint32_t v = src < 32 ? a : c;
+                        if (v < mn || j == 0) {
+                            mn = v;
+                            jl = jr = j;
+                        } else if (v == mn)
+                            jr = j;
+                    }
+                }
+                const uint32_t o = isFwd ? jl : (w - 1 - jr);
+                const uint64_t r = mz::bucket_of_h(mn, t.g.nBuckets);
+                slot[b] = mz::slot_value(mz::slot_high(code[b], k, o), mn, t.g.fpBits);
+                if (valid[b]) {
+                    v0[b] = __ldg(t.buckets + 2 * r);
+                    v1[b] = __ldg(t.buckets + 2 * r + 1);
+                } else {
+                    v0[b] = make_uint4(0, 0, 0, 0);
+                    v1[b] = make_uint4(0, 0, 0, 0);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                bool hit = false;
+                if (valid[b]) {
+                    const uint32_t m = bucket_match<FMT_B8X32>(v0[b], v1[b], slot[b]);
                     hit = m == 1u || (m == 2u && stash_lookup(t, code[b]));
                 }
                 const uint32_t V = __ballot_sync(FULL, valid[b]);
@@ -241,18 +361,35 @@ void plan_windows(ScanPlan &p, const std::vector<uint64_t> &lens,
     p.nSpans = spans;
 }
 
+template <uint32_t FMT, int NB>
+static void launch_nb(const ibs_table *t, const uint64_t *dSeq, const uint64_t *dMask, const ScanPlan &p,
+                      uint64_t s0, uint64_t s1, SegStats *dSpans, cudaStream_t st, int grid, int threads)
+{
+    if (FMT == FMT_MZ8)
+        k_scan_spans_mz<NB><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
+                                                      (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
+    else
+        k_scan_spans<FMT, NB><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
+                                                        (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
+}
+
 template <uint32_t FMT>
 static void launch_spans_fmt(const ibs_table *t, const uint64_t *dSeq, const uint64_t *dMask,
                              const ScanPlan &p, uint64_t s0, uint64_t s1, SegStats *dSpans,
                              cudaStream_t st)
 {
-    const int threads = 256;
-    const uint64_t warps = s1 - s0;
-    const uint64_t want = (warps + 7) / 8;
-    const uint64_t cap = (uint64_t)sm_count() * 8;
+    const ibs_tuning tu = tuning();
+    const int threads = (int)tu.block_threads;
+    const uint64_t warpsPerCta = threads / 32;
+    const uint64_t want = (s1 - s0 + warpsPerCta - 1) / warpsPerCta;
+    const uint64_t cap = (uint64_t)sm_count() * tu.ctas_per_sm;
     const int grid = (int)std::max<uint64_t>(1, std::min(want, cap));
-    k_scan_spans<FMT, kNB><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
-                                                     (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
+    switch (tu.blocks_in_flight) {
+    case 1: launch_nb<FMT, 1>(t, dSeq, dMask, p, s0, s1, dSpans, st, grid, threads); break;
+    case 2: launch_nb<FMT, 2>(t, dSeq, dMask, p, s0, s1, dSpans, st, grid, threads); break;
+    case 8: launch_nb<FMT, 8>(t, dSeq, dMask, p, s0, s1, dSpans, st, grid, threads); break;
+    default: launch_nb<FMT, 4>(t, dSeq, dMask, p, s0, s1, dSpans, st, grid, threads); break;
+    }
 }
 
 static ibs_status launch_spans(const ibs_table *t, const uint64_t *dSeq, const uint64_t *dMask,
@@ -263,6 +400,8 @@ static ibs_status launch_spans(const ibs_table *t, const uint64_t *dSeq, const u
         return IBS_OK;
     if (t->geom.format == FMT_B8X32)
         launch_spans_fmt<FMT_B8X32>(t, dSeq, dMask, p, s0, s1, dSpans, st);
+    else if (t->geom.format == FMT_MZ8)
+        launch_spans_fmt<FMT_MZ8>(t, dSeq, dMask, p, s0, s1, dSpans, st);
     else
         launch_spans_fmt<FMT_B6X40>(t, dSeq, dMask, p, s0, s1, dSpans, st);
     IBS_LAUNCHED();
@@ -578,11 +717,12 @@ extern "C" void ibs_reference_free(ibs_reference *r)
 static ibs_status ensure_plan(ibs_reference *r, uint32_t W, uint32_t k)
 {
     ScanPlan &p = r->plan;
-    if (p.dWin && p.W == W && p.k == k && p.spanLen == kSpanLen)
+    const uint32_t spanLen = tuning().span_len;
+    if (p.dWin && p.W == W && p.k == k && p.spanLen == spanLen)
         return IBS_OK;
     IBS_CUDA(cudaStreamSynchronize(r->stream), "plan sync");
     p.release();
-    plan_windows(p, r->lens, r->baseOff, W, k, kSpanLen);
+    plan_windows(p, r->lens, r->baseOff, W, k, spanLen);
     ibs_status s = upload_plan(p, r->stream);
     if (s != IBS_OK)
         p.release();
@@ -829,7 +969,7 @@ extern "C" ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit,
     cudaFree(p.dSpan0);
     p.dWin = nullptr;
     p.dSpan0 = nullptr;
-    plan_windows(p, lv, off, W, k, kSpanLen);
+    plan_windows(p, lv, off, W, k, tuning().span_len);
     if (p.nSpans > ws.spansCap || !p.dSpans) {
         cudaFree(p.dSpans);
         p.dSpans = nullptr;
@@ -925,4 +1065,53 @@ extern "C" ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit,
     IBS_CUDA(cudaStreamSynchronize(ws.comp), "scan");
     IBS_CUDA(cudaStreamSynchronize(ws.copy), "scan");
     return IBS_OK;
+}
+
+extern "C" ibs_status ibs_set_tuning(const ibs_tuning *t)
+{
+    clear_error();
+    if (!t) {
+        set_error("ibs_set_tuning: null");
+        return IBS_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_tuneMu);
+    ibs_tuning n = g_tune;
+    if (t->span_len) {
+        if (t->span_len % 128 || t->span_len > (1u << 24)) {
+            set_error("ibs_set_tuning: span_len must be a multiple of 128");
+            return IBS_ERR_ARG;
+        }
+        n.span_len = t->span_len;
+    }
+    if (t->blocks_in_flight) {
+        if (t->blocks_in_flight != 1 && t->blocks_in_flight != 2 && t->blocks_in_flight != 4 &&
+            t->blocks_in_flight != 8) {
+            set_error("ibs_set_tuning: blocks_in_flight must be 1, 2, 4 or 8");
+            return IBS_ERR_ARG;
+        }
+        n.blocks_in_flight = t->blocks_in_flight;
+    }
+    if (t->block_threads) {
+        if (t->block_threads != 128 && t->block_threads != 256 && t->block_threads != 512) {
+            set_error("ibs_set_tuning: block_threads must be 128, 256 or 512");
+            return IBS_ERR_ARG;
+        }
+        n.block_threads = t->block_threads;
+    }
+    if (t->ctas_per_sm)
+        n.ctas_per_sm = std::min<uint32_t>(t->ctas_per_sm, 64);
+    if (t->keys_per_bucket > 0)
+        n.keys_per_bucket = t->keys_per_bucket;
+    if (t->table_format)
+        n.table_format = t->table_format == 0xffffffffu ? 0 : t->table_format;
+    g_tune = n;
+    return IBS_OK;
+}
+
+extern "C" void ibs_get_tuning(ibs_tuning *t)
+{
+    if (t) {
+        std::lock_guard<std::mutex> lock(g_tuneMu);
+        *t = g_tune;
+    }
 }

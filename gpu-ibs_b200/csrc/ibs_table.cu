@@ -56,7 +56,7 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
     TableGeom g{};
     g.k = k;
     g.bits = 2 * k;
-    const double lam = (o && o->keys_per_bucket > 0) ? o->keys_per_bucket : 4.0;
+    const double lam = (o && o->keys_per_bucket > 0) ? o->keys_per_bucket : tuning().keys_per_bucket;
     const uint64_t space = g.bits >= 64 ? ~0ull : (1ull << g.bits);
     auto clampN = [&](uint64_t n) {
         if (n < 1)
@@ -70,6 +70,19 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
     const uint64_t n6 = clampN((uint64_t)((double)nKeys / (lam * 6.0 / 8.0)) + 1);
     const uint64_t min6 = g.bits > 40 ? (1ull << (g.bits - 40)) : 1;
     uint32_t fmt = o ? o->force_format : 0;
+    if (fmt == 0 && tuning().table_format == FMT_MZ8 && k >= 16 && k <= 27)
+        fmt = FMT_MZ8; // the tuned default, where the minimizer layout applies
+    if (fmt == FMT_AUTO_HASH)
+        fmt = 0;
+    if (fmt == FMT_MZ8) {
+        // minimizer buckets: the slot value needs nBuckets >= 2^(2k-26)
+        g.format = FMT_MZ8;
+        const uint64_t minMz = g.bits > 26 ? (1ull << (g.bits - 26)) : 1;
+        g.nBuckets = std::min<uint64_t>(std::max(n8, minMz), 1ull << 32);
+        g.fpBits = (uint32_t)std::max<int>(1, 32 - (int)floor_log2(g.nBuckets));
+        g.stashBuckets = 0;
+        return g;
+    }
     if (fmt == 0)
         fmt = (std::max(n8, min8) <= 2 * n8) ? FMT_B8X32 : FMT_B6X40;
     g.format = fmt;
@@ -84,13 +97,28 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
 // ---------------------------------------------------------------------------
 // build kernels
 // ---------------------------------------------------------------------------
+// Bucket and stored fingerprint of a key in either table family.
+__device__ __forceinline__ void locate_key(uint64_t code, const TableGeom &g, uint64_t &r, uint64_t &fp)
+{
+    if (g.format == FMT_MZ8) {
+        uint32_t slot;
+        mz::locate(code, g, r, slot);
+        fp = slot;
+        return;
+    }
+    const uint64_t h = perm_hash(code, g.bits);
+    r = bucket_of(h, g);
+    fp = fp_of(h, g);
+}
+
 __global__ void k_count(const uint64_t *__restrict__ codes, uint64_t n, TableGeom g,
                         uint32_t *__restrict__ cnt)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t h = perm_hash(codes[i], g.bits);
-        atomicAdd(cnt + bucket_of(h, g), 1u);
+        uint64_t r, fp;
+        locate_key(codes[i], g, r, fp);
+        atomicAdd(cnt + r, 1u);
     }
 }
 
@@ -103,7 +131,7 @@ __global__ void k_mark(uint32_t *__restrict__ cnt, uint64_t nb, TableGeom g,
     for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < nb;
          r += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t c = cnt[r];
-        if (g.format == FMT_B8X32) {
+        if (g.format == FMT_B8X32 || g.format == FMT_MZ8) {
             if (c > 8) {
                 words[r * 8 + 7] = B8_OVERFLOW;
                 local += c - 7;
@@ -147,12 +175,11 @@ __global__ void k_place(const uint64_t *__restrict__ codes, uint64_t n, TableGeo
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t code = codes[i];
-        const uint64_t h = perm_hash(code, g.bits);
-        const uint64_t r = bucket_of(h, g);
-        const uint64_t fp = fp_of(h, g);
+        uint64_t r, fp;
+        locate_key(code, g, r, fp);
         const uint32_t s = atomicAdd(cnt + r, 1u);
         bool stashed = false;
-        if (g.format == FMT_B8X32) {
+        if (g.format == FMT_B8X32 || g.format == FMT_MZ8) {
             const uint32_t limit = words[r * 8 + 7] == B8_OVERFLOW ? 7u : 8u;
             if (s < limit)
                 words[r * 8 + s] = (uint32_t)fp;
@@ -227,7 +254,7 @@ static ibs_status build_from_device_codes(ibs_table *t, const uint64_t *dCodes, 
     const uint64_t nb = g.nBuckets;
     IBS_CUDA(cudaMalloc(&t->buckets, nb * 32), "table alloc");
     t->deviceBytes = nb * 32;
-    IBS_CUDA(cudaMemset(t->buckets, g.format == FMT_B8X32 ? 0xff : 0x00, nb * 32), "table init");
+    IBS_CUDA(cudaMemset(t->buckets, g.format == FMT_B6X40 ? 0x00 : 0xff, nb * 32), "table init");
     uint32_t *cnt = nullptr;
     unsigned long long *dOverflow = nullptr;
     int *dErr = nullptr;
@@ -441,15 +468,15 @@ extern "C" int ibs_device_count(void)
 
 extern "C" uint64_t ibs_launch_count(void) { return launch_counter().load(); }
 
-static ibs_status check_device(int dev)
+
+static ibs_status check_format(uint32_t k, const ibs_table_opts *o)
 {
-    const int n = ibs_device_count();
-    if (n == 0) {
-        set_error("no usable CUDA device (the scan has no CPU fallback)");
-        return IBS_ERR_CUDA;
+    if (o && o->force_format == FMT_MZ8 && (k < 16 || k > 27)) {
+        set_error("minimizer-bucketed tables (format 4) need 16 <= k <= 27");
+        return IBS_ERR_UNSUPPORTED;
     }
-    if (dev < 0 || dev >= n) {
-        set_error("device " + std::to_string(dev) + " out of range");
+    if (o && o->force_format > FMT_AUTO_HASH) {
+        set_error("unknown table format " + std::to_string(o->force_format));
         return IBS_ERR_ARG;
     }
     return IBS_OK;
@@ -466,7 +493,10 @@ extern "C" ibs_status ibs_table_from_codes(const uint64_t *codes, uint64_t n, ui
     }
     *out = nullptr;
     const int dev = opts ? opts->device : 0;
-    ibs_status s = check_device(dev);
+    ibs_status s = check_format(k, opts);
+    if (s != IBS_OK)
+        return s;
+    s = check_device_ordinal(dev);
     if (s != IBS_OK)
         return s;
     DeviceGuard guard(dev);
@@ -496,15 +526,26 @@ extern "C" ibs_status ibs_table_from_codes(const uint64_t *codes, uint64_t n, ui
     return IBS_OK;
 }
 
-extern "C" ibs_status ibs_open(const char *prefix, const ibs_table_opts *opts, ibs_table **out)
+ibs_status ibs::check_device_ordinal(int dev)
 {
-    clear_error();
-    if (!prefix || !out) {
-        set_error("ibs_open: bad argument");
+    const int n = ibs_device_count();
+    if (n == 0) {
+        set_error("no usable CUDA device (the scan has no CPU fallback)");
+        return IBS_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= n) {
+        set_error("device " + std::to_string(dev) + " out of range");
         return IBS_ERR_ARG;
     }
-    *out = nullptr;
-    const auto t0 = std::chrono::steady_clock::now();
+    return IBS_OK;
+}
+
+namespace ibs {
+// Decodes <prefix>.kmc_pre/.kmc_suf into canonical codes in device memory
+// (cudaMalloc'd; the caller frees *dCodes). The device must be current.
+ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_t *nOut, uint32_t *kOut)
+{
+    *dCodesOut = nullptr;
     const std::string pre = std::string(prefix) + ".kmc_pre";
     const std::string suf = std::string(prefix) + ".kmc_suf";
     KmcHeader h;
@@ -539,12 +580,9 @@ extern "C" ibs_status ibs_open(const char *prefix, const ibs_table_opts *opts, i
         set_error("KMC: suffix file smaller than expected: " + suf);
         return IBS_ERR_FORMAT;
     }
-    const int dev = opts ? opts->device : 0;
-    ibs_status s = check_device(dev);
+    ibs_status s = check_device_ordinal(dev);
     if (s != IBS_OK)
         return s;
-    DeviceGuard guard(dev);
-
     uint64_t *dCodes = nullptr, *dLut = nullptr;
     uint8_t *dRaw[2] = {nullptr, nullptr};
     uint8_t *hRaw[2] = {nullptr, nullptr};
@@ -632,10 +670,53 @@ extern "C" ibs_status ibs_open(const char *prefix, const ibs_table_opts *opts, i
     }
     cudaFree(dLut);
     dLut = nullptr;
+    *dCodesOut = dCodes;
+    dCodes = nullptr;
+    *nOut = total;
+    *kOut = h.k;
+    cleanup();
+    return IBS_OK;
+}
+} // namespace ibs
+
+extern "C" ibs_status ibs_open(const char *prefix, const ibs_table_opts *opts, ibs_table **out)
+{
+    clear_error();
+    if (!prefix || !out) {
+        set_error("ibs_open: bad argument");
+        return IBS_ERR_ARG;
+    }
+    *out = nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int dev = opts ? opts->device : 0;
+    {
+        // read the header first so a bad file is reported before any device check
+        KmcHeader h;
+        File f(std::string(prefix) + ".kmc_pre");
+        if (!f.f) {
+            set_error(std::string("KMC: cannot open ") + prefix + ".kmc_pre");
+            return IBS_ERR_IO;
+        }
+        ibs_status s = read_kmc_header(f.f, std::string(prefix) + ".kmc_pre", h);
+        if (s != IBS_OK)
+            return s;
+        s = check_format(h.k, opts);
+        if (s != IBS_OK)
+            return s;
+    }
+    ibs_status s = check_device_ordinal(dev);
+    if (s != IBS_OK)
+        return s;
+    DeviceGuard guard(dev);
+    uint64_t *dCodes = nullptr, total = 0;
+    uint32_t k = 0;
+    s = decode_kmc(prefix, dev, &dCodes, &total, &k);
+    if (s != IBS_OK)
+        return s;
     std::unique_ptr<ibs_table> t(new ibs_table);
     t->device = dev;
-    s = build_from_device_codes(t.get(), dCodes, total, h.k, opts);
-    cleanup();
+    s = build_from_device_codes(t.get(), dCodes, total, k, opts);
+    cudaFree(dCodes);
     if (s != IBS_OK) {
         ibs_close(t.release());
         return s;
@@ -686,6 +767,8 @@ extern "C" ibs_status ibs_probe(ibs_table *t, const uint64_t *codes, uint64_t n,
     if (e == cudaSuccess) {
         if (t->geom.format == FMT_B8X32)
             k_probe<FMT_B8X32><<<grid_for(n, 256), 256>>>(t->view(), dCodes, n, dHits);
+        else if (t->geom.format == FMT_MZ8)
+            k_probe<FMT_MZ8><<<grid_for(n, 256), 256>>>(t->view(), dCodes, n, dHits);
         else
             k_probe<FMT_B6X40><<<grid_for(n, 256), 256>>>(t->view(), dCodes, n, dHits);
         IBS_LAUNCHED();
@@ -710,7 +793,7 @@ extern "C" uint64_t ibs_table_bytes_for(uint64_t n_keys, uint32_t k, const ibs_t
 extern "C" ibs_status ibs_device_memory(int device, uint64_t *free_bytes, uint64_t *total_bytes)
 {
     clear_error();
-    ibs_status s = check_device(device);
+    ibs_status s = check_device_ordinal(device);
     if (s != IBS_OK)
         return s;
     DeviceGuard guard(device);

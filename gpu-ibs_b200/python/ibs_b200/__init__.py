@@ -49,6 +49,33 @@ u32p = C.POINTER(C.c_uint32)
 vp = C.c_void_p
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("memory_budget", C.c_uint64), ("max_spans_per_launch", C.c_uint32),
+                ("min_spans_per_request", C.c_uint32), ("one_request_per_launch", C.c_uint32),
+                ("reserved", C.c_uint32 * 5)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("request_id", C.c_uint64), ("sample", C.c_uint32), ("contig", C.c_uint32),
+                ("first_window", C.c_uint64), ("n_windows", C.c_uint64), ("status", C.c_int),
+                ("submit_time", C.c_double), ("done_time", C.c_double), ("rows", C.c_void_p)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "launches", "spans", "probes", "reloads",
+                                          "reload_bytes", "evictions", "resident_bytes", "resident_tables")] + \
+               [(n, C.c_double) for n in ("busy_seconds", "latency_p50", "latency_p99", "latency_max")]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("span_len", C.c_uint32), ("blocks_in_flight", C.c_uint32), ("block_threads", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32), ("keys_per_bucket", C.c_double), ("table_format", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+
+
 class TableOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("keys_per_bucket", C.c_double),
                 ("force_format", C.c_uint32), ("reserved", C.c_uint32 * 5)]
@@ -115,6 +142,32 @@ _ibs_scan_panel = _sig(_lib, "ibs_scan_panel", C.c_int,
                        [C.POINTER(vp), C.c_uint32, vp, C.c_uint32, vp, C.c_uint64])
 _ibs_scan_noalloc = _sig(_lib, "ibs_scan_noalloc", C.c_int,
                          [vp, vp, vp, vp, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp])
+_ibs_pt_create = _sig(_lib, "ibs_panel_table_create", C.c_int,
+                      [C.c_uint32, C.c_uint64, C.POINTER(TableOpts), C.POINTER(vp)])
+_ibs_pt_add_kmc = _sig(_lib, "ibs_panel_table_add_kmc", C.c_int, [vp, C.c_char_p])
+_ibs_pt_add_codes = _sig(_lib, "ibs_panel_table_add_codes", C.c_int, [vp, vp, C.c_uint64, C.c_int])
+_ibs_pt_info = _sig(_lib, "ibs_panel_table_info_get", C.c_int, [vp, C.POINTER(TableInfo), u32p])
+_ibs_pt_probe = _sig(_lib, "ibs_panel_table_probe", C.c_int, [vp, vp, C.c_uint64, vp])
+_ibs_pt_scan = _sig(_lib, "ibs_panel_table_scan", C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint64])
+_ibs_pt_scan_async = _sig(_lib, "ibs_panel_table_scan_async", C.c_int,
+                          [vp, vp, C.c_uint32, vp, C.c_uint64, vp])
+_ibs_pt_close = _sig(_lib, "ibs_panel_table_close", None, [vp])
+_ibs_table_bytes_for = _sig(_lib, "ibs_table_bytes_for", C.c_uint64, [C.c_uint64, C.c_uint32, C.POINTER(TableOpts)])
+_ibs_device_memory = _sig(_lib, "ibs_device_memory", C.c_int, [C.c_int, u64p, u64p])
+_ibs_srv_create = _sig(_lib, "ibs_server_create", C.c_int,
+                       [vp, C.c_uint32, C.c_uint32, C.POINTER(ServerOpts), C.POINTER(vp)])
+_ibs_srv_add_kmc = _sig(_lib, "ibs_server_add_sample_kmc", C.c_int, [vp, C.c_char_p, u32p])
+_ibs_srv_add_codes = _sig(_lib, "ibs_server_add_sample_codes", C.c_int, [vp, vp, C.c_uint64, C.c_int, u32p])
+_ibs_srv_submit = _sig(_lib, "ibs_server_submit", C.c_int,
+                       [vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, u64p])
+_ibs_srv_poll = _sig(_lib, "ibs_server_poll", C.c_int,
+                     [vp, C.POINTER(RequestResult), C.c_uint32, u32p, C.c_int])
+_ibs_srv_release = _sig(_lib, "ibs_server_release", None, [vp, C.POINTER(RequestResult)])
+_ibs_srv_stats = _sig(_lib, "ibs_server_stats_get", C.c_int, [vp, C.POINTER(ServerStats)])
+_ibs_srv_now = _sig(_lib, "ibs_server_now", C.c_double, [vp])
+_ibs_srv_close = _sig(_lib, "ibs_server_close", None, [vp])
+_ibs_set_tuning = _sig(_lib, "ibs_set_tuning", C.c_int, [C.POINTER(Tuning)])
+_ibs_get_tuning = _sig(_lib, "ibs_get_tuning", None, [C.POINTER(Tuning)])
 _ibs_last_error = _sig(_lib, "ibs_last_error", C.c_char_p, [])
 _ibs_device_count = _sig(_lib, "ibs_device_count", C.c_int, [])
 _ibs_launch_count = _sig(_lib, "ibs_launch_count", C.c_uint64, [])
@@ -153,6 +206,16 @@ def _ptr(a) -> int:
     if hasattr(a, "data_ptr"):
         return a.data_ptr()
     raise TypeError(type(a))
+
+
+def set_tuning(t: Tuning):
+    _check(_ibs_set_tuning(C.byref(t)))
+
+
+def get_tuning() -> Tuning:
+    t = Tuning()
+    _ibs_get_tuning(C.byref(t))
+    return t
 
 
 def device_count() -> int:
@@ -217,6 +280,72 @@ class Table:
             self.close()
         except Exception:
             pass
+
+
+class PanelTable:
+    """A joint table over up to 16 samples (ibs_panel_table)."""
+
+    MAX_SAMPLES = 16
+
+    def __init__(self, k: int, expected_keys: int, device: int = 0, keys_per_bucket: float = 0.0):
+        opts = TableOpts(device, keys_per_bucket, 0)
+        h = vp()
+        _check(_ibs_pt_create(k, expected_keys, C.byref(opts), C.byref(h)))
+        self._h = h.value
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def add_kmc(self, prefix: str):
+        _check(_ibs_pt_add_kmc(self._h, str(prefix).encode()))
+
+    def add_codes(self, codes, n: int, on_device: bool):
+        _check(_ibs_pt_add_codes(self._h, _ptr(codes), n, int(on_device)))
+
+    def info(self):
+        i = TableInfo()
+        ns = C.c_uint32()
+        _check(_ibs_pt_info(self._h, C.byref(i), C.byref(ns)))
+        return i, ns.value
+
+    def probe(self, codes) -> np.ndarray:
+        codes = np.ascontiguousarray(codes, dtype=np.uint64)
+        masks = np.zeros(len(codes), dtype=np.uint32)
+        _check(_ibs_pt_probe(self._h, _ptr(codes), len(codes), _ptr(masks)))
+        return masks
+
+    def scan(self, ref: "Reference", W: int) -> np.ndarray:
+        k = self.info()[0].k
+        ns = self.info()[1]
+        n = window_count(ref.lens, W, k)
+        rows = np.zeros(max(n * ns, 1), dtype=WINDOW_DTYPE)
+        _check(_ibs_pt_scan(self._h, ref.handle, W, _ptr(rows), n * ns))
+        return rows[: n * ns].reshape(ns, n)
+
+    def scan_async(self, ref: "Reference", W: int, rows_dev, cap: int, stream: int = 0):
+        _check(_ibs_pt_scan_async(self._h, ref.handle, W, _ptr(rows_dev), cap, stream))
+
+    def close(self):
+        if self._h:
+            _ibs_pt_close(self._h)
+            self._h = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def table_bytes_for(n_keys: int, k: int) -> int:
+    return _ibs_table_bytes_for(n_keys, k, None)
+
+
+def device_memory(device: int = 0) -> tuple[int, int]:
+    f, t = C.c_uint64(), C.c_uint64()
+    _check(_ibs_device_memory(device, C.byref(f), C.byref(t)))
+    return f.value, t.value
 
 
 # ---------------------------------------------------------------------------
@@ -416,3 +545,66 @@ def random_sector_rate(nbytes: int) -> float:
     r = C.c_double()
     _check(_t_sector_rate(nbytes, C.byref(r)), tools=True)
     return r.value
+
+
+class Server:
+    """The serving loop (ibs_server): requests of (sample, contig, window range)."""
+
+    def __init__(self, ref: Reference, W: int, k: int, memory_budget: int = 0, max_spans_per_launch: int = 0,
+                 min_spans_per_request: int = 0, device: int = 0, one_request_per_launch: bool = False):
+        self.ref = ref
+        opts = ServerOpts(device, memory_budget, max_spans_per_launch, min_spans_per_request,
+                          int(one_request_per_launch))
+        h = vp()
+        _check(_ibs_srv_create(ref.handle, W, k, C.byref(opts), C.byref(h)))
+        self._h = h.value
+
+    def add_codes(self, codes, n: int, on_device: bool) -> int:
+        i = C.c_uint32()
+        _check(_ibs_srv_add_codes(self._h, _ptr(codes), n, int(on_device), C.byref(i)))
+        return i.value
+
+    def add_kmc(self, prefix: str) -> int:
+        i = C.c_uint32()
+        _check(_ibs_srv_add_kmc(self._h, str(prefix).encode(), C.byref(i)))
+        return i.value
+
+    def submit(self, sample: int, contig: int, first_window: int = 0, n_windows: int = 0) -> int:
+        rid = C.c_uint64()
+        _check(_ibs_srv_submit(self._h, sample, contig, first_window, n_windows, C.byref(rid)))
+        return rid.value
+
+    def poll(self, max_results: int = 64, timeout_ms: int = 0) -> list[dict]:
+        buf = (RequestResult * max_results)()
+        n = C.c_uint32()
+        _check(_ibs_srv_poll(self._h, buf, max_results, C.byref(n), timeout_ms))
+        out = []
+        for i in range(n.value):
+            r = buf[i]
+            rows = np.ctypeslib.as_array(C.cast(r.rows, C.POINTER(C.c_int32)),
+                                         shape=(max(int(r.n_windows), 1) * 6,)).copy().view(WINDOW_DTYPE)
+            out.append(dict(request_id=r.request_id, sample=r.sample, contig=r.contig,
+                            first_window=r.first_window, n_windows=r.n_windows, status=r.status,
+                            submit_time=r.submit_time, done_time=r.done_time,
+                            rows=rows[: int(r.n_windows)]))
+            _ibs_srv_release(self._h, C.byref(buf[i]))
+        return out
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(_ibs_srv_stats(self._h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in ServerStats._fields_}
+
+    def now(self) -> float:
+        return _ibs_srv_now(self._h)
+
+    def close(self):
+        if self._h:
+            _ibs_srv_close(self._h)
+            self._h = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,114 @@
+"""Autotuner of the window scan: sweeps the table layout and load (bucket
+format and keys per bucket) and the kernel launch shape (span length =
+positions per warp task, 32-position blocks in flight per lane, threads per
+CTA, CTAs per SM) on the device, times every point with CUDA events, and
+writes the sweep and its best point to gpu-ibs_b200/tuning/<gpu>.json.
+
+    python -m ibs_b200.autotune [--scale 0.25] [--out PATH]
+
+The workload is plain_2gbp scaled down (default 500 Mbp and ~5.5e8 k-mers:
+tables of several GB, far beyond L2, so a point's timing is DRAM-bound as at
+full size). `apply()` loads a committed result into the library.
+"""
+from __future__ import annotations
+
+import argparse
+import itertools
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import (PKG_DIR, Reference, Table, Tuning, get_tuning, scan_async, set_tuning, window_count)
+from . import configs
+
+TUNING_DIR = PKG_DIR / "tuning"
+
+
+def default_path() -> Path:
+    return TUNING_DIR / "b200.json"
+
+
+def apply(path: Path | None = None) -> dict | None:
+    """Loads a tuning result (the best point) into the library; returns it."""
+    path = Path(path) if path else default_path()
+    if not path.exists():
+        return None
+    best = json.loads(path.read_text())["best"]
+    set_tuning(Tuning(span_len=best["span_len"], blocks_in_flight=best["blocks_in_flight"],
+                      block_threads=best["block_threads"], ctas_per_sm=best["ctas_per_sm"],
+                      keys_per_bucket=best["keys_per_bucket"], table_format=best["table_format"]))
+    return best
+
+
+def sweep(scale: float = 0.25, reps: int = 3, quick: bool = False) -> dict:
+    import torch
+    w = configs.plain_2gbp(scale=scale)
+    k, W = w.k, w.window
+    lens = w.ref.lens
+    sw, mw = w.ref.packed_words()
+    dseq = torch.empty(sw, dtype=torch.int64, device="cuda")
+    dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
+    w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
+    bound = w.samples[0].codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
+    codes = torch.empty(bound, dtype=torch.int64, device="cuda")
+    n = w.samples[0].codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), codes.data_ptr(), bound)
+    ref = Reference(dseq.data_ptr(), dmask.data_ptr(), lens, on_device=True)
+    n_win = window_count(lens, W, k)
+    rows = torch.empty(n_win * 6, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    base = get_tuning()
+    layouts = [(1, 4.0), (4, 4.0)] if quick else [(1, 3.0), (1, 4.0), (1, 5.0), (4, 3.0), (4, 4.0), (4, 5.0)]
+    shapes = list(itertools.product([2048, 4096, 16384] if not quick else [4096],
+                                    [2, 4] if quick else [1, 2, 4, 8],
+                                    [256] if quick else [128, 256, 512],
+                                    [4, 8] if quick else [2, 4, 8, 16]))
+    points, reference_rows = [], None
+    for fmt, kpb in layouts:
+        table = Table.from_codes(codes.data_ptr(), n, k, on_device=True, force_format=fmt, keys_per_bucket=kpb)
+        info = table.info()
+        for span, nb, threads, ctas in shapes:
+            set_tuning(Tuning(span_len=span, blocks_in_flight=nb, block_threads=threads, ctas_per_sm=ctas))
+            scan_async(table, ref, W, rows.data_ptr(), n_win, stream.cuda_stream)  # plan + warm-up
+            stream.synchronize()
+            got = rows.cpu().numpy().view(np.int32).copy()
+            if reference_rows is None:
+                reference_rows = got
+            ok = bool(np.array_equal(got, reference_rows))
+            e0.record(stream)
+            for _ in range(reps):
+                scan_async(table, ref, W, rows.data_ptr(), n_win, stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            points.append(dict(table_format=fmt, keys_per_bucket=kpb, span_len=span, blocks_in_flight=nb,
+                               block_threads=threads, ctas_per_sm=ctas, ms=ms, rows_equal=ok,
+                               table_gb=info.device_bytes / 1e9, stash_keys=int(info.stash_keys)))
+        table.close()
+    set_tuning(base)
+    good = [p for p in points if p["rows_equal"]]
+    best = min(good, key=lambda p: p["ms"])
+    ref.free()
+    return {"gpu": torch.cuda.get_device_name(), "workload": w.name, "reference_bp": int(sum(map(int, lens))),
+            "sample_kmers": int(n), "reps": reps, "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
+            "best": best, "points": points}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--scale", type=float, default=0.25)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--quick", action="store_true")
+    ap.add_argument("--out", default=str(default_path()))
+    args = ap.parse_args()
+    res = sweep(args.scale, args.reps, args.quick)
+    Path(args.out).parent.mkdir(parents=True, exist_ok=True)
+    Path(args.out).write_text(json.dumps(res, indent=1) + "\n")
+    b = res["best"]
+    print(json.dumps({"best": b, "points": len(res["points"])}))
+
+
+if __name__ == "__main__":
+    main()

@@ -59,7 +59,9 @@ typedef struct ibs_reference ibs_reference; /* a device-resident 2-bit packed re
 typedef struct ibs_table_opts {
     int device;             /* CUDA device ordinal (default 0) */
     double keys_per_bucket; /* target mean keys per 32 B bucket (0 = default 4.0) */
-    uint32_t force_format;  /* 0 = automatic, 1 = B8x32, 2 = B6x40 */
+    uint32_t force_format;  /* 0 = the tuned default (ibs_tuning.table_format), 1 = B8x32,
+                               2 = B6x40, 4 = minimizer buckets (16 <= k <= 27),
+                               5 = hash buckets, B8x32 or B6x40 by size */
     uint32_t reserved[5];
 } ibs_table_opts;
 
@@ -165,6 +167,102 @@ ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit, const uint64_t
 ibs_status ibs_scan_panel(ibs_table *const *tables, uint32_t n_tables, ibs_reference *ref,
                           uint32_t W, ibs_window *rows, uint64_t cap);
 
+/* ---- joint panel tables ----------------------------------------------------
+ * One table over up to IBS_PANEL_MAX_SAMPLES samples (the reference's panel
+ * limit MAX_DBS, src/gpu/EncodeProbeCore.hpp:291): each 32-byte bucket slot
+ * holds a k-mer fingerprint and the mask of the samples that contain it, so
+ * a reference position costs one bucket load for the whole panel. Rows of
+ * every sample equal its single-sample scan. Replaces the reference's panel
+ * engine (encodeProbeMultiKernel src/gpu/EncodeProbe.cu:175-193 over the
+ * round's resident DeviceKmerIndex images, src/KmerPanel.hpp:373-439).
+ *
+ * expected_keys: the number of distinct k-mers over the panel (the union);
+ * it sizes the buckets and the overflow stash. Samples are added one at a
+ * time (sample i = the i-th call); rows are sample-major:
+ * rows[i * n_windows + w]. The scan is a persistent kernel over a work queue
+ * of (window, position-range) spans; ibs_panel_table_scan_async captures it
+ * (with its work reset and finalizer) as a CUDA graph on the first call for
+ * a (reference, W, rows, stream) and replays the graph after that. */
+#define IBS_PANEL_MAX_SAMPLES 16
+typedef struct ibs_panel_table ibs_panel_table;
+ibs_status ibs_panel_table_create(uint32_t k, uint64_t expected_keys, const ibs_table_opts *opts,
+                                  ibs_panel_table **out);
+ibs_status ibs_panel_table_add_kmc(ibs_panel_table *p, const char *kmc_prefix);
+ibs_status ibs_panel_table_add_codes(ibs_panel_table *p, const uint64_t *codes, uint64_t n,
+                                     int codes_on_device);
+ibs_status ibs_panel_table_info_get(const ibs_panel_table *p, ibs_table_info *info,
+                                    uint32_t *n_samples);
+/* Sample masks of n codes (bit i = sample i holds the k-mer). */
+ibs_status ibs_panel_table_probe(ibs_panel_table *p, const uint64_t *codes, uint64_t n,
+                                 uint32_t *masks);
+ibs_status ibs_panel_table_scan(ibs_panel_table *p, ibs_reference *ref, uint32_t W,
+                                ibs_window *rows, uint64_t cap);
+ibs_status ibs_panel_table_scan_async(ibs_panel_table *p, ibs_reference *ref, uint32_t W,
+                                      ibs_window *rows_dev, uint64_t cap, void *stream);
+void ibs_panel_table_close(ibs_panel_table *p);
+
+/* ---- serving ------------------------------------------------------------------
+ * A request loop over one resident reference (no counterpart in the
+ * reference, whose CLI scans whole references in batch): requests for
+ * different samples and window ranges arrive at any time; sample tables are
+ * admitted against a device-memory budget, evicted least-recently-used and
+ * reloaded from pinned host copies on a side stream; the loop batches
+ * continuously: every launch carries span slices of all runnable requests
+ * over their different tables, so a request submitted while others run
+ * joins the next launch, and a long request never holds back a short one. A
+ * request's rows are exactly the rows of the same windows in a full scan of
+ * its sample (alone or in any mix).
+ *
+ * The server owns a background thread; submit/poll are thread-safe. */
+typedef struct ibs_server ibs_server;
+
+typedef struct ibs_server_opts {
+    int device;
+    uint64_t memory_budget;     /* bytes of resident sample tables (0 = 80% of free memory) */
+    uint32_t max_spans_per_launch; /* 0 = 1<<15 */
+    uint32_t min_spans_per_request; /* per launch, 0 = 16 */
+    uint32_t one_request_per_launch; /* 1: no batching (every launch carries one whole request) */
+    uint32_t reserved[5];
+} ibs_server_opts;
+
+typedef struct ibs_request_result {
+    uint64_t request_id;
+    uint32_t sample, contig;
+    uint64_t first_window, n_windows; /* window indices within the contig */
+    ibs_status status;
+    double submit_time, done_time;    /* seconds on the server's clock */
+    ibs_window *rows;                 /* n_windows rows, owned by the server until released */
+} ibs_request_result;
+
+typedef struct ibs_server_stats {
+    uint64_t submitted, completed, launches, spans, probes;
+    uint64_t reloads, reload_bytes, evictions;
+    uint64_t resident_bytes, resident_tables;
+    double busy_seconds;              /* device time of the span launches */
+    double latency_p50, latency_p99, latency_max; /* seconds, completed requests */
+} ibs_server_stats;
+
+ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t k, const ibs_server_opts *opts,
+                             ibs_server **out);
+/* Registers a sample (its table is built now, copied to pinned host memory
+ * for reloads, and kept resident while the budget allows). */
+ibs_status ibs_server_add_sample_kmc(ibs_server *s, const char *kmc_prefix, uint32_t *sample_id);
+ibs_status ibs_server_add_sample_codes(ibs_server *s, const uint64_t *codes, uint64_t n,
+                                       int codes_on_device, uint32_t *sample_id);
+/* Windows [first_window, first_window + n_windows) of contig `contig`
+ * (window i starts at i * (W - k)); n_windows = 0 means to the contig's end. */
+ibs_status ibs_server_submit(ibs_server *s, uint32_t sample, uint32_t contig, uint64_t first_window,
+                             uint64_t n_windows, uint64_t *request_id);
+/* Up to max finished requests (oldest first); timeout_ms < 0 waits for one. */
+ibs_status ibs_server_poll(ibs_server *s, ibs_request_result *out, uint32_t max, uint32_t *n_out,
+                           int timeout_ms);
+/* Frees a polled result's rows. */
+void ibs_server_release(ibs_server *s, ibs_request_result *r);
+ibs_status ibs_server_stats_get(ibs_server *s, ibs_server_stats *st);
+/* Seconds on the server's clock (the clock of submit_time / done_time). */
+double ibs_server_now(ibs_server *s);
+void ibs_server_close(ibs_server *s);
+
 /* ibs_scan_noalloc: the scan of ibs_scan_async without any memory
  * allocation. No counterpart in the reference. It is for callers that cannot
  * allocate device memory while they scan: a serving process that gave all
@@ -188,6 +286,23 @@ ibs_status ibs_scan_panel(ibs_table *const *tables, uint32_t n_tables, ibs_refer
 ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev, const uint64_t *nmask_dev,
                             const uint64_t *lens, uint32_t n_contigs, uint32_t W,
                             ibs_window *rows_dev, uint64_t cap, void *stream);
+
+/* ---- tuning -------------------------------------------------------------------
+ * Launch shape of the scan kernels and the default table load, process-wide.
+ * The committed autotuner (gpu-ibs_b200/python/ibs_b200/autotune.py) sweeps
+ * these on the device and records the best in gpu-ibs_b200/tuning/. Zero
+ * fields keep the current value. */
+typedef struct ibs_tuning {
+    uint32_t span_len;         /* k-mer positions per warp task (multiple of 128) */
+    uint32_t blocks_in_flight; /* 32-position blocks each lane keeps in flight: 1, 2, 4 or 8 */
+    uint32_t block_threads;    /* threads per CTA: 128, 256 or 512 */
+    uint32_t ctas_per_sm;      /* resident CTAs per SM the grid is sized for */
+    double keys_per_bucket;    /* default load of new tables */
+    uint32_t table_format;     /* default format of new tables (0 = automatic, 4 = minimizer buckets) */
+    uint32_t reserved[3];
+} ibs_tuning;
+ibs_status ibs_set_tuning(const ibs_tuning *t);
+void ibs_get_tuning(ibs_tuning *t);
 
 /* Last error message of this thread ("" when none). */
 const char *ibs_last_error(void);

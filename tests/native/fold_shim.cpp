@@ -52,3 +52,71 @@ extern "C" uint64_t hash_collisions(uint32_t bits)
     delete[] seen;
     return coll;
 }
+
+// ---- minimizer-bucketed table (gpu-ibs_b200/csrc/mz_core.cuh) -------------
+#include "mz_core.cuh"
+
+static TableGeom mz_geom(uint32_t k, uint64_t nBuckets)
+{
+    TableGeom g{};
+    g.k = k;
+    g.bits = 2 * k;
+    g.format = FMT_MZ8;
+    g.nBuckets = nBuckets;
+    g.fpBits = 32 - (63 - __builtin_clzll(nBuckets));
+    return g;
+}
+
+// Build side: bucket and slot of canonical codes.
+extern "C" void mz_locate(const uint64_t *codes, uint64_t n, uint32_t k, uint64_t nBuckets,
+                          uint64_t *bucket, uint32_t *slot)
+{
+    const TableGeom g = mz_geom(k, nBuckets);
+    for (uint64_t i = 0; i < n; ++i)
+        mz::locate(codes[i], g, bucket[i], slot[i]);
+}
+
+// Query side as the scan kernel computes it: along the forward strand of
+// `bases` (values 0-3), 16-mer hashes per position, the window minimum over
+// the next w hashes with its leftmost/rightmost offsets, the strand of the
+// canonical k-mer, then bucket and slot. Positions 0..n-k.
+extern "C" void mz_query(const uint8_t *bases, uint64_t n, uint32_t k, uint64_t nBuckets,
+                         uint64_t *bucket, uint32_t *slot)
+{
+    const TableGeom g = mz_geom(k, nBuckets);
+    const uint32_t w = mz::w_of(k);
+    if (n < k)
+        return;
+    const uint64_t nm = n - mz::M + 1;
+    uint32_t *h = new uint32_t[nm];
+    for (uint64_t q = 0; q < nm; ++q) {
+        uint32_t f = 0;
+        for (uint32_t t = 0; t < mz::M; ++t)
+            f = (f << 2) | bases[q + t];
+        h[q] = mz::hash16(mz::canon16(f));
+    }
+    const uint64_t kmask = key_mask(2 * k);
+    for (uint64_t q = 0; q + k <= n; ++q) {
+        uint64_t fwd = 0, rc = 0;
+        for (uint32_t t = 0; t < k; ++t) {
+            fwd = (fwd << 2) | bases[q + t];
+            rc |= (uint64_t)(3 - bases[q + t]) << (2 * t);
+        }
+        rc &= kmask;
+        const bool isFwd = fwd <= rc;
+        const uint64_t C = isFwd ? fwd : rc;
+        uint32_t mn = 0xffffffffu, jl = 0, jr = 0;
+        for (uint32_t j = 0; j < w; ++j) {
+            const uint32_t v = h[q + j];
+            if (v < mn || j == 0) {
+                mn = v;
+                jl = jr = j;
+            } else if (v == mn)
+                jr = j;
+        }
+        const uint32_t o = isFwd ? jl : (w - 1 - jr);
+        bucket[q] = mz::bucket_of_h(mn, g.nBuckets);
+        slot[q] = mz::slot_value(mz::slot_high(C, k, o), mn, g.fpBits);
+    }
+    delete[] h;
+}

@@ -1,0 +1,83 @@
+"""The joint panel table: one bucket load per position for up to 16 samples,
+every sample's rows equal to its single-sample scan."""
+import numpy as np
+import pytest
+
+import corpus
+import ibs_b200 as ib
+import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _samples(ref_spec, seq, mask, n, k=25):
+    out = []
+    for s in range(n):
+        smp = ib.SampleSpec(seed=900 + s, k=k, class_rate=(0.0001, 0.005, 0.02, 0.05),
+                            class_prob=(0.2, 0.4, 0.3, 0.1), block_len=20_000,
+                            present_frac=0.3 + 0.7 * ((s * 7) % 10) / 10, random_frac=0.05)
+        out.append(np.unique(smp.codes_host(ref_spec, seq, mask)))
+    return out
+
+
+@pytest.mark.parametrize("n_samples,k", [(1, 25), (5, 25), (16, 25), (16, 31)])
+def test_panel_rows_equal_single_scans(n_samples, k):
+    ref_spec = ib.RefSpec(seed=77, lens=[400_000, 123_457, 24, 31, 90_000], n_frac=0.003,
+                          n_run=(1, 200), lower_frac=0.02)
+    seq, mask = ref_spec.reference_host()
+    samples = _samples(ref_spec, seq, mask, n_samples, k)
+    union = len(np.unique(np.concatenate(samples)))
+    pt = ib.PanelTable(k, union)
+    for c in samples:
+        pt.add_codes(c, len(c), on_device=False)
+    info, ns = pt.info()
+    assert ns == n_samples
+    # masks against set membership
+    rng = np.random.default_rng(3)
+    q = np.concatenate([rng.choice(np.concatenate(samples), 20_000), corpus.random_codes(rng, 20_000, k)])
+    masks = pt.probe(q)
+    want = np.zeros(len(q), np.uint32)
+    for i, c in enumerate(samples):
+        want |= np.isin(q, c).astype(np.uint32) << np.uint32(i)
+    assert np.array_equal(masks, want)
+    ref = ib.Reference(seq, mask, ref_spec.lens)
+    W = 5000
+    panel = pt.scan(ref, W)
+    import torch
+    n = ib.window_count(ref_spec.lens, W, k)
+    dev = torch.zeros(max(n * ns, 1) * 6, dtype=torch.int32, device="cuda")
+    st = torch.cuda.Stream()
+    for _ in range(3):  # capture, then graph replays
+        dev.zero_()
+        pt.scan_async(ref, W, dev.data_ptr(), n * ns, st.cuda_stream)
+        st.synchronize()
+        again = dev[: n * ns * 6].cpu().numpy().view(ib.WINDOW_DTYPE).reshape(ns, n)
+        assert np.array_equal(again, panel)
+    for i, c in enumerate(samples):
+        t = ib.Table.from_codes(c, len(c), k, on_device=False)
+        single = ib.scan(t, ref, W)
+        assert np.array_equal(panel[i], single), f"sample {i}"
+        t.close()
+    pt.close()
+
+
+def test_panel_from_kmc_matches_goldens(build_case):
+    names = ["edge_k25", "edge_k25_kmc1", "plain_1mbp"]
+    cases = [build_case(n) for n in names]
+    ixs = [orc.Index(str(c["prefix"])) for c in cases]
+    union = len(np.unique(np.concatenate([ix.list_codes() for ix in ixs])))
+    pt = ib.PanelTable(25, union, keys_per_bucket=4.5)  # a dense table: the stash is used
+    for c in cases:
+        pt.add_kmc(str(c["prefix"]))
+    # each golden case's reference against the whole panel: its own sample's rows match its golden
+    for i, (name, c) in enumerate(zip(names, cases)):
+        gold = corpus.load_golden(name)
+        ids, seqs = orc.read_sequence_file(str(c["ref"]))
+        seq, mask, lens = ib.pack_ascii(seqs)
+        ref = ib.Reference(seq, mask, lens)
+        W = c["windows"][0]
+        rows = pt.scan(ref, W)
+        assert orc.tsv_text(ids, [len(s) for s in seqs], rows[i], W, 25) == gold["tsv"][str(W)]
+        for j, ix in enumerate(ixs):
+            assert np.array_equal(rows[j], orc.scan(ix, seqs, W, 25, threads=4))
+    pt.close()

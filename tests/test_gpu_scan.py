@@ -160,3 +160,45 @@ def test_scan_argument_errors(build_case):
     assert e.value.status == 1
     empty = ib.Reference(*ib.pack_ascii([b""])[:2], np.array([0], np.uint64))
     assert len(ib.scan(t, empty, 1000)) == 0
+
+
+@pytest.mark.parametrize("name", ["edge_k25", "edge_k25_kmc1", "edge_k25_crlf", "plain_1mbp", "edge_k25_gz"])
+def test_minimizer_table_matches_reference_golden(name, build_case):
+    gold = corpus.load_golden(name)
+    case = build_case(name)
+    t = ib.Table.open(str(case["prefix"]), force_format=4)
+    info = t.info()
+    assert info.format == 4
+    ix = orc.Index(str(case["prefix"]))
+    assert t.probe(ix.list_codes()).all()
+    q = corpus.random_codes(np.random.default_rng(6), 100_000, case["k"])
+    assert np.array_equal(t.probe(q), ix.probe(q))
+    for W in case["windows"]:
+        for path in ("resident", "packed"):
+            ids, lens, rows = rows_of_case(case, t, W, path)
+            assert tsv_of(ids, lens, rows, W, case["k"]) == gold["tsv"][str(W)], (name, W, path)
+    t.close()
+
+
+def test_minimizer_table_40mbp_and_overflow(tmp_path):
+    from ibs_b200 import configs
+    w = configs.plain_2gbp(scale=0.02)
+    case = corpus.build_workload(w, tmp_path)
+    ix = orc.Index(str(case["prefix"]))
+    ids, seqs = orc.read_sequence_file(str(case["ref"]))
+    want = orc.scan(ix, seqs, w.window, w.k, threads=16)
+    seq, mask, lens = ib.pack_ascii(seqs)
+    ref = ib.Reference(seq, mask, lens)
+    for kpb in (4.0, 7.0):  # 7 keys per bucket forces overflow into the stash
+        t = ib.Table.open(str(case["prefix"]), force_format=4, keys_per_bucket=kpb)
+        if kpb == 7.0:
+            assert t.info().stash_keys > 0
+        assert np.array_equal(ib.scan(t, ref, w.window), want)
+        t.close()
+
+
+def test_minimizer_format_rejects_unsupported_k(build_case):
+    case = build_case("edge_k31")
+    with pytest.raises(ib.IbsError) as e:
+        ib.Table.open(str(case["prefix"]), force_format=4)
+    assert e.value.status == 6

@@ -1,0 +1,103 @@
+"""The serving loop: every request's rows equal the same windows of a full
+single-sample scan, alone and in a concurrent mix, with tables evicted and
+reloaded under a memory budget."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import ibs_b200 as ib
+
+pytestmark = pytest.mark.gpu
+
+W, K = 5000, 25
+
+
+@pytest.fixture(scope="module")
+def world():
+    ref_spec = ib.RefSpec(seed=321, lens=[3_000_000, 1_500_000, 700_000, 24, 0, 250_000], n_frac=0.002,
+                          n_run=(1, 300))
+    seq, mask = ref_spec.reference_host()
+    ref = ib.Reference(seq, mask, ref_spec.lens)
+    samples = []
+    for s in range(6):
+        smp = ib.SampleSpec(seed=500 + s, k=K, class_rate=(0.0001, 0.005, 0.02, 0.05),
+                            class_prob=(0.2, 0.4, 0.3, 0.1), block_len=50_000, present_frac=0.4 + 0.1 * s,
+                            random_frac=0.05)
+        samples.append(smp.codes_host(ref_spec, seq, mask))
+    # the full single-sample scans, alone
+    full = []
+    for c in samples:
+        t = ib.Table.from_codes(c, len(c), K, on_device=False)
+        full.append(ib.scan(t, ref, W))
+        t.close()
+    starts = np.concatenate([[0], np.cumsum([ib.window_count(ref_spec.lens[:i + 1], W, K) -
+                                             ib.window_count(ref_spec.lens[:i], W, K)
+                                             for i in range(len(ref_spec.lens))])])
+    yield dict(ref=ref, ref_spec=ref_spec, samples=samples, full=full, starts=starts)
+    ref.free()
+
+
+def expected(world, r):
+    rows = world["full"][r["sample"]]
+    a = world["starts"][r["contig"]] + r["first_window"]
+    return rows[a:a + r["n_windows"]]
+
+
+def make_server(world, budget_tables=2.5):
+    sizes = [ib.table_bytes_for(len(c), K) for c in world["samples"]]
+    budget = int(max(sizes) * budget_tables)
+    srv = ib.Server(world["ref"], W, K, memory_budget=budget, max_spans_per_launch=512, min_spans_per_request=8)
+    ids = [srv.add_codes(c, len(c), on_device=False) for c in world["samples"]]
+    assert ids == list(range(len(world["samples"])))
+    return srv
+
+
+def random_requests(world, n, seed):
+    rng = np.random.default_rng(seed)
+    lens = world["ref_spec"].lens
+    reqs = []
+    for _ in range(n):
+        c = int(rng.integers(0, len(lens)))
+        nw = ib.window_count(lens[c:c + 1], W, K)
+        first = int(rng.integers(0, max(nw, 1)))
+        cnt = int(rng.integers(1, max(nw - first, 1) + 1)) if nw else 0
+        reqs.append((int(rng.integers(0, len(world["samples"]))), c, first, cnt))
+    return reqs
+
+
+def test_requests_alone_equal_full_scan_rows(world):
+    srv = make_server(world)
+    for req in random_requests(world, 25, 1):
+        srv.submit(*req)
+        (r,) = srv.poll(1, timeout_ms=-1)
+        assert r["status"] == 0
+        assert np.array_equal(r["rows"], expected(world, r)), req
+    srv.close()
+
+
+def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world):
+    srv = make_server(world, budget_tables=2.2)
+    reqs = random_requests(world, 300, 2) + [(s, 0, 0, 0) for s in range(6)]  # whole-contig requests too
+    done = []
+
+    def producer():
+        rng = np.random.default_rng(9)
+        for req in reqs:
+            srv.submit(*req)
+            time.sleep(float(rng.exponential(0.0005)))
+
+    th = threading.Thread(target=producer)
+    th.start()
+    while len(done) < len(reqs):
+        done += srv.poll(64, timeout_ms=2000)
+    th.join()
+    for r in done:
+        assert r["status"] == 0
+        assert np.array_equal(r["rows"], expected(world, r)), (r["sample"], r["contig"], r["first_window"])
+    st = srv.stats()
+    assert st["completed"] == len(reqs)
+    assert st["evictions"] > 0 and st["reloads"] > 0, st
+    assert st["latency_p99"] >= st["latency_p50"] > 0
+    srv.close()

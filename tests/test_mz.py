@@ -1,0 +1,65 @@
+"""The minimizer-bucketed table's key map (gpu-ibs_b200/csrc/mz_core.cuh,
+compiled for the host): the scan kernel's query-side computation equals the
+build-side one on every position of either strand, and (bucket, slot)
+identifies a k-mer exactly."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import corpus
+
+vp = ctypes.c_void_p
+
+
+def _ptr(a):
+    return a.ctypes.data_as(vp)
+
+
+def locate(shim, codes, k, nb):
+    codes = np.ascontiguousarray(codes, np.uint64)
+    b = np.zeros(len(codes), np.uint64)
+    s = np.zeros(len(codes), np.uint32)
+    shim.mz_locate(_ptr(codes), ctypes.c_uint64(len(codes)), ctypes.c_uint32(k), ctypes.c_uint64(nb),
+                   _ptr(b), _ptr(s))
+    return b, s
+
+
+def query(shim, bases, k, nb):
+    bases = np.ascontiguousarray(bases, np.uint8)
+    n = max(len(bases) - k + 1, 0)
+    b = np.zeros(n, np.uint64)
+    s = np.zeros(n, np.uint32)
+    shim.mz_query(_ptr(bases), ctypes.c_uint64(len(bases)), ctypes.c_uint32(k), ctypes.c_uint64(nb),
+                  _ptr(b), _ptr(s))
+    return b, s
+
+
+@pytest.mark.parametrize("k", [16, 21, 25, 27])
+def test_query_side_equals_build_side(native_shim, k):
+    rng = np.random.default_rng(k)
+    nb = 1 << max(2 * k - 26, 20)
+    # random sequence plus repeats that force minimizer ties
+    seq = rng.integers(0, 4, 200_000).astype(np.uint8)
+    unit = rng.integers(0, 4, 17).astype(np.uint8)
+    seq[5000:5000 + 17 * 40] = np.tile(unit, 40)
+    seq[9000:9200] = 0
+    rc = (3 - seq[::-1]).copy()
+    for s_ in (seq, rc):
+        qb, qs = query(native_shim, s_, k, nb)
+        text = bytes(np.frombuffer(b"ACGT", np.uint8)[s_])
+        codes = corpus.canonical_codes_np(text, k)
+        lb, ls = locate(native_shim, codes, k, nb)
+        assert np.array_equal(qb, lb) and np.array_equal(qs, ls)
+
+
+@pytest.mark.parametrize("k", [20, 25, 27])
+def test_bucket_and_slot_identify_the_kmer(native_shim, k):
+    rng = np.random.default_rng(100 + k)
+    nb = 1 << max(2 * k - 26, 18)
+    codes = np.unique(corpus.random_codes(rng, 400_000, k))
+    b, s = locate(native_shim, codes, k, nb)
+    assert (b < nb).all()
+    assert (s < (1 << 31)).all(), "slot values must stay below the B8x32 sentinels"
+    pairs = b.astype(np.uint64) * np.uint64(1 << 32) + s.astype(np.uint64)
+    assert len(np.unique(pairs)) == len(codes)
