@@ -286,7 +286,8 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
     torch.cuda.synchronize()
     t_gen = time.time() - t0
     t0 = time.time()
-    table = ib.Table.from_codes(dcodes.data_ptr(), n_codes, k, on_device=True, device=dev)
+    table = ib.Table.from_codes(dcodes.data_ptr(), n_codes, k, on_device=True, device=dev,
+                                force_format=args.table_format, keys_per_bucket=args.keys_per_bucket)
     info = table.info()
     t_build = time.time() - t0
     log(f"[bench r{rank}] generated {sum(map(int, lens)) / 1e9:.3f} Gbp + {n_codes / 1e9:.3f}e9 k-mers "
@@ -422,9 +423,12 @@ def panel_arm(args, rank: int):
     w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
     ref = ib.Reference(dseq.data_ptr(), dmask.data_ptr(), lens, on_device=True)
 
+    def sample_codes_bound(i):
+        return w.samples[i].codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
+
     def sample_codes(i):
         smp = w.samples[i]
-        bound = smp.codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
+        bound = sample_codes_bound(i)
         buf = torch.empty(bound, dtype=torch.int64, device="cuda")
         n = smp.codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), buf.data_ptr(), bound)
         return buf, n
@@ -440,8 +444,6 @@ def panel_arm(args, rank: int):
         sampled.append(torch.unique(sel))
         del buf, v, sel
         torch.cuda.empty_cache()
-    union_est = int(torch.unique(torch.cat(sampled)).numel() * 64 * 1.02) + (1 << 20)
-    del sampled
     # plain path: one table and one scan launch per sample (scan time only)
     stream = torch.cuda.Stream()
     rows_single = torch.empty(max(n_win, 1) * 6, dtype=torch.int32, device="cuda")
@@ -461,40 +463,83 @@ def panel_arm(args, rank: int):
         plain_ms += e0.elapsed_time(e1)
         singles.append(rows_single[: n_win * 6].cpu().numpy().view(ib.WINDOW_DTYPE).copy())
         t.close()
-    # batched: one joint table, graph-replayed scans
-    pt = ib.PanelTable(k, union_est)
+    del rows_single
+    torch.cuda.empty_cache()
+
+    # batched: joint tables of as many samples as fit next to the build's
+    # scratch (one sample's codes); all 16 in one table when memory allows
+    kpb = args.panel_keys_per_bucket
+    free, _ = torch.cuda.mem_get_info()
+    max_codes = max(sample_codes_bound(i) for i in range(len(w.samples))) * 8
+    rows_bytes = n_win * len(w.samples) * 24 + 64 * n_win * len(w.samples)
+    budget = free - max_codes - (2 << 30) * 2 - rows_bytes - (6 << 30)
+
+    union_of = {}
+
+    def joint_bytes(members):
+        u = int(torch.unique(torch.cat([sampled[j] for j in members])).numel() * 64 * 1.02) + (1 << 20)
+        union_of[tuple(members)] = u
+        return u / kpb * 32 * 1.15
+
+    groups, cur = [], []
     for i in range(len(w.samples)):
-        buf, n = sample_codes(i)
-        pt.add_codes(buf.data_ptr(), n, on_device=True)
-        del buf
+        if cur and joint_bytes(cur + [i]) > budget:
+            groups.append(cur)
+            cur = []
+        cur.append(i)
+    groups.append(cur)
+    for members in groups:
+        joint_bytes(members)
+    log(f"[panel] {len(groups)} joint table group(s) {groups} under a {budget / 1e9:.1f} GB budget; "
+        f"union estimates {[union_of[tuple(m)] for m in groups]}")
+    del sampled
+    panel_ms, launches, table_gb, union_est, got = 0.0, 0, [], [], [None] * len(w.samples)
+    build_s = 0.0
+    for members in groups:
+        tb = time.time()
+        pt = ib.PanelTable(k, union_of[tuple(members)], keys_per_bucket=kpb)
+        for i in members:
+            buf, n = sample_codes(i)
+            pt.add_codes(buf.data_ptr(), n, on_device=True)
+            del buf
+            torch.cuda.empty_cache()
+        info, ns = pt.info()
+        build_s += time.time() - tb
+        table_gb.append(info.device_bytes / 1e9)
+        union_est.append(union_of[tuple(members)])
+        rows = torch.empty(max(n_win * ns, 1) * 6, dtype=torch.int32, device="cuda")
+        for _ in range(args.warmup):
+            pt.scan_async(ref, W, rows.data_ptr(), n_win * ns, stream.cuda_stream)
+        stream.synchronize()
+        launches0 = ib.launch_count()
+        e0.record(stream)
+        for _ in range(args.steps):
+            pt.scan_async(ref, W, rows.data_ptr(), n_win * ns, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        panel_ms += e0.elapsed_time(e1) / args.steps
+        launches += ib.launch_count() - launches0
+        g = rows[: n_win * ns * 6].cpu().numpy().view(ib.WINDOW_DTYPE).reshape(ns, n_win)
+        for j, i in enumerate(members):
+            got[i] = g[j].copy()
+        del rows
+        pt.close()
         torch.cuda.empty_cache()
-    info, ns = pt.info()
     t_build = time.time() - t0
-    rows = torch.empty(max(n_win * ns, 1) * 6, dtype=torch.int32, device="cuda")
-    for _ in range(args.warmup):
-        pt.scan_async(ref, W, rows.data_ptr(), n_win * ns, stream.cuda_stream)
-    stream.synchronize()
-    launches0 = ib.launch_count()
-    e0.record(stream)
-    for _ in range(args.steps):
-        pt.scan_async(ref, W, rows.data_ptr(), n_win * ns, stream.cuda_stream)
-    e1.record(stream)
-    e1.synchronize()
-    panel_ms = e0.elapsed_time(e1) / args.steps
-    launches = ib.launch_count() - launches0
-    got = rows[: n_win * ns * 6].cpu().numpy().view(ib.WINDOW_DTYPE).reshape(ns, n_win)
+    ns = len(w.samples)
     mismatched = [i for i in range(ns) if not np.array_equal(got[i], singles[i])]
     assert not mismatched, f"panel rows differ from single-sample rows for samples {mismatched}"
     probes = positions * ns
     out = {"workload": w.name, "samples": ns, "sample_kmers": sizes, "k": k, "window": W,
            "reference_bp": int(sum(map(int, lens))), "positions": int(positions),
-           "union_keys_estimate": union_est, "joint_table_gb": info.device_bytes / 1e9,
-           "build_s": t_build,
+           "groups": groups, "union_keys_estimate": union_est, "joint_table_gb": table_gb,
+           "keys_per_bucket": kpb, "build_s": build_s, "setup_s": t_build,
            "batched_probes_per_s": probes / (panel_ms * 1e-3), "batched_ms_per_scan": panel_ms,
            "plain_probes_per_s": probes / (plain_ms * 1e-3), "plain_ms_all_samples": plain_ms,
            "speedup_vs_plain": plain_ms / panel_ms, "graph_launches_per_scan": launches / args.steps,
-           "rows_equal_single_sample": True}
-    pt.close()
+           "rows_equal_single_sample": True,
+           "note": "batched = joint tables (one per group; one group when all samples fit), each scan a "
+                   "replayed CUDA graph; plain = one table and one scan launch per sample; scan time only"}
     ref.free()
     return out
 
@@ -675,10 +720,14 @@ def main():
     ap.add_argument("--cpu-slice", type=int, default=50_000_000, help="bases per CPU-baseline slice")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--table-format", type=int, default=0,
+                    help="sample table layout: 0 library default, 1 B8x32, 2 B6x40, 4 minimizer-bucketed")
+    ap.add_argument("--keys-per-bucket", type=float, default=0.0, help="table load (0: library default)")
     ap.add_argument("--panel", action="store_true", help="also measure the 16-sample batched panel")
     ap.add_argument("--panel-only", action="store_true")
     ap.add_argument("--panel-samples", type=int, default=16)
     ap.add_argument("--panel-scale", type=float, default=1.0)
+    ap.add_argument("--panel-keys-per-bucket", type=float, default=3.0)
     ap.add_argument("--serve", action="store_true", help="also measure the served request stream")
     ap.add_argument("--serve-only", action="store_true")
     ap.add_argument("--serve-samples", type=int, default=16)

@@ -20,6 +20,7 @@
 #include "scan_device.cuh"
 
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <memory>
 
@@ -31,6 +32,7 @@ constexpr uint32_t kSlots = 5;
 constexpr uint32_t kSpanLen = 8192;
 constexpr int kNB = 4;
 constexpr uint64_t kStashEmpty = ~0ull;
+constexpr uint64_t kBuildChunk = 1ull << 27; // keys per build step (1 GiB of scratch each way)
 
 struct View {
     TableGeom g;
@@ -141,7 +143,7 @@ __global__ void k_find(View t, uint32_t *words, unsigned long long *stashWords, 
 }
 
 __global__ void k_insert(View t, uint32_t *words, unsigned long long *stashWords, const uint64_t *codes,
-                         uint64_t n, uint32_t bit, int *err)
+                         uint64_t n, uint32_t bit, uint64_t *failed, unsigned long long *nFailed)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
@@ -181,6 +183,32 @@ __global__ void k_insert(View t, uint32_t *words, unsigned long long *stashWords
                 }
             }
             b = (b + 1) & (t.stashBuckets - 1);
+        }
+        if (!placed) // the stash is full: the host grows it and inserts these again
+            failed[atomicAdd(nFailed, 1ull)] = code;
+    }
+}
+
+// Moves every stash entry into a larger stash (the build's stash growth).
+__global__ void k_stash_move(const ulonglong2 *old, uint64_t oldEntries, unsigned long long *fresh,
+                             uint64_t freshBuckets, int *err)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < oldEntries;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const ulonglong2 e = old[i];
+        if (e.x == kStashEmpty)
+            continue;
+        uint64_t b = stash_home(e.x, freshBuckets);
+        bool placed = false;
+        for (uint64_t s = 0; s < freshBuckets && !placed; ++s) {
+            for (int j = 0; j < 2 && !placed; ++j) {
+                unsigned long long *entry = fresh + 4 * b + 2 * j;
+                if (atomicCAS(entry, kStashEmpty, (unsigned long long)e.x) == kStashEmpty) {
+                    entry[1] = e.y;
+                    placed = true;
+                }
+            }
+            b = (b + 1) & (freshBuckets - 1);
         }
         if (!placed)
             atomicExch(err, 1);
@@ -357,6 +385,21 @@ int grid_for(uint64_t n)
     return (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 16));
 }
 
+// Expected fraction of keys beyond a bucket's kSlots slots when the keys per
+// bucket are Poisson(lam).
+double overflow_fraction(double lam)
+{
+    if (lam <= 0)
+        return 0;
+    double p = std::exp(-lam), over = 0;
+    for (int x = 0; x < 400; ++x) {
+        if (x > (int)kSlots)
+            over += (x - (int)kSlots) * p;
+        p *= lam / (x + 1);
+    }
+    return over / lam;
+}
+
 uint64_t next_pow2(uint64_t x)
 {
     uint64_t p = 1;
@@ -382,7 +425,8 @@ struct ibs_panel_table {
     uint64_t deviceBytes = 0;
     double buildSeconds = 0;
     int *dErr = nullptr;
-    unsigned long long *dCounters = nullptr; // [0] pending count, [1] scan work counter
+    unsigned long long *dCounters = nullptr; // [0] pending count, [1] scan work counter, [2] failed
+    uint32_t stashGrowths = 0;
     // scan plan and scratch
     const ibs_reference *planRef = nullptr;
     std::vector<uint64_t> planLens;
@@ -424,7 +468,10 @@ extern "C" ibs_status ibs_panel_table_create(uint32_t k, uint64_t expected_keys,
         nb = std::min<uint64_t>(nb, 1ull << g.bits);
     g.nBuckets = nb;
     g.fpBits = (uint32_t)std::max<int>(1, (int)g.bits - (int)(63 - __builtin_clzll(nb)));
-    p->stashBuckets = next_pow2(std::max<uint64_t>(1u << 16, (uint64_t)(expected_keys * 0.06) / 2 + 1));
+    // keys per bucket are ~Poisson(expected / nBuckets); the stash holds the
+    // expected overflow at <= 2/3 load (it grows during the build if needed)
+    const double over = (double)expected_keys * overflow_fraction((double)expected_keys / (double)nb);
+    p->stashBuckets = next_pow2(std::max<uint64_t>(1u << 12, (uint64_t)(over * 0.75) + 1));
     g.stashBuckets = p->stashBuckets;
     IBS_CUDA(cudaMalloc(&p->buckets, nb * 32), "panel table alloc");
     IBS_CUDA(cudaMemset(p->buckets, 0, nb * 32), "panel table init");
@@ -434,9 +481,38 @@ extern "C" ibs_status ibs_panel_table_create(uint32_t k, uint64_t expected_keys,
     IBS_CUDA(cudaGetLastError(), "panel stash init");
     IBS_CUDA(cudaMalloc(&p->dErr, sizeof(int)), "panel alloc");
     IBS_CUDA(cudaMemset(p->dErr, 0, sizeof(int)), "panel alloc");
-    IBS_CUDA(cudaMalloc(&p->dCounters, 16), "panel alloc");
+    IBS_CUDA(cudaMalloc(&p->dCounters, 32), "panel alloc");
     p->deviceBytes = nb * 32 + p->stashBuckets * 32;
     *out = p.release();
+    return IBS_OK;
+}
+
+// Doubles the stash and moves its entries over.
+static ibs_status grow_stash(ibs_panel_table *p)
+{
+    const uint64_t nb = p->stashBuckets * 2;
+    ulonglong2 *fresh = nullptr;
+    IBS_CUDA(cudaMalloc(&fresh, nb * 32), "panel stash growth");
+    std::unique_ptr<ulonglong2, cudaError_t (*)(void *)> guard(fresh, cudaFree);
+    k_stash_init<<<grid_for(nb * 2), 256>>>(fresh, nb * 2);
+    IBS_LAUNCHED();
+    IBS_CUDA(cudaMemset(p->dErr, 0, sizeof(int)), "panel stash growth");
+    k_stash_move<<<grid_for(p->stashBuckets * 2), 256>>>(p->stash, p->stashBuckets * 2,
+                                                         reinterpret_cast<unsigned long long *>(fresh), nb,
+                                                         p->dErr);
+    IBS_LAUNCHED();
+    int err = 0;
+    IBS_CUDA(cudaMemcpy(&err, p->dErr, sizeof(int), cudaMemcpyDeviceToHost), "panel stash growth");
+    if (err) { // cannot happen: the new stash has twice the entries
+        set_error("panel table: stash growth lost entries");
+        return IBS_ERR_STATE;
+    }
+    cudaFree(p->stash);
+    p->stash = guard.release();
+    p->deviceBytes += p->stashBuckets * 32;
+    p->stashBuckets = nb;
+    p->geom.stashBuckets = nb;
+    p->stashGrowths++;
     return IBS_OK;
 }
 
@@ -452,28 +528,46 @@ static ibs_status panel_add_device_codes(ibs_panel_table *p, const uint64_t *dCo
         cudaGraphExecDestroy(p->graph);
         p->graph = nullptr;
     }
-    uint64_t *pending = nullptr;
-    IBS_CUDA(cudaMalloc(&pending, std::max<uint64_t>(n, 1) * 8), "panel pending alloc");
-    std::unique_ptr<uint64_t, cudaError_t (*)(void *)> guard(pending, cudaFree);
-    IBS_CUDA(cudaMemset(p->dCounters, 0, 8), "panel build");
-    View v = p->view();
-    uint32_t *words = reinterpret_cast<uint32_t *>(p->buckets);
-    unsigned long long *stashWords = reinterpret_cast<unsigned long long *>(p->stash);
-    if (n) {
-        k_find<<<grid_for(n), 256>>>(v, words, stashWords, dCodes, n, bit, pending, p->dCounters);
+    // keys go in chunks, so the build's scratch stays small next to the table
+    const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(n, kBuildChunk));
+    uint64_t *pending = nullptr, *failed = nullptr;
+    IBS_CUDA(cudaMalloc(&pending, chunk * 8), "panel pending alloc");
+    std::unique_ptr<uint64_t, cudaError_t (*)(void *)> g1(pending, cudaFree);
+    IBS_CUDA(cudaMalloc(&failed, chunk * 8), "panel pending alloc");
+    std::unique_ptr<uint64_t, cudaError_t (*)(void *)> g2(failed, cudaFree);
+    unsigned long long *cnt = p->dCounters; // [0] pending, [2] failed
+    for (uint64_t c0 = 0; c0 < n; c0 += chunk) {
+        const uint64_t m = std::min<uint64_t>(chunk, n - c0);
+        IBS_CUDA(cudaMemset(cnt, 0, 8), "panel build");
+        View v = p->view();
+        k_find<<<grid_for(m), 256>>>(v, reinterpret_cast<uint32_t *>(p->buckets),
+                                     reinterpret_cast<unsigned long long *>(p->stash), dCodes + c0, m, bit,
+                                     pending, cnt);
         IBS_LAUNCHED();
-    }
-    unsigned long long nPend = 0;
-    IBS_CUDA(cudaMemcpy(&nPend, p->dCounters, 8, cudaMemcpyDeviceToHost), "panel build find");
-    if (nPend) {
-        k_insert<<<grid_for(nPend), 256>>>(v, words, stashWords, pending, nPend, bit, p->dErr);
-        IBS_LAUNCHED();
-    }
-    int err = 0;
-    IBS_CUDA(cudaMemcpy(&err, p->dErr, sizeof(int), cudaMemcpyDeviceToHost), "panel build insert");
-    if (err) {
-        set_error("panel table: stash full (raise expected_keys)");
-        return IBS_ERR_CAPACITY;
+        unsigned long long nPend = 0;
+        IBS_CUDA(cudaMemcpy(&nPend, cnt, 8, cudaMemcpyDeviceToHost), "panel build find");
+        const uint64_t *todo = pending;
+        for (int round = 0; nPend; ++round) {
+            if (round > 40) { // each round doubles the stash: 2^40 x its start is out of reach
+                set_error("panel table: stash growth did not converge");
+                return IBS_ERR_STATE;
+            }
+            IBS_CUDA(cudaMemset(cnt + 2, 0, 8), "panel build");
+            View w = p->view();
+            k_insert<<<grid_for(nPend), 256>>>(w, reinterpret_cast<uint32_t *>(p->buckets),
+                                               reinterpret_cast<unsigned long long *>(p->stash), todo, nPend,
+                                               bit, todo == failed ? pending : failed, cnt + 2);
+            IBS_LAUNCHED();
+            unsigned long long nFail = 0;
+            IBS_CUDA(cudaMemcpy(&nFail, cnt + 2, 8, cudaMemcpyDeviceToHost), "panel build insert");
+            if (!nFail)
+                break;
+            ibs_status st = grow_stash(p);
+            if (st != IBS_OK)
+                return st;
+            todo = todo == failed ? pending : failed;
+            nPend = nFail;
+        }
     }
     p->nSamples++;
     p->keysAdded += n;

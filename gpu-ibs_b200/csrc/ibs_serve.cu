@@ -272,10 +272,17 @@ struct ibs_server {
 
 namespace {
 
+bool table_ready(Sample &smp);
+
 ibs_status make_resident(ibs_server *s, Sample &smp)
 {
     if (smp.dev)
         return IBS_OK;
+    // a finished reload makes its table evictable, whether or not a request
+    // has looked at it since (tables loaded at registration included)
+    for (auto &o : s->samples)
+        if (o->dev && o->loading)
+            table_ready(*o);
     // evict least-recently-used idle tables until this one fits
     while (s->resident + smp.bytes() > s->budget) {
         Sample *victim = nullptr;
@@ -384,14 +391,23 @@ bool iterate(ibs_server *s)
             s->queue.pop_front();
         }
         const double t = s->now();
+        std::vector<Request *> failed;
         for (auto &rp : s->active) {
             Request *r = rp.get();
             if (r->curWin == r->nw)
                 continue; // every span issued; its finalize is in flight
             Sample &smp = *s->samples[r->sample];
-            if (!smp.dev && make_resident(s, smp) != IBS_OK) {
-                cudaGetLastError();
-                continue;
+            if (!smp.dev) {
+                const ibs_status rs = make_resident(s, smp);
+                if (rs == IBS_ERR_STATE)
+                    continue; // every resident table is busy: retry after a retire
+                if (rs != IBS_OK) {
+                    // a table that is not resident has no launch in flight,
+                    // so none of this request's spans is on the device
+                    cudaGetLastError();
+                    failed.push_back(r);
+                    continue;
+                }
             }
             if (!table_ready(smp))
                 continue;
@@ -404,6 +420,26 @@ bool iterate(ibs_server *s)
             }
             runnable.push_back(r);
         }
+        for (Request *r : failed) {
+            ibs_request_result res{};
+            res.request_id = r->id;
+            res.sample = r->sample;
+            res.contig = r->contig;
+            res.first_window = r->w0;
+            res.n_windows = 0;
+            res.status = IBS_ERR_CUDA;
+            res.submit_time = r->submitT;
+            res.done_time = t;
+            res.rows = static_cast<ibs_window *>(malloc(sizeof(ibs_window)));
+            s->sumAlloc.release(r->sumOff, r->totalSpans);
+            s->rowAlloc.release(r->rowOff, r->nw);
+            s->st.completed++;
+            s->st.failed++;
+            s->done.push_back(res);
+            s->active.remove_if([r](const std::unique_ptr<Request> &p) { return p.get() == r; });
+        }
+        if (!failed.empty())
+            s->doneCv.notify_all();
     }
     if (runnable.empty()) {
         std::lock_guard<std::mutex> lock(s->mu);
@@ -807,6 +843,8 @@ extern "C" ibs_status ibs_server_stats_get(ibs_server *s, ibs_server_stats *out)
     out->latency_p50 = percentile(s->latencies, 0.50);
     out->latency_p99 = percentile(s->latencies, 0.99);
     out->latency_max = s->latencies.empty() ? 0 : *std::max_element(s->latencies.begin(), s->latencies.end());
+    out->queued = s->queue.size();
+    out->running = s->active.size();
     return IBS_OK;
 }
 

@@ -64,7 +64,8 @@ class RequestResult(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "launches", "spans", "probes", "reloads",
                                           "reload_bytes", "evictions", "resident_bytes", "resident_tables")] + \
-               [(n, C.c_double) for n in ("busy_seconds", "latency_p50", "latency_p99", "latency_max")]
+               [(n, C.c_double) for n in ("busy_seconds", "latency_p50", "latency_p99", "latency_max")] + \
+               [(n, C.c_uint64) for n in ("failed", "queued", "running")]
 
 
 class Tuning(C.Structure):
@@ -577,7 +578,13 @@ class Server:
     def poll(self, max_results: int = 64, timeout_ms: int = 0) -> list[dict]:
         buf = (RequestResult * max_results)()
         n = C.c_uint32()
-        _check(_ibs_srv_poll(self._h, buf, max_results, C.byref(n), timeout_ms))
+        if timeout_ms < 0:  # wait in bounded slices so that Python signals are still handled
+            while True:
+                _check(_ibs_srv_poll(self._h, buf, max_results, C.byref(n), 1000))
+                if n.value:
+                    break
+        else:
+            _check(_ibs_srv_poll(self._h, buf, max_results, C.byref(n), timeout_ms))
         out = []
         for i in range(n.value):
             r = buf[i]

@@ -240,6 +240,8 @@ typedef struct ibs_server_stats {
     uint64_t resident_bytes, resident_tables;
     double busy_seconds;              /* device time of the span launches */
     double latency_p50, latency_p99, latency_max; /* seconds, completed requests */
+    uint64_t failed;                  /* completed with a non-OK status (a table reload failed) */
+    uint64_t queued, running;         /* waiting for admission / admitted and not yet complete */
 } ibs_server_stats;
 
 ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t k, const ibs_server_opts *opts,

@@ -81,3 +81,29 @@ def test_panel_from_kmc_matches_goldens(build_case):
         for j, ix in enumerate(ixs):
             assert np.array_equal(rows[j], orc.scan(ix, seqs, W, 25, threads=4))
     pt.close()
+
+
+def test_panel_stash_grows_when_keys_exceed_the_estimate():
+    ref_spec = ib.RefSpec(seed=78, lens=[300_000, 50_000], n_frac=0.002, n_run=(1, 100))
+    seq, mask = ref_spec.reference_host()
+    samples = _samples(ref_spec, seq, mask, 4, k=15)  # k=15: no minimum bucket count
+    union = len(np.unique(np.concatenate(samples)))
+    pt = ib.PanelTable(15, union // 12)  # ~36 keys per 5-slot bucket: most keys overflow
+    first = pt.info()[0].stash_buckets
+    for c in samples:
+        pt.add_codes(c, len(c), on_device=False)
+    info, ns = pt.info()
+    assert info.stash_buckets > first
+    rng = np.random.default_rng(4)
+    q = np.concatenate([np.concatenate(samples), corpus.random_codes(rng, 20_000, 15)])
+    want = np.zeros(len(q), np.uint32)
+    for i, c in enumerate(samples):
+        want |= np.isin(q, c).astype(np.uint32) << np.uint32(i)
+    assert np.array_equal(pt.probe(q), want)
+    ref = ib.Reference(seq, mask, ref_spec.lens)
+    panel = pt.scan(ref, 5000)
+    for i, c in enumerate(samples):
+        t = ib.Table.from_codes(c, len(c), 15, on_device=False)
+        assert np.array_equal(panel[i], ib.scan(t, ref, 5000)), f"sample {i}"
+        t.close()
+    pt.close()

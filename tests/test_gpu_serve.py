@@ -71,7 +71,9 @@ def test_requests_alone_equal_full_scan_rows(world):
     srv = make_server(world)
     for req in random_requests(world, 25, 1):
         srv.submit(*req)
-        (r,) = srv.poll(1, timeout_ms=-1)
+        got = srv.poll(1, timeout_ms=60_000)
+        assert len(got) == 1, ("no result within 60 s", req, srv.stats())
+        (r,) = got
         assert r["status"] == 0
         assert np.array_equal(r["rows"], expected(world, r)), req
     srv.close()
@@ -90,9 +92,11 @@ def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world):
 
     th = threading.Thread(target=producer)
     th.start()
-    while len(done) < len(reqs):
+    deadline = time.time() + 300
+    while len(done) < len(reqs) and time.time() < deadline:
         done += srv.poll(64, timeout_ms=2000)
     th.join()
+    assert len(done) == len(reqs), ("requests left unfinished", srv.stats())
     for r in done:
         assert r["status"] == 0
         assert np.array_equal(r["rows"], expected(world, r)), (r["sample"], r["contig"], r["first_window"])
