@@ -545,14 +545,17 @@ def panel_arm(args, rank: int):
 
 
 def served_arm(args, rank: int):
-    """Served scan stream over the 2 Gbp reference and a pool of resident
-    samples: Poisson arrivals, regions log-uniform from 1 Mbp to a whole
-    contig; the batching server against the same server taking one request
-    per launch. Every result is checked against the sample's full-scan rows."""
+    """Served scan stream: the 4.2 Gbp panel reference and a pool of 16
+    resident samples; Poisson arrivals; each request one sample and a region
+    log-uniform from 1 Mbp to a whole contig. The batching server over joint
+    panel tables (requests sharing windows are scanned together) against the
+    plain path (per-sample tables, one request per launch) on the same GPU.
+    Every result is checked against its sample's full-scan rows."""
     import torch
     import ibs_b200 as ib
     from ibs_b200 import configs
-    w = configs.plain_2gbp(scale=args.serve_scale)
+    w = configs.panel_4gbp(n_samples=args.serve_samples, scale=args.serve_scale,
+                           sample_scale=args.serve_sample_scale)
     k, W = w.k, w.window
     lens = w.ref.lens
     sw, mw = w.ref.packed_words()
@@ -560,49 +563,41 @@ def served_arm(args, rank: int):
     dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
     w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
     ref = ib.Reference(dseq.data_ptr(), dmask.data_ptr(), lens, on_device=True)
-    rng = np.random.default_rng(404)
-    n_samples = args.serve_samples
-    base = w.samples[0].c
-    specs = [ib.SampleSpec(seed=4000 + i, k=k, class_rate=tuple(base.class_rate)[:4],
-                           class_prob=tuple(base.class_prob)[:4], block_len=int(base.block_len),
-                           present_frac=float(np.exp(rng.uniform(np.log(0.05), np.log(0.5)))),
-                           random_frac=0.10) for i in range(n_samples)]
-    full = []
+    n_samples = len(w.samples)
     win_start = np.concatenate([[0], np.cumsum([ib.window_count(lens[c:c + 1], W, k) for c in range(len(lens))])])
+    n_win = int(win_start[-1])
     t0 = time.time()
-    n_keys = []
 
-    def codes(sp):
+    def codes(i):
+        sp = w.samples[i]
         bound = sp.codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
         buf = torch.empty(bound, dtype=torch.int64, device="cuda")
         n = sp.codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), buf.data_ptr(), bound)
         return buf, n
 
-    rows_dev = torch.empty(int(win_start[-1]) * 6, dtype=torch.int32, device="cuda")
-    for sp in specs:  # every sample's full-scan rows, to check the served results
-        buf, n = codes(sp)
+    # every sample's full-scan rows (to check the served results) and a 1/64
+    # hash sample of its k-mers (to size the joint tables)
+    full, n_keys, sampled, max_bound = [], [], [], 0
+    rows_dev = torch.empty(n_win * 6, dtype=torch.int32, device="cuda")
+    for i in range(n_samples):
+        buf, n = codes(i)
+        max_bound = max(max_bound, buf.numel())
         n_keys.append(n)
+        v = buf[:n]
+        sampled.append(torch.unique(v[((v * 0x9E3779B97F4A7C15) >> 58) == 0]))
         t = ib.Table.from_codes(buf.data_ptr(), n, k, on_device=True)
-        ib.scan_async(t, ref, W, rows_dev.data_ptr(), int(win_start[-1]), 0)
+        del buf, v
+        torch.cuda.empty_cache()
+        ib.scan_async(t, ref, W, rows_dev.data_ptr(), n_win, 0)
         torch.cuda.synchronize()
         full.append(rows_dev.cpu().numpy().view(ib.WINDOW_DTYPE).copy())
         t.close()
-        del buf
-        torch.cuda.empty_cache()
     del rows_dev
     torch.cuda.empty_cache()
     setup_s = time.time() - t0
 
-    def server(mode):
-        srv = ib.Server(ref, W, k, memory_budget=args.serve_budget_gb << 30,
-                        one_request_per_launch=(mode == "serial"))
-        for sp in specs:
-            buf, n = codes(sp)
-            srv.add_codes(buf.data_ptr(), n, on_device=True)
-            del buf
-            torch.cuda.empty_cache()
-        return srv
     # the request stream
+    rng = np.random.default_rng(404)
     reqs = []
     step = W - k
     for _ in range(args.serve_requests):
@@ -632,34 +627,89 @@ def served_arm(args, rank: int):
         else:
             for req in reqs:
                 srv.submit(*req)
-        while len(done) < len(reqs):
+        deadline = time.time() + 1800
+        while len(done) < len(reqs) and time.time() < deadline:
             done += srv.poll(256, timeout_ms=1000)
+        assert len(done) == len(reqs), f"served requests unfinished: {srv.stats()}"
         makespan = srv.now() - t_start
         st = srv.stats()
         lat = np.array([r["done_time"] - r["submit_time"] for r in done])
         for r in done:
+            assert r["status"] == 0, "a served request failed"
             a = int(win_start[r["contig"]] + r["first_window"])
             assert np.array_equal(r["rows"], full[r["sample"]][a:a + int(r["n_windows"])]), "served rows differ"
         probes = st["probes"] - stats0["probes"]
-        return {"requests": len(done), "probes": int(probes), "makespan_s": makespan,
-                "probes_per_s": probes / makespan,
-                "device_probes_per_s": probes / max(1e-9, st["busy_seconds"] - stats0["busy_seconds"]),
+        busy = st["busy_seconds"] - stats0["busy_seconds"]
+        return {"requests": len(done), "probes": int(probes), "scanned": int(st["scanned"] - stats0["scanned"]),
+                "makespan_s": makespan, "probes_per_s": probes / makespan,
+                "device_busy_s": busy, "probes_per_device_s": probes / max(busy, 1e-9),
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
                 "latency_max_s": float(lat.max()), "launches": int(st["launches"] - stats0["launches"]),
                 "reloads": int(st["reloads"] - stats0["reloads"]),
                 "reload_bytes": int(st["reload_bytes"] - stats0["reload_bytes"])}
 
-    out = {"workload": f"plain_2gbp reference x {n_samples} resident samples",
-           "sample_kmers": n_keys, "requests": len(reqs), "arrival_rate_per_s": args.serve_rate,
-           "setup_s": setup_s, "budget_gb": args.serve_budget_gb}
-    for mode in ("batched", "serial"):
-        srv = server(mode)
-        out[f"{mode}_poisson"] = run(srv, True)
-        out[f"{mode}_saturated"] = run(srv, False)
-        srv.close()
-    out["saturated_speedup_vs_one_request_per_launch"] = (out["batched_saturated"]["probes_per_s"] /
-                                                         out["serial_saturated"]["probes_per_s"])
+    out = {"workload": f"{w.name} reference x {n_samples} resident samples", "k": k, "window": W,
+           "reference_bp": int(sum(map(int, lens))), "sample_kmers": n_keys, "requests": len(reqs),
+           "arrival_rate_per_s": args.serve_rate, "region": "log-uniform 1 Mbp .. whole contig",
+           "setup_s": setup_s}
+
+    # plain path: per-sample tables, one request per launch
+    free, _ = torch.cuda.mem_get_info()
+    srv = ib.Server(ref, W, k, memory_budget=int(free * 0.85), one_request_per_launch=True)
+    for i in range(n_samples):
+        buf, n = codes(i)
+        srv.add_codes(buf.data_ptr(), n, on_device=True)
+        del buf
+        torch.cuda.empty_cache()
+    out["plain_tables_gb"] = srv.stats()["resident_bytes"] / 1e9
+    out["plain_poisson"] = run(srv, True)
+    out["plain_saturated"] = run(srv, False)
+    srv.close()
+    torch.cuda.empty_cache()
+
+    # batched: joint panel tables (as many samples per table as memory allows)
+    kpb = args.panel_keys_per_bucket
+    free, _ = torch.cuda.mem_get_info()
+    budget = free - max_bound * 8 - (4 << 30) - (8 << 30)
+    union_of = {}
+
+    def joint_bytes(members):
+        u = int(torch.unique(torch.cat([sampled[j] for j in members])).numel() * 64 * 1.02) + (1 << 20)
+        union_of[tuple(members)] = u
+        return u / kpb * 32 * 1.15
+
+    groups, cur = [], []
+    for i in range(n_samples):
+        if cur and sum(joint_bytes(g) for g in groups) + joint_bytes(cur + [i]) > budget:
+            groups.append(cur)
+            cur = []
+        cur.append(i)
+    groups.append(cur)
+    del sampled
+    srv = ib.Server(ref, W, k, memory_budget=int(free * 0.85))
+    id_of = {}
+    for members in groups:
+        pt = ib.PanelTable(k, union_of[tuple(members)], keys_per_bucket=kpb)
+        for i in members:
+            buf, n = codes(i)
+            pt.add_codes(buf.data_ptr(), n, on_device=True)
+            del buf
+            torch.cuda.empty_cache()
+        for i, sid in zip(members, srv.add_panel(pt, release=True)):
+            id_of[i] = sid
+        pt.close()
+        torch.cuda.empty_cache()
+    assert all(id_of[i] == i for i in range(n_samples))
+    out["batched_groups"] = groups
+    out["batched_tables_gb"] = srv.stats()["resident_bytes"] / 1e9
+    out["batched_poisson"] = run(srv, True)
+    out["batched_saturated"] = run(srv, False)
+    srv.close()
+    out["saturated_speedup_vs_plain"] = (out["batched_saturated"]["probes_per_s"] /
+                                         out["plain_saturated"]["probes_per_s"])
     out["rows_equal_full_scan"] = True
+    out["note"] = ("probes = positions of the completed requests (a window shared by k requests counts k "
+                   "times); scanned = positions the device scanned")
     ref.free()
     return out
 
@@ -731,10 +781,11 @@ def main():
     ap.add_argument("--serve", action="store_true", help="also measure the served request stream")
     ap.add_argument("--serve-only", action="store_true")
     ap.add_argument("--serve-samples", type=int, default=16)
-    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=50.0)
-    ap.add_argument("--serve-scale", type=float, default=1.0)
-    ap.add_argument("--serve-budget-gb", type=int, default=120)
+    ap.add_argument("--serve-scale", type=float, default=1.0, help="reference length scale")
+    ap.add_argument("--serve-sample-scale", type=float, default=0.5,
+                    help="sample size scale (the 16 full-size samples do not fit on one GPU together)")
     args = ap.parse_args()
 
     from ibs_b200 import configs

@@ -1,22 +1,7 @@
-// Panel scan: one reference pass against up to 16 samples through ONE joint
-// table whose slots carry a sample-membership mask.
-//
-// The reference's panel mode encodes each batch once and probes every
-// resident database separately (encodeProbeMultiKernel + MultiBsProbe,
-// src/gpu/EncodeProbe.cu:82-108, :175-193; MAX_DBS = 16,
-// src/gpu/EncodeProbeCore.hpp:291), so a position costs one index search
-// per sample. Here the samples' k-mer sets are merged into one table: a
-// position costs one random 32-byte bucket load whatever the panel size,
-// and the mask in the matching slot says which samples hold the k-mer.
-// Every sample's rows are still exactly its single-sample rows.
-//
-// Bucket format P5x48 (one 32-byte sector): u32 fingerprints of slots 0-4
-// (words 0-4), u16 sample masks of slots 0-4 (bytes 20-29), slot count
-// (byte 30), flags (byte 31, bit 0 = some key of this bucket is in the
-// stash). The fingerprint is the same quotient of the bijective k-mer hash
-// as in the single-sample table, so it needs nBuckets >= 2^(2k-32).
-// Stash: {code, mask} pairs, two per 32-byte bucket, linear probing.
-#include "ibs_internal.cuh"
+// Panel scan over the joint table of panel_core.cuh: build (two-phase
+// insertion per sample), the persistent span kernel and its CUDA graph, and
+// the ibs_panel_table_* entry points.
+#include "panel_core.cuh"
 #include "scan_device.cuh"
 
 #include <chrono>
@@ -27,62 +12,9 @@
 namespace ibs {
 namespace panel {
 
-constexpr uint32_t kMaxSamples = IBS_PANEL_MAX_SAMPLES;
-constexpr uint32_t kSlots = 5;
 constexpr uint32_t kSpanLen = 8192;
 constexpr int kNB = 4;
-constexpr uint64_t kStashEmpty = ~0ull;
 constexpr uint64_t kBuildChunk = 1ull << 27; // keys per build step (1 GiB of scratch each way)
-
-struct View {
-    TableGeom g;
-    const uint4 *buckets;
-    const ulonglong2 *stash; // {code, mask}
-    uint64_t stashBuckets;   // power of two; two entries each
-};
-
-__device__ __forceinline__ uint32_t stash_mask(const View &t, uint64_t code)
-{
-    uint64_t b = stash_home(code, t.stashBuckets);
-    for (uint64_t i = 0; i < t.stashBuckets; ++i) {
-        const ulonglong2 e0 = __ldg(t.stash + 2 * b), e1 = __ldg(t.stash + 2 * b + 1);
-        if (e0.x == code)
-            return (uint32_t)e0.y;
-        if (e1.x == code)
-            return (uint32_t)e1.y;
-        if (e0.x == kStashEmpty || e1.x == kStashEmpty)
-            return 0;
-        b = (b + 1) & (t.stashBuckets - 1);
-    }
-    return 0;
-}
-
-// Sample mask of a k-mer given its bucket halves and fingerprint; bit 31
-// set = look in the stash.
-__device__ __forceinline__ uint32_t bucket_mask(const uint4 &v0, const uint4 &v1, uint32_t fp)
-{
-    const uint32_t cnt = (v1.w >> 16) & 0xff;
-    uint32_t m = 0;
-    m |= (0 < cnt && v0.x == fp) ? (v1.y & 0xffff) : 0u;
-    m |= (1 < cnt && v0.y == fp) ? (v1.y >> 16) : 0u;
-    m |= (2 < cnt && v0.z == fp) ? (v1.z & 0xffff) : 0u;
-    m |= (3 < cnt && v0.w == fp) ? (v1.z >> 16) : 0u;
-    m |= (4 < cnt && v1.x == fp) ? (v1.w & 0xffff) : 0u;
-    if (!m && ((v1.w >> 24) & 1u))
-        m = 0x80000000u;
-    return m;
-}
-
-__device__ __forceinline__ uint32_t lookup_mask(const View &t, uint64_t code)
-{
-    const uint64_t h = perm_hash(code, t.g.bits);
-    const uint64_t r = bucket_of(h, t.g);
-    const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);
-    uint32_t m = bucket_mask(v0, v1, (uint32_t)fp_of(h, t.g));
-    if (m & 0x80000000u)
-        m = stash_mask(t, code);
-    return m;
-}
 
 // ---- build: phase A finds keys already present and ORs in the sample bit;
 // phase B inserts the rest. Within one sample the keys are unique, so no
@@ -213,40 +145,6 @@ __global__ void k_stash_move(const ulonglong2 *old, uint64_t oldEntries, unsigne
         if (!placed)
             atomicExch(err, 1);
     }
-}
-
-// Block statistics of one sample from its valid (V) and hit (H) masks,
-// computed by one lane with bit operations: the gaps between hits are the
-// runs of valid misses, visited one run at a time.
-__device__ __forceinline__ SegStats block_stats_serial(uint32_t V, uint32_t H, int k)
-{
-    SegStats b;
-    b.pad = 0;
-    b.total = __popc(V);
-    b.obs = __popc(H);
-    b.gaps = 0;
-    b.dist = 0;
-    if (H == 0) {
-        b.lead = b.trail = b.total;
-        return b;
-    }
-    const uint32_t first = __ffs(H) - 1;
-    const uint32_t last = 31 - __clz(H);
-    b.lead = __popc(V & ((1u << first) - 1u));
-    b.trail = last == 31 ? 0u : __popc(V >> (last + 1));
-    // valid misses strictly between the first and the last hit
-    const uint64_t inner = ((2ull << last) - 1ull) & ~((2ull << first) - 1ull);
-    uint32_t m = V & ~H & (uint32_t)inner;
-    while (m) {
-        const uint32_t start = __ffs(m) - 1;
-        const uint32_t next = H & ~((2u << start) - 1u); // hits after the run starts (nonzero)
-        const uint32_t j = __ffs(next) - 1;
-        const uint32_t g = __popc(m & ((1u << j) - 1u));
-        b.gaps += 1;
-        b.dist += gap_distance(g, k);
-        m &= ~((1u << j) - 1u);
-    }
-    return b;
 }
 
 template <int NB>
@@ -414,31 +312,6 @@ uint64_t next_pow2(uint64_t x)
 using namespace ibs;
 using namespace ibs::panel;
 
-struct ibs_panel_table {
-    int device = 0;
-    TableGeom geom{};
-    uint4 *buckets = nullptr;
-    ulonglong2 *stash = nullptr;
-    uint64_t stashBuckets = 0;
-    uint32_t nSamples = 0;
-    uint64_t keysAdded = 0; // sum of the samples' key counts
-    uint64_t deviceBytes = 0;
-    double buildSeconds = 0;
-    int *dErr = nullptr;
-    unsigned long long *dCounters = nullptr; // [0] pending count, [1] scan work counter, [2] failed
-    uint32_t stashGrowths = 0;
-    // scan plan and scratch
-    const ibs_reference *planRef = nullptr;
-    std::vector<uint64_t> planLens;
-    ScanPlan plan;
-    SegStats *dSpans = nullptr;
-    uint64_t spansCap = 0;
-    // captured scan graph for (reference, W, rows, stream)
-    cudaGraphExec_t graph = nullptr;
-    const void *graphKey[3] = {nullptr, nullptr, nullptr};
-    uint32_t graphW = 0;
-    View view() const { return View{geom, buckets, stash, stashBuckets}; }
-};
 
 extern "C" ibs_status ibs_panel_table_create(uint32_t k, uint64_t expected_keys,
                                              const ibs_table_opts *opts, ibs_panel_table **out)
@@ -516,8 +389,19 @@ static ibs_status grow_stash(ibs_panel_table *p)
     return IBS_OK;
 }
 
+// A panel whose table was handed to a server keeps only its handle.
+static ibs_status check_live(const ibs_panel_table *p)
+{
+    if (p->buckets)
+        return IBS_OK;
+    set_error("panel table: its device table was released to a server");
+    return IBS_ERR_STATE;
+}
+
 static ibs_status panel_add_device_codes(ibs_panel_table *p, const uint64_t *dCodes, uint64_t n)
 {
+    if (check_live(p) != IBS_OK)
+        return IBS_ERR_STATE;
     if (p->nSamples >= kMaxSamples) {
         set_error("panel table already holds " + std::to_string(kMaxSamples) + " samples");
         return IBS_ERR_CAPACITY;
@@ -645,6 +529,8 @@ extern "C" ibs_status ibs_panel_table_probe(ibs_panel_table *p, const uint64_t *
         set_error("ibs_panel_table_probe: bad argument");
         return IBS_ERR_ARG;
     }
+    if (check_live(p) != IBS_OK)
+        return IBS_ERR_STATE;
     if (!n)
         return IBS_OK;
     DeviceGuard guard(p->device);
@@ -733,6 +619,8 @@ extern "C" ibs_status ibs_panel_table_scan_async(ibs_panel_table *p, ibs_referen
         set_error("ibs_panel_table_scan_async: row capacity too small (samples x windows)");
         return IBS_ERR_ARG;
     }
+    if (check_live(p) != IBS_OK)
+        return IBS_ERR_STATE;
     DeviceGuard guard(p->device);
     ibs_status s = panel_plan(p, ref, W);
     if (s != IBS_OK)
@@ -786,6 +674,8 @@ extern "C" ibs_status ibs_panel_table_scan(ibs_panel_table *p, ibs_reference *re
         set_error("ibs_panel_table_scan: row capacity too small (samples x windows)");
         return IBS_ERR_ARG;
     }
+    if (check_live(p) != IBS_OK)
+        return IBS_ERR_STATE;
     DeviceGuard guard(p->device);
     ibs_window *d = nullptr;
     IBS_CUDA(cudaMalloc(&d, std::max<uint64_t>(need, 1) * sizeof(ibs_window)), "row alloc");
@@ -807,6 +697,23 @@ extern "C" ibs_status ibs_panel_table_scan(ibs_panel_table *p, ibs_reference *re
     IBS_CUDA(e, "panel scan");
     return IBS_OK;
 }
+
+namespace ibs {
+// Frees the panel's device table (the server keeps a host image of it).
+void panel_release_table(ibs_panel_table *p)
+{
+    DeviceGuard guard(p->device);
+    if (p->graph) {
+        cudaGraphExecDestroy(p->graph);
+        p->graph = nullptr;
+    }
+    cudaFree(p->buckets);
+    cudaFree(p->stash);
+    p->buckets = nullptr;
+    p->stash = nullptr;
+    p->deviceBytes = 0;
+}
+} // namespace ibs
 
 extern "C" void ibs_panel_table_close(ibs_panel_table *p)
 {

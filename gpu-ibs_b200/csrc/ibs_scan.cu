@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                     }
                 }
                 const uint32_t o = isFwd ? jl : (w - 1 - jr);
-                const uint64_t r = mz::bucket_of_h(mn, t.g.nBuckets);
+                const uint64_t r = mz::bucket_of_h(mn, code[b], t.g.nBuckets);
                 slot[b] = mz::slot_value(mz::slot_high(code[b], k, o), mn, t.g.fpBits);
                 if (valid[b]) {
                     v0[b] = __ldg(t.buckets + 2 * r);

@@ -1,19 +1,31 @@
-// The serving loop: continuous batching of window-scan requests over
-// resident sample tables.
+// The serving loop: continuous batching of window-scan requests.
 //
-// A request names a sample and a range of windows of one contig. Its work
-// is the spans of those windows (up to kSpanLen positions of one window
-// each). A background thread runs the loop: admit requests, make their
-// tables resident (least-recently-used eviction under a byte budget, reload
-// from a pinned host image on a side stream), then launch one span kernel
-// carrying slices of every runnable request -- each a work item that names
-// its table -- followed by a finalizer for the requests whose last spans ran.
-// Up to two launches are in flight; a request submitted meanwhile joins the
-// next one. Rows are the same windows' rows of a full scan of the sample.
+// A request names a sample and a range of windows of one contig. Samples
+// live in device tables, here called groups: a single-sample table (hash
+// formats B8x32 / B6x40) or a joint panel table (P5x48, one sample-mask per
+// key, up to 16 samples). Windows are numbered across contigs, so a request
+// is an interval of that numbering.
+//
+// A background thread runs iterations. Each one admits new requests, makes
+// the groups they need resident (least-recently-used eviction under a byte
+// budget, reload from a pinned host image on a side stream) and then, for
+// every resident group with pending windows, takes the next run of pending
+// windows from that group's sweep cursor. Each such window is scanned ONCE
+// for all the pending requests that contain it: in a joint table one bucket
+// load per position answers every requesting sample, and two requests of one
+// sample share the scan. The span kernels write one statistics summary per
+// (span, requesting sample); the finalizer folds each (request, window)'s
+// summaries into that request's row. Two iterations are in flight at a time
+// and a request submitted meanwhile joins the next one. A request's rows are
+// the same windows' rows of a full scan of its sample, whatever it was
+// batched with.
+//
+// With one_request_per_launch an iteration runs the windows of one request
+// only, against its own table: the plain path, one launch per request.
 //
 // No device code waits on the host: each launch is a finite kernel over a
-// finite work list, so nothing here can spin on the GPU.
-#include "ibs_internal.cuh"
+// finite work list.
+#include "panel_core.cuh"
 #include "scan_device.cuh"
 
 #include <algorithm>
@@ -33,39 +45,41 @@ namespace serve {
 
 constexpr uint32_t kSpanLen = 4096;
 constexpr int kNB = 4;
-constexpr uint64_t kSumPool = 4ull << 20;  // span summaries (32 B each): 128 MiB
-constexpr uint64_t kRowPool = 2ull << 20;  // rows (24 B each): 48 MiB
+constexpr uint64_t kSumCap = 1ull << 20;   // span summaries per launch (32 B each): 32 MiB
+constexpr uint64_t kPosCap = 512ull << 20; // reference positions scanned per launch
+constexpr uint64_t kFinCap = 1ull << 20;   // (request, window) rows finalized per launch
+constexpr uint64_t kRowPool = 4ull << 20;  // rows of admitted requests (24 B each): 96 MiB
+constexpr uint32_t kMaxGroups = 4096;
 constexpr int kDepth = 2;                  // launches in flight
 
 struct WorkItem {
     uint64_t base;   // packed base offset of the window's first base
     uint32_t p0, p1; // positions of the window
-    uint32_t table;  // index into this launch's table views
-    uint32_t pad;
-    uint64_t out;    // summary slot
+    uint32_t view;   // index into this launch's views of its kind
+    uint32_t mask;   // requesting samples (bits of a joint table; 1 for a single table)
+    uint64_t out;    // first summary slot; sample of rank i writes out + i
 };
 
 struct FinItem {
-    uint64_t sum;    // first summary slot of the window
-    uint32_t nSpans;
+    uint64_t sum;    // summary of the window's first span for this request's sample
+    uint32_t nSpans, stride;
     int32_t start, end;
-    uint32_t pad;
     uint64_t row;    // row slot
 };
 
 template <int NB>
-__global__ void __launch_bounds__(256) k_serve_spans(const TableView *__restrict__ views,
-                                                     const WorkItem *__restrict__ items, uint32_t nItems,
-                                                     const uint64_t *__restrict__ seq,
-                                                     const uint64_t *__restrict__ mask,
-                                                     SegStats *__restrict__ sums)
+__global__ void __launch_bounds__(256) k_serve_single(const TableView *__restrict__ views,
+                                                      const WorkItem *__restrict__ items, uint32_t nItems,
+                                                      const uint64_t *__restrict__ seq,
+                                                      const uint64_t *__restrict__ mask,
+                                                      SegStats *__restrict__ sums)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = warp; i < nItems; i += nWarps) {
         const WorkItem it = items[i];
-        const TableView t = views[it.table];
+        const TableView t = views[it.view];
         const uint32_t k = t.g.k;
         const uint64_t kmask = key_mask(2 * k);
         const uint64_t kbits = (1ull << k) - 1;
@@ -112,6 +126,75 @@ __global__ void __launch_bounds__(256) k_serve_spans(const TableView *__restrict
     }
 }
 
+// Joint tables: one bucket load per position; lane j keeps the statistics
+// of sample j when j is in the item's mask.
+template <int NB>
+__global__ void __launch_bounds__(256) k_serve_joint(const panel::View *__restrict__ views,
+                                                     const WorkItem *__restrict__ items, uint32_t nItems,
+                                                     const uint64_t *__restrict__ seq,
+                                                     const uint64_t *__restrict__ mask,
+                                                     SegStats *__restrict__ sums)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < nItems; i += nWarps) {
+        const WorkItem it = items[i];
+        const panel::View t = views[it.view];
+        const uint32_t k = t.g.k;
+        const uint64_t kmask = key_mask(2 * k);
+        const uint64_t kbits = (1ull << k) - 1;
+        const uint32_t want = it.mask & 0xffffu;
+        SegStats acc = seg_empty();
+        for (uint32_t p = it.p0; p < it.p1; p += 32 * NB) {
+            uint4 v0[NB], v1[NB];
+            uint64_t code[NB];
+            uint32_t fp[NB];
+            bool valid[NB];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const uint32_t q = p + 32 * b + lane;
+                const bool in = q < it.p1;
+                const uint64_t G = it.base + (in ? q : it.p0);
+                bool acgt;
+                code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
+                valid[b] = in && acgt;
+                const uint64_t h = perm_hash(code[b], t.g.bits);
+                const uint64_t r = bucket_of(h, t.g);
+                fp[b] = (uint32_t)fp_of(h, t.g);
+                if (valid[b]) {
+                    v0[b] = __ldg(t.buckets + 2 * r);
+                    v1[b] = __ldg(t.buckets + 2 * r + 1);
+                } else {
+                    v0[b] = make_uint4(0, 0, 0, 0);
+                    v1[b] = make_uint4(0, 0, 0, 0);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                uint32_t m = 0;
+                if (valid[b]) {
+                    m = panel::bucket_mask(v0[b], v1[b], fp[b]);
+                    if (m & 0x80000000u)
+                        m = panel::stash_mask(t, code[b]);
+                }
+                const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
+                uint32_t myH = 0;
+                for (uint32_t rest = want; rest; rest &= rest - 1) { // warp-uniform
+                    const uint32_t j = __ffs(rest) - 1;
+                    const uint32_t Hj = __ballot_sync(dev::FULL_MASK, (m >> j) & 1u);
+                    if (lane == j)
+                        myH = Hj;
+                }
+                if ((want >> lane) & 1u)
+                    acc = seg_combine(acc, panel::block_stats_serial(V, myH, (int)k), (int)k);
+            }
+        }
+        if ((want >> lane) & 1u)
+            sums[it.out + __popc(want & ((1u << lane) - 1u))] = acc;
+    }
+}
+
 __global__ void k_serve_finalize(const FinItem *__restrict__ fin, uint32_t n, const SegStats *__restrict__ sums,
                                  int k, ibs_window *__restrict__ rows)
 {
@@ -120,7 +203,7 @@ __global__ void k_serve_finalize(const FinItem *__restrict__ fin, uint32_t n, co
         const FinItem f = fin[i];
         SegStats acc = seg_empty();
         for (uint32_t s = 0; s < f.nSpans; ++s)
-            acc = seg_combine(acc, sums[f.sum + s], k);
+            acc = seg_combine(acc, sums[f.sum + (uint64_t)s * f.stride], k);
         WindowRow row;
         row.start = f.start;
         row.end = f.end;
@@ -181,10 +264,13 @@ class RangeAlloc
     std::map<uint64_t, uint64_t> free_;
 };
 
-struct Sample {
+// A device table holding one sample (single) or several (joint).
+struct Group {
     uint32_t id = 0;
+    bool joint = false;
+    uint32_t nSamples = 1;
     TableGeom geom{};
-    uint64_t nKeys = 0;
+    uint64_t stashBuckets = 0;       // joint tables: stash buckets of two {code, mask} entries
     uint64_t bucketBytes = 0, stashBytes = 0;
     void *host = nullptr;            // pinned image: buckets, then stash
     uint8_t *dev = nullptr;          // resident copy (pool memory) or null
@@ -192,40 +278,44 @@ struct Sample {
     bool loading = false;
     double lastUse = 0;
     int inflight = 0;                // launches in flight that use the table
+    uint64_t cursor = 0;             // sweep position (global window index)
     uint64_t bytes() const { return bucketBytes + stashBytes; }
-    TableView view() const
+    TableView single_view() const
     {
         return TableView{geom, reinterpret_cast<const uint4 *>(dev),
                          stashBytes ? reinterpret_cast<const uint64_t *>(dev + bucketBytes) : nullptr};
     }
+    panel::View joint_view() const
+    {
+        return panel::View{geom, reinterpret_cast<const uint4 *>(dev),
+                           reinterpret_cast<const ulonglong2 *>(dev + bucketBytes), stashBuckets};
+    }
+};
+
+struct SampleRef {
+    uint32_t group, bit;
 };
 
 struct Request {
     uint64_t id = 0;
     uint32_t sample = 0, contig = 0;
-    uint64_t w0 = 0, nw = 0;
+    uint64_t w0 = 0, nw = 0, g0 = 0; // g0: global index of the first window
+    uint64_t positions = 0;
     double submitT = 0;
-    std::vector<FinItem> win;        // per window (sum/row relative to the request's slots)
-    std::vector<uint64_t> winBase;   // packed base per window
-    std::vector<uint32_t> winPos;    // positions per window
-    uint64_t totalSpans = 0, scheduled = 0;
-    uint64_t sumOff = 0, rowOff = 0;
-    uint64_t curWin = 0, curSpanInWin = 0; // scheduling cursor
-    bool admitted = false;
+    std::vector<std::pair<uint64_t, uint64_t>> remaining; // global windows not yet planned
+    uint64_t planned = 0, rowOff = 0;
 };
 
 struct Launch {
-    std::vector<uint32_t> tables;       // sample ids used
-    std::vector<Request *> finishing;   // requests whose last spans ran here
+    std::vector<uint32_t> groups;       // groups used (claimed: inflight)
+    std::vector<Request *> finishing;   // requests whose last windows ran here
     cudaEvent_t start = nullptr, stop = nullptr;
-    WorkItem *hItems = nullptr;
-    FinItem *hFin = nullptr;
-    TableView *hViews = nullptr;
-    WorkItem *dItems = nullptr;
-    FinItem *dFin = nullptr;
-    TableView *dViews = nullptr;
-    uint64_t probes = 0;
-    uint32_t nItems = 0;
+    WorkItem *hSingle = nullptr, *hJoint = nullptr, *dSingle = nullptr, *dJoint = nullptr;
+    FinItem *hFin = nullptr, *dFin = nullptr;
+    TableView *hSV = nullptr, *dSV = nullptr;
+    panel::View *hJV = nullptr, *dJV = nullptr;
+    SegStats *dSums = nullptr;
+    uint64_t positions = 0;
     bool active = false;
 };
 
@@ -240,17 +330,18 @@ struct ibs_server {
     ibs_reference *ref = nullptr;
     uint32_t W = 0, k = 0;
     uint64_t budget = 0, resident = 0;
-    uint32_t maxItems = 1u << 15, minPer = 16;
-    bool serial = false; // one whole request per launch
-    std::vector<std::unique_ptr<Sample>> samples;
-    std::vector<std::vector<uint64_t>> contigWin; // per contig: window count
+    uint64_t itemCap = kSumCap;
+    bool serial = false; // one request per launch
+    std::vector<std::unique_ptr<Group>> groups;
+    std::vector<SampleRef> samples;
+    std::vector<uint64_t> contigWin0; // global index of each contig's first window; back() = total
     cudaStream_t comp = nullptr, side = nullptr;
-    SegStats *dSums = nullptr;
     ibs_window *dRows = nullptr;
     ibs_window *hRows = nullptr; // pinned mirror of dRows
-    RangeAlloc sumAlloc{kSumPool}, rowAlloc{kRowPool};
+    RangeAlloc rowAlloc{kRowPool};
     Launch launches[kDepth];
     int nextLaunch = 0;
+    int sms = 148;
     // request state
     std::mutex mu;
     std::condition_variable cv, doneCv;
@@ -268,25 +359,47 @@ struct ibs_server {
     {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
+    // window x (global index): its contig's packed base offset plus the window's bounds
+    void window(uint64_t x, uint64_t &base, uint32_t &nPos, int32_t &start, int32_t &end) const
+    {
+        const uint32_t c = (uint32_t)(std::upper_bound(contigWin0.begin(), contigWin0.end(), x) -
+                                      contigWin0.begin()) - 1;
+        const uint64_t j = (x - contigWin0[c]) * ((uint64_t)W - k);
+        const uint64_t e = std::min<uint64_t>(j + W, ref->lens[c]);
+        base = ref->baseOff[c] + j;
+        nPos = e - j >= k ? (uint32_t)(e - j - k + 1) : 0;
+        start = (int32_t)j;
+        end = (int32_t)e;
+    }
 };
 
 namespace {
 
-bool table_ready(Sample &smp);
-
-ibs_status make_resident(ibs_server *s, Sample &smp)
+bool table_ready(Group &g)
 {
-    if (smp.dev)
+    if (!g.dev)
+        return false;
+    if (g.loading) {
+        if (cudaEventQuery(g.loaded) != cudaSuccess)
+            return false;
+        g.loading = false;
+    }
+    return true;
+}
+
+ibs_status make_resident(ibs_server *s, Group &g)
+{
+    if (g.dev)
         return IBS_OK;
     // a finished reload makes its table evictable, whether or not a request
     // has looked at it since (tables loaded at registration included)
-    for (auto &o : s->samples)
+    for (auto &o : s->groups)
         if (o->dev && o->loading)
             table_ready(*o);
     // evict least-recently-used idle tables until this one fits
-    while (s->resident + smp.bytes() > s->budget) {
-        Sample *victim = nullptr;
-        for (auto &o : s->samples)
+    while (s->resident + g.bytes() > s->budget) {
+        Group *victim = nullptr;
+        for (auto &o : s->groups)
             if (o->dev && !o->inflight && !o->loading && (!victim || o->lastUse < victim->lastUse))
                 victim = o.get();
         if (!victim)
@@ -296,26 +409,28 @@ ibs_status make_resident(ibs_server *s, Sample &smp)
         s->resident -= victim->bytes();
         s->st.evictions++;
     }
-    IBS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&smp.dev), smp.bytes(), s->side), "table reload alloc");
-    IBS_CUDA(cudaMemcpyAsync(smp.dev, smp.host, smp.bytes(), cudaMemcpyHostToDevice, s->side), "table reload");
-    IBS_CUDA(cudaEventRecord(smp.loaded, s->side), "table reload event");
-    smp.loading = true;
-    s->resident += smp.bytes();
+    IBS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&g.dev), g.bytes(), s->side), "table reload alloc");
+    IBS_CUDA(cudaMemcpyAsync(g.dev, g.host, g.bytes(), cudaMemcpyHostToDevice, s->side), "table reload");
+    IBS_CUDA(cudaEventRecord(g.loaded, s->side), "table reload event");
+    g.loading = true;
+    s->resident += g.bytes();
     s->st.reloads++;
-    s->st.reload_bytes += smp.bytes();
+    s->st.reload_bytes += g.bytes();
     return IBS_OK;
 }
 
-bool table_ready(Sample &smp)
+ibs_request_result result_of(const Request &r, ibs_status status, double t)
 {
-    if (!smp.dev)
-        return false;
-    if (smp.loading) {
-        if (cudaEventQuery(smp.loaded) != cudaSuccess)
-            return false;
-        smp.loading = false;
-    }
-    return true;
+    ibs_request_result res{};
+    res.request_id = r.id;
+    res.sample = r.sample;
+    res.contig = r.contig;
+    res.first_window = r.w0;
+    res.n_windows = status == IBS_OK ? r.nw : 0;
+    res.status = status;
+    res.submit_time = r.submitT;
+    res.done_time = t;
+    return res;
 }
 
 // Completes launch L: its finishing requests' rows move to their results.
@@ -329,36 +444,181 @@ void retire(ibs_server *s, Launch &L)
         s->st.busy_seconds += ms * 1e-3;
     const double t = s->now();
     std::lock_guard<std::mutex> lock(s->mu);
-    for (uint32_t id : L.tables)
-        s->samples[id]->inflight--;
-    s->st.probes += L.probes;
+    for (uint32_t g : L.groups)
+        s->groups[g]->inflight--;
+    s->st.scanned += L.positions;
     for (Request *r : L.finishing) {
-        ibs_request_result res{};
-        res.request_id = r->id;
-        res.sample = r->sample;
-        res.contig = r->contig;
-        res.first_window = r->w0;
-        res.n_windows = r->nw;
-        res.status = IBS_OK;
-        res.submit_time = r->submitT;
-        res.done_time = t;
+        ibs_request_result res = result_of(*r, IBS_OK, t);
         res.rows = static_cast<ibs_window *>(malloc(std::max<uint64_t>(r->nw, 1) * sizeof(ibs_window)));
         memcpy(res.rows, s->hRows + r->rowOff, r->nw * sizeof(ibs_window));
-        s->sumAlloc.release(r->sumOff, r->totalSpans);
         s->rowAlloc.release(r->rowOff, r->nw);
         s->latencies.push_back(t - r->submitT);
         s->st.completed++;
+        s->st.probes += r->positions;
         s->done.push_back(res);
-        for (auto it = s->active.begin(); it != s->active.end(); ++it)
-            if (it->get() == r) {
-                s->active.erase(it);
-                break;
-            }
+        s->active.remove_if([r](const std::unique_ptr<Request> &p) { return p.get() == r; });
     }
     L.finishing.clear();
-    L.tables.clear();
+    L.groups.clear();
     L.active = false;
     s->doneCv.notify_all();
+}
+
+// Removes [lo, hi) (inside one of its intervals) from r's remaining windows.
+void take(Request &r, uint64_t lo, uint64_t hi)
+{
+    for (size_t i = 0; i < r.remaining.size(); ++i) {
+        auto &iv = r.remaining[i];
+        if (lo < iv.first || hi > iv.second)
+            continue;
+        const std::pair<uint64_t, uint64_t> left{iv.first, lo}, right{hi, iv.second};
+        r.remaining.erase(r.remaining.begin() + i);
+        if (right.second > right.first)
+            r.remaining.insert(r.remaining.begin() + i, right);
+        if (left.second > left.first)
+            r.remaining.insert(r.remaining.begin() + i, left);
+        r.planned += hi - lo;
+        return;
+    }
+}
+
+// Plan budget of one launch.
+struct Budget {
+    uint64_t sums, positions, fins, items;
+};
+
+struct Piece {
+    uint64_t a, b;
+    Request *r;
+    uint32_t bit;
+};
+
+// Plans the next run of pending windows of group g from its sweep cursor
+// (or from the start of the single request's remaining windows when
+// `cursorOverride` is set) into launch L. `used` counts the launch's
+// summary slots, positions, rows and work items so far; this group stops at
+// `limit` (its share), except that its first window may use anything left
+// under `cap`, so that every group with a resident table makes progress.
+void plan_group(ibs_server *s, Launch &L, Group &g, uint32_t view, const std::vector<Request *> &reqs,
+                const Budget &limit, const Budget &cap, Budget &used, uint32_t &nSingle, uint32_t &nJoint,
+                uint32_t &nFin, bool cursorOverride)
+{
+    const uint64_t NW = s->contigWin0.back();
+    std::vector<Piece> pieces;
+    for (Request *r : reqs)
+        for (auto &iv : r->remaining)
+            pieces.push_back(Piece{iv.first, iv.second, r, s->samples[r->sample].bit});
+    if (pieces.empty())
+        return;
+    uint64_t cursor = cursorOverride ? pieces.front().a : g.cursor;
+    uint64_t x0 = ~0ull;
+    for (auto &p : pieces)
+        if (p.b > cursor)
+            x0 = std::min(x0, std::max(p.a, cursor));
+    if (x0 == ~0ull) { // nothing at or after the cursor: wrap around
+        cursor = 0;
+        for (auto &p : pieces)
+            x0 = std::min(x0, p.a);
+    }
+    // masks and requester counts of windows [x0, x0 + span) from per-bit difference arrays
+    const uint64_t span = std::min<uint64_t>(NW - x0, 1u << 16);
+    const uint32_t nBits = g.joint ? g.nSamples : 1;
+    std::vector<int32_t> diff((size_t)nBits * (span + 1), 0);
+    for (auto &p : pieces) {
+        const uint64_t lo = std::max(p.a, x0), hi = std::min(p.b, x0 + span);
+        if (lo >= hi)
+            continue;
+        diff[(size_t)p.bit * (span + 1) + (lo - x0)]++;
+        diff[(size_t)p.bit * (span + 1) + (hi - x0)]--;
+    }
+    std::vector<int32_t> run(nBits, 0);
+    std::vector<uint32_t> maskOf, baseOf;
+    std::vector<uint64_t> sumOf;
+    uint64_t x1 = x0;
+    for (uint64_t x = x0; x < x0 + span; ++x) {
+        uint32_t m = 0, requesters = 0;
+        for (uint32_t b = 0; b < nBits; ++b) {
+            run[b] += diff[(size_t)b * (span + 1) + (x - x0)];
+            if (run[b] > 0) {
+                m |= 1u << b;
+                requesters += (uint32_t)run[b];
+            }
+        }
+        uint64_t base;
+        uint32_t nPos;
+        int32_t st, en;
+        s->window(x, base, nPos, st, en);
+        const uint64_t spans = (nPos + kSpanLen - 1) / kSpanLen;
+        const uint64_t slots = m ? spans * __builtin_popcount(m) : 0;
+        const uint64_t pos = m ? nPos : 0;
+        const uint64_t items = m ? spans : 0;
+        auto within = [&](const Budget &b) {
+            return used.sums + slots <= b.sums && used.positions + pos <= b.positions &&
+                   used.fins + requesters <= b.fins && used.items + items <= b.items;
+        };
+        if (!(within(limit) || (x == x0 && within(cap))))
+            break;
+        maskOf.push_back(m);
+        sumOf.push_back(used.sums);
+        if (m) {
+            for (uint64_t sp = 0; sp < spans; ++sp) {
+                WorkItem it;
+                it.base = base;
+                it.p0 = (uint32_t)(sp * kSpanLen);
+                it.p1 = std::min<uint32_t>(it.p0 + kSpanLen, nPos);
+                it.view = view;
+                it.mask = g.joint ? m : 1u;
+                it.out = used.sums + sp * __builtin_popcount(m);
+                if (g.joint)
+                    L.hJoint[nJoint++] = it;
+                else
+                    L.hSingle[nSingle++] = it;
+            }
+            used.sums += slots;
+            used.positions += pos;
+            used.items += items;
+            used.fins += requesters;
+            L.positions += pos;
+        }
+        x1 = x + 1;
+    }
+    // rows: every piece's windows inside [x0, x1)
+    for (auto &p : pieces) {
+        const uint64_t lo = std::max(p.a, x0), hi = std::min(p.b, x1);
+        if (lo >= hi)
+            continue;
+        for (uint64_t x = lo; x < hi; ++x) {
+            const uint32_t m = maskOf[x - x0];
+            uint64_t base;
+            uint32_t nPos;
+            FinItem &f = L.hFin[nFin++];
+            s->window(x, base, nPos, f.start, f.end);
+            f.nSpans = (nPos + kSpanLen - 1) / kSpanLen;
+            f.stride = __builtin_popcount(m);
+            f.sum = sumOf[x - x0] + __builtin_popcount(m & ((1u << p.bit) - 1u));
+            f.row = p.r->rowOff + (x - p.r->g0);
+        }
+        take(*p.r, lo, hi);
+        if (p.r->planned == p.r->nw)
+            L.finishing.push_back(p.r);
+    }
+    if (!cursorOverride)
+        g.cursor = x1 >= NW ? 0 : x1;
+}
+
+void fail_requests(ibs_server *s, const std::vector<Request *> &reqs, double t)
+{
+    for (Request *r : reqs) {
+        ibs_request_result res = result_of(*r, IBS_ERR_CUDA, t);
+        res.rows = static_cast<ibs_window *>(malloc(sizeof(ibs_window)));
+        s->rowAlloc.release(r->rowOff, r->nw);
+        s->st.completed++;
+        s->st.failed++;
+        s->done.push_back(res);
+        s->active.remove_if([r](const std::unique_ptr<Request> &p) { return p.get() == r; });
+    }
+    if (!reqs.empty())
+        s->doneCv.notify_all();
 }
 
 // One loop iteration: plans and enqueues a launch. Returns false when there
@@ -367,164 +627,116 @@ bool iterate(ibs_server *s)
 {
     Launch &L = s->launches[s->nextLaunch];
     retire(s, L); // its staging buffers are reused below
-    std::vector<Request *> runnable;
+    uint32_t nSingle = 0, nJoint = 0, nFin = 0, nSV = 0, nJV = 0;
+    L.positions = 0;
     {
         std::lock_guard<std::mutex> lock(s->mu);
-        // admit queued requests while the summary and row pools have room
+        // admit queued requests while the row pool has room
         while (!s->queue.empty() && !(s->serial && !s->active.empty())) {
             Request *r = s->queue.front().get();
-            uint64_t so, ro;
-            if (!s->sumAlloc.alloc(r->totalSpans, so))
+            uint64_t ro;
+            if (!s->rowAlloc.alloc(r->nw, ro))
                 break;
-            if (!s->rowAlloc.alloc(r->nw, ro)) {
-                s->sumAlloc.release(so, r->totalSpans);
-                break;
-            }
-            r->sumOff = so;
             r->rowOff = ro;
-            for (auto &f : r->win) {
-                f.sum += so;
-                f.row += ro;
-            }
-            r->admitted = true;
             s->active.push_back(std::move(s->queue.front()));
             s->queue.pop_front();
         }
-        const double t = s->now();
-        std::vector<Request *> failed;
+        // pending windows per group (one request in serial mode)
+        std::map<uint32_t, std::vector<Request *>> demand;
         for (auto &rp : s->active) {
-            Request *r = rp.get();
-            if (r->curWin == r->nw)
-                continue; // every span issued; its finalize is in flight
-            Sample &smp = *s->samples[r->sample];
-            if (!smp.dev) {
-                const ibs_status rs = make_resident(s, smp);
+            if (rp->remaining.empty())
+                continue; // every window planned; its last launch is in flight
+            demand[s->samples[rp->sample].group].push_back(rp.get());
+            if (s->serial)
+                break;
+        }
+        const double t = s->now();
+        std::vector<uint32_t> ready;
+        for (auto &d : demand) {
+            Group &g = *s->groups[d.first];
+            if (!g.dev) {
+                const ibs_status rs = make_resident(s, g);
                 if (rs == IBS_ERR_STATE)
                     continue; // every resident table is busy: retry after a retire
                 if (rs != IBS_OK) {
                     // a table that is not resident has no launch in flight,
-                    // so none of this request's spans is on the device
+                    // so none of these requests' windows is on the device
                     cudaGetLastError();
-                    failed.push_back(r);
+                    fail_requests(s, d.second, t);
                     continue;
                 }
             }
-            if (!table_ready(smp))
+            if (!table_ready(g))
                 continue;
-            smp.lastUse = t;
-            // claim the table for this launch now, so that making another
-            // request's table resident cannot evict it while we plan
-            if (std::find(L.tables.begin(), L.tables.end(), r->sample) == L.tables.end()) {
-                smp.inflight++;
-                L.tables.push_back(r->sample);
+            g.lastUse = t;
+            g.inflight++; // claimed: making another table resident cannot evict it now
+            L.groups.push_back(d.first);
+            ready.push_back(d.first);
+        }
+        if (ready.empty())
+            return false;
+        const Budget cap{kSumCap, kPosCap, kFinCap, s->itemCap};
+        Budget used{0, 0, 0, 0};
+        for (size_t i = 0; i < ready.size(); ++i) {
+            const uint32_t gi = ready[i];
+            Group &g = *s->groups[gi];
+            const uint64_t left = ready.size() - i; // fair share of what the groups before left over
+            const Budget limit{used.sums + (cap.sums - used.sums) / left,
+                               used.positions + (cap.positions - used.positions) / left,
+                               used.fins + (cap.fins - used.fins) / left,
+                               used.items + (cap.items - used.items) / left};
+            uint32_t view;
+            if (g.joint) {
+                view = nJV;
+                L.hJV[nJV++] = g.joint_view();
+            } else {
+                view = nSV;
+                L.hSV[nSV++] = g.single_view();
             }
-            runnable.push_back(r);
+            plan_group(s, L, g, view, demand[gi], limit, cap, used, nSingle, nJoint, nFin, s->serial);
         }
-        for (Request *r : failed) {
-            ibs_request_result res{};
-            res.request_id = r->id;
-            res.sample = r->sample;
-            res.contig = r->contig;
-            res.first_window = r->w0;
-            res.n_windows = 0;
-            res.status = IBS_ERR_CUDA;
-            res.submit_time = r->submitT;
-            res.done_time = t;
-            res.rows = static_cast<ibs_window *>(malloc(sizeof(ibs_window)));
-            s->sumAlloc.release(r->sumOff, r->totalSpans);
-            s->rowAlloc.release(r->rowOff, r->nw);
-            s->st.completed++;
-            s->st.failed++;
-            s->done.push_back(res);
-            s->active.remove_if([r](const std::unique_ptr<Request> &p) { return p.get() == r; });
-        }
-        if (!failed.empty())
-            s->doneCv.notify_all();
     }
-    if (runnable.empty()) {
-        std::lock_guard<std::mutex> lock(s->mu);
-        for (uint32_t id : L.tables)
-            s->samples[id]->inflight--;
-        L.tables.clear();
-        return false;
-    }
-    // spans: every runnable request gets a share of the launch
-    const uint64_t share =
-        s->serial ? ~0ull : std::max<uint64_t>(s->minPer, s->maxItems / runnable.size());
-    uint32_t nItems = 0, nFin = 0;
-    std::map<uint32_t, uint32_t> slot; // sample -> view index
-    L.probes = 0;
-    for (uint32_t i = 0; i < L.tables.size(); ++i) {
-        slot[L.tables[i]] = i;
-        L.hViews[i] = s->samples[L.tables[i]]->view();
-    }
-    for (Request *r : runnable) {
-        const uint32_t vi = slot[r->sample];
-        uint64_t taken = 0;
-        while (r->curWin < r->nw && taken < share && nItems < s->maxItems) {
-            const uint32_t nPos = r->winPos[r->curWin];
-            const uint64_t spans = (nPos + kSpanLen - 1) / kSpanLen;
-            if (r->curSpanInWin < spans) {
-                WorkItem &it = L.hItems[nItems++];
-                it.base = r->winBase[r->curWin];
-                it.p0 = (uint32_t)(r->curSpanInWin * kSpanLen);
-                it.p1 = std::min<uint32_t>(it.p0 + kSpanLen, nPos);
-                it.table = vi;
-                it.pad = 0;
-                it.out = r->win[r->curWin].sum + r->curSpanInWin;
-                L.probes += it.p1 - it.p0;
-                r->curSpanInWin++;
-                r->scheduled++;
-                taken++;
-            }
-            if (r->curSpanInWin >= spans) {
-                r->curWin++;
-                r->curSpanInWin = 0;
-            }
-        }
-        if (r->curWin == r->nw) { // last spans issued: finalize in this launch
-            for (uint64_t w = 0; w < r->nw; ++w)
-                L.hFin[nFin++] = r->win[w];
-            L.finishing.push_back(r);
-        }
-        if (nItems >= s->maxItems)
-            break;
-    }
-    L.nItems = nItems;
     cudaStream_t st = s->comp;
-    cudaMemcpyAsync(L.dViews, L.hViews, slot.size() * sizeof(TableView), cudaMemcpyHostToDevice, st);
-    if (nItems)
-        cudaMemcpyAsync(L.dItems, L.hItems, nItems * sizeof(WorkItem), cudaMemcpyHostToDevice, st);
+    if (nSV)
+        cudaMemcpyAsync(L.dSV, L.hSV, nSV * sizeof(TableView), cudaMemcpyHostToDevice, st);
+    if (nJV)
+        cudaMemcpyAsync(L.dJV, L.hJV, nJV * sizeof(panel::View), cudaMemcpyHostToDevice, st);
+    if (nSingle)
+        cudaMemcpyAsync(L.dSingle, L.hSingle, nSingle * sizeof(WorkItem), cudaMemcpyHostToDevice, st);
+    if (nJoint)
+        cudaMemcpyAsync(L.dJoint, L.hJoint, nJoint * sizeof(WorkItem), cudaMemcpyHostToDevice, st);
     if (nFin)
         cudaMemcpyAsync(L.dFin, L.hFin, nFin * sizeof(FinItem), cudaMemcpyHostToDevice, st);
     cudaEventRecord(L.start, st);
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (nItems) {
-        const int grid = (int)std::min<uint64_t>((nItems + 7) / 8, (uint64_t)sms * 8);
-        k_serve_spans<kNB><<<grid, 256, 0, st>>>(L.dViews, L.dItems, nItems, s->ref->dSeq, s->ref->dMask,
-                                                 s->dSums);
+    if (nSingle) {
+        const int grid = (int)std::min<uint64_t>((nSingle + 7) / 8, (uint64_t)s->sms * 8);
+        k_serve_single<kNB><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq, s->ref->dMask,
+                                                  L.dSums);
         IBS_LAUNCHED();
     }
-    cudaEventRecord(L.stop, st);
+    if (nJoint) {
+        const int grid = (int)std::min<uint64_t>((nJoint + 7) / 8, (uint64_t)s->sms * 8);
+        k_serve_joint<kNB><<<grid, 256, 0, st>>>(L.dJV, L.dJoint, nJoint, s->ref->dSeq, s->ref->dMask,
+                                                 L.dSums);
+        IBS_LAUNCHED();
+    }
     if (nFin) {
-        const int grid = (int)std::min<uint64_t>((nFin + 255) / 256, (uint64_t)sms * 8);
-        k_serve_finalize<<<grid, 256, 0, st>>>(L.dFin, nFin, s->dSums, (int)s->k, s->dRows);
+        const int grid = (int)std::min<uint64_t>((nFin + 255) / 256, (uint64_t)s->sms * 8);
+        k_serve_finalize<<<grid, 256, 0, st>>>(L.dFin, nFin, L.dSums, (int)s->k, s->dRows);
         IBS_LAUNCHED();
-        for (Request *r : L.finishing)
-            if (r->nw)
-                cudaMemcpyAsync(s->hRows + r->rowOff, s->dRows + r->rowOff, r->nw * sizeof(ibs_window),
-                                cudaMemcpyDeviceToHost, st);
-        cudaEventRecord(L.stop, st); // results ready
     }
+    for (Request *r : L.finishing)
+        if (r->nw)
+            cudaMemcpyAsync(s->hRows + r->rowOff, s->dRows + r->rowOff, r->nw * sizeof(ibs_window),
+                            cudaMemcpyDeviceToHost, st);
+    cudaEventRecord(L.stop, st);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         std::lock_guard<std::mutex> lock(s->mu);
         s->fatal = std::string("CUDA error in serving launch: ") + cudaGetErrorString(e);
     }
     s->st.launches++;
-    s->st.spans += nItems;
+    s->st.spans += nSingle + nJoint;
     L.active = true;
     s->nextLaunch = (s->nextLaunch + 1) % kDepth;
     return true;
@@ -558,37 +770,49 @@ void loop(ibs_server *s)
         retire(s, L);
 }
 
-ibs_status add_table(ibs_server *s, ibs_table *t, uint32_t *id)
+// Registers a device table (copied to a pinned host image) as a group of
+// n samples; returns the first sample id.
+ibs_status add_group(ibs_server *s, bool joint, uint32_t nSamples, const TableGeom &geom, uint64_t stashBuckets,
+                     const void *dBuckets, const void *dStash, uint32_t *first, ibs_panel_table *release = nullptr)
 {
-    std::unique_ptr<Sample> smp(new Sample);
-    smp->geom = t->geom;
-    smp->nKeys = t->nKeys;
-    smp->bucketBytes = t->geom.nBuckets * 32;
-    smp->stashBytes = t->geom.stashBuckets * 32;
-    IBS_CUDA(cudaMallocHost(&smp->host, smp->bytes()), "pinned table image");
-    IBS_CUDA(cudaMemcpy(smp->host, t->buckets, smp->bucketBytes, cudaMemcpyDeviceToHost), "table image");
-    if (smp->stashBytes)
-        IBS_CUDA(cudaMemcpy(static_cast<uint8_t *>(smp->host) + smp->bucketBytes, t->stash, smp->stashBytes,
-                            cudaMemcpyDeviceToHost),
-                 "table image");
-    IBS_CUDA(cudaEventCreateWithFlags(&smp->loaded, cudaEventDisableTiming), "event create");
-    std::lock_guard<std::mutex> lock(s->mu);
-    if (s->samples.size() >= 4096) {
-        set_error("server: at most 4096 samples");
-        return IBS_ERR_CAPACITY;
-    }
-    if (smp->bytes() > s->budget) {
-        set_error("server: this sample's table is larger than the memory budget");
-        return IBS_ERR_CAPACITY;
-    }
-    if (t->geom.k != s->k) {
-        set_error("server: sample k differs from the server's k");
+    if (geom.k != s->k) {
+        set_error("server: the table's k differs from the server's k");
         return IBS_ERR_ARG;
     }
-    smp->id = (uint32_t)s->samples.size();
-    *id = smp->id;
-    s->samples.push_back(std::move(smp));
-    Sample &ref = *s->samples.back();
+    std::unique_ptr<Group> g(new Group);
+    g->joint = joint;
+    g->nSamples = nSamples;
+    g->geom = geom;
+    g->stashBuckets = stashBuckets;
+    g->bucketBytes = geom.nBuckets * 32;
+    g->stashBytes = (joint ? stashBuckets : geom.stashBuckets) * 32;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->groups.size() >= kMaxGroups || s->samples.size() + nSamples > kMaxGroups) {
+            set_error("server: at most 4096 samples");
+            return IBS_ERR_CAPACITY;
+        }
+        if (g->bytes() > s->budget) {
+            set_error("server: this table is larger than the memory budget");
+            return IBS_ERR_CAPACITY;
+        }
+    }
+    IBS_CUDA(cudaMallocHost(&g->host, g->bytes()), "pinned table image");
+    IBS_CUDA(cudaMemcpy(g->host, dBuckets, g->bucketBytes, cudaMemcpyDeviceToHost), "table image");
+    if (g->stashBytes)
+        IBS_CUDA(cudaMemcpy(static_cast<uint8_t *>(g->host) + g->bucketBytes, dStash, g->stashBytes,
+                            cudaMemcpyDeviceToHost),
+                 "table image");
+    IBS_CUDA(cudaEventCreateWithFlags(&g->loaded, cudaEventDisableTiming), "event create");
+    if (release)
+        panel_release_table(release);
+    std::lock_guard<std::mutex> lock(s->mu);
+    g->id = (uint32_t)s->groups.size();
+    *first = (uint32_t)s->samples.size();
+    for (uint32_t b = 0; b < nSamples; ++b)
+        s->samples.push_back(SampleRef{g->id, b});
+    s->groups.push_back(std::move(g));
+    Group &ref = *s->groups.back();
     if (s->resident + ref.bytes() <= s->budget) {
         ibs_status st = make_resident(s, ref);
         if (st != IBS_OK)
@@ -617,12 +841,9 @@ extern "C" ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t
     s->k = k;
     DeviceGuard guard(s->device);
     if (opts && opts->max_spans_per_launch)
-        s->maxItems = opts->max_spans_per_launch;
-    if (opts && opts->min_spans_per_request)
-        s->minPer = opts->min_spans_per_request;
+        s->itemCap = std::min<uint64_t>(opts->max_spans_per_launch, kSumCap);
     s->serial = opts && opts->one_request_per_launch;
-    if (s->serial)
-        s->maxItems = std::max<uint32_t>(s->maxItems, (uint32_t)kSumPool);
+    cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
     size_t fr = 0, tot = 0;
     IBS_CUDA(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
     s->budget = (opts && opts->memory_budget) ? opts->memory_budget : (uint64_t)(fr * 0.8);
@@ -632,21 +853,26 @@ extern "C" ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t
     IBS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "mempool");
     IBS_CUDA(cudaStreamCreateWithFlags(&s->comp, cudaStreamNonBlocking), "stream create");
     IBS_CUDA(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking), "stream create");
-    IBS_CUDA(cudaMalloc(&s->dSums, kSumPool * sizeof(SegStats)), "summary pool");
     IBS_CUDA(cudaMalloc(&s->dRows, kRowPool * sizeof(ibs_window)), "row pool");
     IBS_CUDA(cudaMallocHost(&s->hRows, kRowPool * sizeof(ibs_window)), "pinned row pool");
     for (auto &L : s->launches) {
         IBS_CUDA(cudaEventCreate(&L.start), "event create");
         IBS_CUDA(cudaEventCreate(&L.stop), "event create");
-        IBS_CUDA(cudaMallocHost(&L.hItems, s->maxItems * sizeof(WorkItem)), "pinned staging");
-        IBS_CUDA(cudaMallocHost(&L.hFin, kRowPool * sizeof(FinItem)), "pinned staging");
-        IBS_CUDA(cudaMallocHost(&L.hViews, 4096 * sizeof(TableView)), "pinned staging");
-        IBS_CUDA(cudaMalloc(&L.dItems, s->maxItems * sizeof(WorkItem)), "staging");
-        IBS_CUDA(cudaMalloc(&L.dFin, kRowPool * sizeof(FinItem)), "staging");
-        IBS_CUDA(cudaMalloc(&L.dViews, 4096 * sizeof(TableView)), "staging");
+        IBS_CUDA(cudaMallocHost(&L.hSingle, kSumCap * sizeof(WorkItem)), "pinned staging");
+        IBS_CUDA(cudaMallocHost(&L.hJoint, kSumCap * sizeof(WorkItem)), "pinned staging");
+        IBS_CUDA(cudaMallocHost(&L.hFin, kFinCap * sizeof(FinItem)), "pinned staging");
+        IBS_CUDA(cudaMallocHost(&L.hSV, kMaxGroups * sizeof(TableView)), "pinned staging");
+        IBS_CUDA(cudaMallocHost(&L.hJV, kMaxGroups * sizeof(panel::View)), "pinned staging");
+        IBS_CUDA(cudaMalloc(&L.dSingle, kSumCap * sizeof(WorkItem)), "staging");
+        IBS_CUDA(cudaMalloc(&L.dJoint, kSumCap * sizeof(WorkItem)), "staging");
+        IBS_CUDA(cudaMalloc(&L.dFin, kFinCap * sizeof(FinItem)), "staging");
+        IBS_CUDA(cudaMalloc(&L.dSV, kMaxGroups * sizeof(TableView)), "staging");
+        IBS_CUDA(cudaMalloc(&L.dJV, kMaxGroups * sizeof(panel::View)), "staging");
+        IBS_CUDA(cudaMalloc(&L.dSums, kSumCap * sizeof(SegStats)), "summary pool");
     }
+    s->contigWin0.push_back(0);
     for (size_t c = 0; c < ref->lens.size(); ++c)
-        s->contigWin.push_back({windows_in_contig(ref->lens[c], W, k)});
+        s->contigWin0.push_back(s->contigWin0.back() + windows_in_contig(ref->lens[c], W, k));
     ibs_server *raw = s.get();
     s->worker = std::thread(loop, raw);
     *out = s.release();
@@ -669,7 +895,7 @@ extern "C" ibs_status ibs_server_add_sample_codes(ibs_server *s, const uint64_t 
     if (st != IBS_OK)
         return st;
     DeviceGuard guard(s->device);
-    st = add_table(s, t, id);
+    st = add_group(s, false, 1, t->geom, 0, t->buckets, t->stash, id);
     ibs_close(t);
     return st;
 }
@@ -689,8 +915,36 @@ extern "C" ibs_status ibs_server_add_sample_kmc(ibs_server *s, const char *prefi
     if (st != IBS_OK)
         return st;
     DeviceGuard guard(s->device);
-    st = add_table(s, t, id);
+    st = add_group(s, false, 1, t->geom, 0, t->buckets, t->stash, id);
     ibs_close(t);
+    return st;
+}
+
+extern "C" ibs_status ibs_server_add_panel(ibs_server *s, ibs_panel_table *p, int release_panel,
+                                           uint32_t *first_id)
+{
+    clear_error();
+    if (!s || !p || !first_id) {
+        set_error("ibs_server_add_panel: bad argument");
+        return IBS_ERR_ARG;
+    }
+    if (p->nSamples == 0) {
+        set_error("ibs_server_add_panel: the panel table holds no samples");
+        return IBS_ERR_ARG;
+    }
+    if (p->device != s->device) {
+        set_error("ibs_server_add_panel: the panel table is on another device");
+        return IBS_ERR_ARG;
+    }
+    if (!p->buckets) {
+        set_error("ibs_server_add_panel: the panel's table was already released");
+        return IBS_ERR_STATE;
+    }
+    DeviceGuard guard(s->device);
+    // the host image first; then, when asked, the panel's device copy goes
+    // before the server uploads its own, so that one copy is on the device
+    ibs_status st = add_group(s, true, p->nSamples, p->geom, p->stashBuckets, p->buckets, p->stash, first_id,
+                              release_panel ? p : nullptr);
     return st;
 }
 
@@ -709,48 +963,39 @@ extern "C" ibs_status ibs_server_submit(ibs_server *s, uint32_t sample, uint32_t
             set_error(s->fatal);
             return IBS_ERR_CUDA;
         }
-        if (sample >= s->samples.size() || contig >= s->contigWin.size()) {
+        if (sample >= s->samples.size() || contig + 1 >= s->contigWin0.size()) {
             set_error("ibs_server_submit: unknown sample or contig");
             return IBS_ERR_ARG;
         }
     }
-    const uint64_t nwC = s->contigWin[contig][0];
+    const uint64_t nwC = s->contigWin0[contig + 1] - s->contigWin0[contig];
     if (first > nwC || (first == nwC && nwC)) {
         set_error("ibs_server_submit: first window beyond the contig");
         return IBS_ERR_ARG;
     }
     if (n == 0 || first + n > nwC)
         n = nwC - first;
+    if (n > kRowPool) {
+        set_error("ibs_server_submit: request larger than the server's row pool (split it)");
+        return IBS_ERR_CAPACITY;
+    }
+    if (((uint64_t)s->W + kSpanLen - 1) / kSpanLen * IBS_PANEL_MAX_SAMPLES > kSumCap) {
+        set_error("ibs_server_submit: windows this long do not fit one launch");
+        return IBS_ERR_CAPACITY;
+    }
     r->sample = sample;
     r->contig = contig;
     r->w0 = first;
     r->nw = n;
-    const uint64_t L = s->ref->lens[contig];
-    const uint64_t step = (uint64_t)s->W - s->k;
-    uint64_t spans = 0;
-    r->win.resize(n);
-    r->winBase.resize(n);
-    r->winPos.resize(n);
-    for (uint64_t i = 0; i < n; ++i) {
-        const uint64_t j = (first + i) * step;
-        const uint64_t end = std::min<uint64_t>(j + s->W, L);
-        const uint64_t nb = end - j;
-        const uint32_t nPos = nb >= s->k ? (uint32_t)(nb - s->k + 1) : 0;
-        FinItem &f = r->win[i];
-        f.sum = spans;
-        f.nSpans = (nPos + kSpanLen - 1) / kSpanLen;
-        f.start = (int32_t)j;
-        f.end = (int32_t)end;
-        f.pad = 0;
-        f.row = i;
-        r->winBase[i] = s->ref->baseOff[contig] + j;
-        r->winPos[i] = nPos;
-        spans += f.nSpans;
-    }
-    r->totalSpans = spans;
-    if (spans > kSumPool || n > kRowPool) {
-        set_error("ibs_server_submit: request larger than the server's pools (split it)");
-        return IBS_ERR_CAPACITY;
+    r->g0 = s->contigWin0[contig] + first;
+    if (n)
+        r->remaining.push_back({r->g0, r->g0 + n});
+    for (uint64_t x = r->g0; x < r->g0 + n; ++x) {
+        uint64_t base;
+        uint32_t nPos;
+        int32_t a, b;
+        s->window(x, base, nPos, a, b);
+        r->positions += nPos;
     }
     std::lock_guard<std::mutex> lock(s->mu);
     r->id = s->nextId++;
@@ -759,13 +1004,7 @@ extern "C" ibs_status ibs_server_submit(ibs_server *s, uint32_t sample, uint32_t
         *request_id = r->id;
     s->st.submitted++;
     if (n == 0) { // an empty contig has no windows: done at once
-        ibs_request_result res{};
-        res.request_id = r->id;
-        res.sample = sample;
-        res.contig = contig;
-        res.first_window = first;
-        res.status = IBS_OK;
-        res.submit_time = res.done_time = r->submitT;
+        ibs_request_result res = result_of(*r, IBS_OK, r->submitT);
         res.rows = static_cast<ibs_window *>(malloc(sizeof(ibs_window)));
         s->latencies.push_back(0.0);
         s->st.completed++;
@@ -837,8 +1076,8 @@ extern "C" ibs_status ibs_server_stats_get(ibs_server *s, ibs_server_stats *out)
     *out = s->st;
     out->resident_bytes = s->resident;
     uint64_t n = 0;
-    for (auto &smp : s->samples)
-        n += smp->dev ? 1 : 0;
+    for (auto &g : s->groups)
+        n += g->dev ? 1 : 0;
     out->resident_tables = n;
     out->latency_p50 = percentile(s->latencies, 0.50);
     out->latency_p99 = percentile(s->latencies, 0.99);
@@ -865,24 +1104,32 @@ extern "C" void ibs_server_close(ibs_server *s)
         DeviceGuard guard(s->device);
         cudaStreamSynchronize(s->comp);
         cudaStreamSynchronize(s->side);
-        for (auto &smp : s->samples) {
-            if (smp->dev)
-                cudaFreeAsync(smp->dev, s->side);
-            cudaFreeHost(smp->host);
-            cudaEventDestroy(smp->loaded);
+        for (auto &g : s->groups) {
+            if (g->dev)
+                cudaFreeAsync(g->dev, s->side);
+            cudaFreeHost(g->host);
+            cudaEventDestroy(g->loaded);
         }
         cudaStreamSynchronize(s->side);
+        // hand the tables' pool memory back, so that later allocations see it
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess)
+            cudaMemPoolTrimTo(pool, 0);
         for (auto &L : s->launches) {
             cudaEventDestroy(L.start);
             cudaEventDestroy(L.stop);
-            cudaFreeHost(L.hItems);
+            cudaFreeHost(L.hSingle);
+            cudaFreeHost(L.hJoint);
             cudaFreeHost(L.hFin);
-            cudaFreeHost(L.hViews);
-            cudaFree(L.dItems);
+            cudaFreeHost(L.hSV);
+            cudaFreeHost(L.hJV);
+            cudaFree(L.dSingle);
+            cudaFree(L.dJoint);
             cudaFree(L.dFin);
-            cudaFree(L.dViews);
+            cudaFree(L.dSV);
+            cudaFree(L.dJV);
+            cudaFree(L.dSums);
         }
-        cudaFree(s->dSums);
         cudaFree(s->dRows);
         cudaFreeHost(s->hRows);
         cudaStreamDestroy(s->comp);

@@ -3,17 +3,22 @@
 // A canonical k-mer C is filed under its minimizer: among C's w = k - 15
 // 16-mers, the one whose canonical form has the smallest bijective 32-bit
 // hash h (ties: the leftmost in C). Consecutive reference positions mostly
-// share their minimizer (a "super-k-mer" of ~ (w+1)/2 positions), so they
-// land in the same 32-byte bucket and a warp's loads collapse onto a few
-// DRAM sectors.
+// share their minimizer (runs of up to w positions), so their probes fall in
+// one place of the table.
 //
-// The slot value identifies C exactly inside its bucket: bucket =
-// floor(h * nBuckets / 2^32), so the low hbits of h single out h (hence the
-// canonical minimizer M) among the bucket's hash interval; C is then M at
-// offset o, in orientation s (M or its reverse complement), with the other
-// k-16 bases around it:
-//   slot = ((o << 1 | s) << 2(k-16) | C-without-the-16-mer) << hbits | (h mod 2^hbits)
-// which must fit 31 bits (B8x32 sentinels): nBuckets >= 2^(2k-26).
+// The table is an array of 128-byte lines of four 32-byte sectors; a sector
+// is a B8x32 bucket. The minimizer picks the line and C itself picks one of
+// its four sectors, so a minimizer's k-mers (up to w of them, too many for
+// one 8-slot sector) spread over the line, and a warp's loads for a run of
+// positions touch one DRAM line.
+//
+// The slot value identifies C exactly inside its line: with g = spread(h)
+// (a bijection of 32-bit values), line = floor(g * nLines / 2^32), so the
+// low hbits of g single out g, hence h and the canonical minimizer M, among
+// the line's interval; C is then M at offset o, in orientation s (M or its
+// reverse complement), with the other k-16 bases around it:
+//   slot = ((o << 1 | s) << 2(k-16) | C-without-the-16-mer) << hbits | (g mod 2^hbits)
+// which must fit 31 bits (B8x32 sentinels): nLines >= 2^(2k-26).
 #pragma once
 
 #include "ibs_core.cuh"
@@ -89,11 +94,28 @@ IBS_HD void minimizer(uint64_t C, uint32_t k, uint32_t &h, uint32_t &o)
     }
 }
 
-IBS_HD uint64_t bucket_of_h(uint32_t h, uint64_t nBuckets) { return ((uint64_t)h * nBuckets) >> 32; }
+// A minimizer's hash is the smallest of w hashes, so minimizer hashes crowd
+// towards 0; the line is taken from a bijective remix of it, which is
+// uniform over the minimizers again. Being a bijection, the remix (hence h)
+// is still identified by (line, its low hbits).
+IBS_HD uint32_t spread(uint32_t h) { return (uint32_t)perm_hash(h ^ 0x6a09e667u, 32); }
+
+constexpr uint32_t kSectorsPerLine = 4;
+
+IBS_HD uint64_t line_of_h(uint32_t h, uint64_t nLines) { return ((uint64_t)spread(h) * nLines) >> 32; }
+
+// Sector of C inside its line: two well-mixed bits of the code.
+IBS_HD uint32_t sector_of(uint64_t C) { return (uint32_t)((C * 0x9e3779b97f4a7c15ull) >> 62); }
+
+// Bucket (32-byte sector index) of canonical k-mer C with minimizer hash h.
+IBS_HD uint64_t bucket_of_h(uint32_t h, uint64_t C, uint64_t nBuckets)
+{
+    return line_of_h(h, nBuckets / kSectorsPerLine) * kSectorsPerLine + sector_of(C);
+}
 
 IBS_HD uint32_t slot_value(uint32_t high, uint32_t h, uint32_t hbits)
 {
-    return (high << hbits) | (h & (uint32_t)key_mask(hbits));
+    return (high << hbits) | (spread(h) & (uint32_t)key_mask(hbits));
 }
 
 // Slot value and bucket of a canonical k-mer.
@@ -101,7 +123,7 @@ IBS_HD void locate(uint64_t C, const TableGeom &g, uint64_t &bucket, uint32_t &s
 {
     uint32_t h, o;
     minimizer(C, g.k, h, o);
-    bucket = bucket_of_h(h, g.nBuckets);
+    bucket = bucket_of_h(h, C, g.nBuckets);
     slot = slot_value(slot_high(C, g.k, o), h, g.fpBits);
 }
 

@@ -65,7 +65,7 @@ class ServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "launches", "spans", "probes", "reloads",
                                           "reload_bytes", "evictions", "resident_bytes", "resident_tables")] + \
                [(n, C.c_double) for n in ("busy_seconds", "latency_p50", "latency_p99", "latency_max")] + \
-               [(n, C.c_uint64) for n in ("failed", "queued", "running")]
+               [(n, C.c_uint64) for n in ("failed", "queued", "running", "scanned")]
 
 
 class Tuning(C.Structure):
@@ -159,6 +159,7 @@ _ibs_srv_create = _sig(_lib, "ibs_server_create", C.c_int,
                        [vp, C.c_uint32, C.c_uint32, C.POINTER(ServerOpts), C.POINTER(vp)])
 _ibs_srv_add_kmc = _sig(_lib, "ibs_server_add_sample_kmc", C.c_int, [vp, C.c_char_p, u32p])
 _ibs_srv_add_codes = _sig(_lib, "ibs_server_add_sample_codes", C.c_int, [vp, vp, C.c_uint64, C.c_int, u32p])
+_ibs_srv_add_panel = _sig(_lib, "ibs_server_add_panel", C.c_int, [vp, vp, C.c_int, u32p])
 _ibs_srv_submit = _sig(_lib, "ibs_server_submit", C.c_int,
                        [vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, u64p])
 _ibs_srv_poll = _sig(_lib, "ibs_server_poll", C.c_int,
@@ -569,6 +570,15 @@ class Server:
         i = C.c_uint32()
         _check(_ibs_srv_add_kmc(self._h, str(prefix).encode(), C.byref(i)))
         return i.value
+
+    def add_panel(self, panel: "PanelTable", release: bool = False) -> list[int]:
+        """Registers every sample of a joint panel table; returns their ids.
+        With release=True the panel's device table is freed first (the panel
+        then only accepts close())."""
+        ns = panel.info()[1]
+        i = C.c_uint32()
+        _check(_ibs_srv_add_panel(self._h, panel._h, int(release), C.byref(i)))
+        return list(range(i.value, i.value + ns))
 
     def submit(self, sample: int, contig: int, first_window: int = 0, n_windows: int = 0) -> int:
         rid = C.c_uint64()

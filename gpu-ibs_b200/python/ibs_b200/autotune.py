@@ -60,11 +60,11 @@ def sweep(scale: float = 0.25, reps: int = 3, quick: bool = False) -> dict:
     stream = torch.cuda.Stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     base = get_tuning()
-    layouts = [(1, 4.0), (4, 4.0)] if quick else [(1, 3.0), (1, 4.0), (1, 5.0), (4, 3.0), (4, 4.0), (4, 5.0)]
+    layouts = [(1, 3.0), (4, 3.0)] if quick else [(1, 3.0), (1, 4.0), (4, 2.0), (4, 3.0), (4, 4.0)]
     shapes = list(itertools.product([2048, 4096, 16384] if not quick else [4096],
                                     [2, 4] if quick else [1, 2, 4, 8],
-                                    [256] if quick else [128, 256, 512],
-                                    [4, 8] if quick else [2, 4, 8, 16]))
+                                    [256, 512] if quick else [128, 256, 512],
+                                    [8, 16] if quick else [4, 8, 16]))
     points, reference_rows = [], None
     for fmt, kpb in layouts:
         table = Table.from_codes(codes.data_ptr(), n, k, on_device=True, force_format=fmt, keys_per_bucket=kpb)

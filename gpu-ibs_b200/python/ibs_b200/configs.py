@@ -74,7 +74,7 @@ def plain_2gbp(scale: float = 1.0) -> Workload:
 PANEL_4GBP_LENS = [750, 450, 600, 700, 550, 650, 500]
 
 
-def panel_4gbp(n_samples: int = 16, scale: float = 1.0) -> Workload:
+def panel_4gbp(n_samples: int = 16, scale: float = 1.0, sample_scale: float = 1.0) -> Workload:
     lens = [int(x * MB * scale) for x in PANEL_4GBP_LENS]
     ref = RefSpec(seed=3, lens=lens, n_frac=0.01, n_run=(50, 500),
                   names=[f"chr{i + 1}H" for i in range(len(lens))])
@@ -82,7 +82,7 @@ def panel_4gbp(n_samples: int = 16, scale: float = 1.0) -> Workload:
     positions = sum(lens)
     samples = []
     for s in range(n_samples):
-        target = math.exp(rng.uniform(math.log(0.3e9), math.log(2.1e9))) * scale
+        target = math.exp(rng.uniform(math.log(0.3e9), math.log(2.1e9))) * scale * sample_scale
         present = min(1.0, target / (positions * 1.10))
         intro = []
         for _ in range(int(rng.integers(2, 6))):
@@ -93,5 +93,7 @@ def panel_4gbp(n_samples: int = 16, scale: float = 1.0) -> Workload:
         samples.append(SampleSpec(seed=3000 + s, k=31, class_rate=BLOCK_RATES, class_prob=BLOCK_PROBS,
                                   block_len=1 * MB, present_frac=present, random_frac=0.10,
                                   intro=intro, intro_rate=0.0001))
-    return Workload("panel_4gbp", ref, samples, dict(k=31, p=7, sig_len=9, n_bins=512, counter_size=1),
-                    description=f"4.2 Gbp x {n_samples} samples of 0.3e9-2.1e9 k=31 k-mers, W=50 kbp")
+    name = "panel_4gbp" if sample_scale == 1.0 else f"panel_4gbp_samples_x{sample_scale:g}"
+    return Workload(name, ref, samples, dict(k=31, p=7, sig_len=9, n_bins=512, counter_size=1),
+                    description=f"4.2 Gbp x {n_samples} samples of {0.3 * sample_scale:g}e9-"
+                                f"{2.1 * sample_scale:g}e9 k=31 k-mers, W=50 kbp")

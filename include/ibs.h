@@ -242,6 +242,8 @@ typedef struct ibs_server_stats {
     double latency_p50, latency_p99, latency_max; /* seconds, completed requests */
     uint64_t failed;                  /* completed with a non-OK status (a table reload failed) */
     uint64_t queued, running;         /* waiting for admission / admitted and not yet complete */
+    uint64_t scanned;                 /* reference positions the device scanned: a window that several
+                                         requests share counts once (probes counts it per request) */
 } ibs_server_stats;
 
 ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t k, const ibs_server_opts *opts,
@@ -251,6 +253,16 @@ ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t k, const i
 ibs_status ibs_server_add_sample_kmc(ibs_server *s, const char *kmc_prefix, uint32_t *sample_id);
 ibs_status ibs_server_add_sample_codes(ibs_server *s, const uint64_t *codes, uint64_t n,
                                        int codes_on_device, uint32_t *sample_id);
+/* Registers every sample of a joint panel table; the server keeps its own
+ * pinned host image and device copy. The samples get ids first_sample_id ..
+ * first_sample_id + n - 1 in the panel's order. Requests for samples of one
+ * panel that cover the same windows are scanned together: one bucket load
+ * per position answers all of them. With release_panel != 0 the panel's own
+ * device table is freed before the server uploads its copy (one copy on the
+ * device at a time); the panel handle then only accepts ibs_panel_table_close
+ * (other calls return IBS_ERR_STATE). */
+ibs_status ibs_server_add_panel(ibs_server *s, ibs_panel_table *panel, int release_panel,
+                                uint32_t *first_sample_id);
 /* Windows [first_window, first_window + n_windows) of contig `contig`
  * (window i starts at i * (W - k)); n_windows = 0 means to the contig's end. */
 ibs_status ibs_server_submit(ibs_server *s, uint32_t sample, uint32_t contig, uint64_t first_window,

@@ -52,11 +52,12 @@ def build_case(case_root):
 @pytest.fixture(scope="session")
 def native_shim():
     """tests/native/fold_shim.so: the window-statistics fold of
-    gpu-ibs_b200/csrc/ibs_core.cuh compiled for the host."""
+    gpu-ibs_b200/csrc/ibs_core.cuh and the minimizer key map of mz_core.cuh
+    compiled for the host."""
     src = REPO / "tests" / "native" / "fold_shim.cpp"
     out = REPO / "tests" / "native" / "fold_shim.so"
-    if not out.exists() or out.stat().st_mtime < max(src.stat().st_mtime,
-                                                       (REPO / "gpu-ibs_b200/csrc/ibs_core.cuh").stat().st_mtime):
+    deps = [src, REPO / "gpu-ibs_b200/csrc/ibs_core.cuh", REPO / "gpu-ibs_b200/csrc/mz_core.cuh"]
+    if not out.exists() or out.stat().st_mtime < max(d.stat().st_mtime for d in deps):
         subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-o", str(out), str(src),
                         f"-I{REPO / 'gpu-ibs_b200' / 'csrc'}"], check=True)
     import ctypes

@@ -62,8 +62,8 @@ static TableGeom mz_geom(uint32_t k, uint64_t nBuckets)
     g.k = k;
     g.bits = 2 * k;
     g.format = FMT_MZ8;
-    g.nBuckets = nBuckets;
-    g.fpBits = 32 - (63 - __builtin_clzll(nBuckets));
+    g.nBuckets = nBuckets; // a multiple of the four sectors of a line
+    g.fpBits = 32 - (63 - __builtin_clzll(nBuckets / mz::kSectorsPerLine));
     return g;
 }
 
@@ -115,7 +115,7 @@ extern "C" void mz_query(const uint8_t *bases, uint64_t n, uint32_t k, uint64_t 
                 jr = j;
         }
         const uint32_t o = isFwd ? jl : (w - 1 - jr);
-        bucket[q] = mz::bucket_of_h(mn, g.nBuckets);
+        bucket[q] = mz::bucket_of_h(mn, C, g.nBuckets);
         slot[q] = mz::slot_value(mz::slot_high(C, k, o), mn, g.fpBits);
     }
     delete[] h;

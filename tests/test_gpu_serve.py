@@ -105,3 +105,59 @@ def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world):
     assert st["evictions"] > 0 and st["reloads"] > 0, st
     assert st["latency_p99"] >= st["latency_p50"] > 0
     srv.close()
+
+
+def make_panel_server(world, serial=False):
+    """The six samples as one joint panel table, plus sample 0 once more as a
+    single-sample table (id 6), in one server."""
+    union = len(np.unique(np.concatenate(world["samples"])))
+    pt = ib.PanelTable(K, union)
+    for c in world["samples"]:
+        pt.add_codes(c, len(c), on_device=False)
+    srv = ib.Server(world["ref"], W, K, one_request_per_launch=serial)
+    ids = srv.add_panel(pt, release=serial)  # either way the server keeps its own copy
+    if serial:
+        with pytest.raises(ib.IbsError) as e:
+            pt.probe(world["samples"][0][:10])
+        assert e.value.status == 9
+    pt.close()
+    assert ids == list(range(6))
+    c = world["samples"][0]
+    assert srv.add_codes(c, len(c), on_device=False) == 6
+    return srv
+
+
+def expected_any(world, r):
+    s = r["sample"] if r["sample"] < 6 else 0
+    rows = world["full"][s]
+    a = world["starts"][r["contig"]] + r["first_window"]
+    return rows[a:a + r["n_windows"]]
+
+
+@pytest.mark.parametrize("serial", [False, True])
+def test_panel_server_alone_and_in_a_mix(world, serial):
+    srv = make_panel_server(world, serial)
+    # alone
+    for req in random_requests(world, 10, 3):
+        srv.submit(*req)
+        got = srv.poll(1, timeout_ms=60_000)
+        assert len(got) == 1, ("no result within 60 s", req, srv.stats())
+        assert got[0]["status"] == 0
+        assert np.array_equal(got[0]["rows"], expected_any(world, got[0])), req
+    # a burst that overlaps heavily: every sample (and the single-table copy) over the same regions
+    reqs = [(s, c, 0, 0) for c in (0, 1, 5) for s in range(7)] + random_requests(world, 60, 4)
+    for req in reqs:
+        srv.submit(*req)
+    done, deadline = [], time.time() + 300
+    while len(done) < len(reqs) and time.time() < deadline:
+        done += srv.poll(64, timeout_ms=2000)
+    assert len(done) == len(reqs), ("requests left unfinished", srv.stats())
+    for r in done:
+        assert r["status"] == 0
+        assert np.array_equal(r["rows"], expected_any(world, r)), (r["sample"], r["contig"], r["first_window"])
+    st = srv.stats()
+    if serial:
+        assert st["scanned"] == st["probes"]  # one request per launch: nothing shared
+    else:
+        assert st["scanned"] < st["probes"]  # windows shared between requests were scanned once
+    srv.close()

@@ -38,7 +38,7 @@ def query(shim, bases, k, nb):
 @pytest.mark.parametrize("k", [16, 21, 25, 27])
 def test_query_side_equals_build_side(native_shim, k):
     rng = np.random.default_rng(k)
-    nb = 1 << max(2 * k - 26, 20)
+    nb = 4 << max(2 * k - 26, 20)  # four sectors per line, nLines >= 2^(2k-26)
     # random sequence plus repeats that force minimizer ties
     seq = rng.integers(0, 4, 200_000).astype(np.uint8)
     unit = rng.integers(0, 4, 17).astype(np.uint8)
@@ -56,10 +56,31 @@ def test_query_side_equals_build_side(native_shim, k):
 @pytest.mark.parametrize("k", [20, 25, 27])
 def test_bucket_and_slot_identify_the_kmer(native_shim, k):
     rng = np.random.default_rng(100 + k)
-    nb = 1 << max(2 * k - 26, 18)
+    nb = 4 << max(2 * k - 26, 18)
     codes = np.unique(corpus.random_codes(rng, 400_000, k))
     b, s = locate(native_shim, codes, k, nb)
     assert (b < nb).all()
     assert (s < (1 << 31)).all(), "slot values must stay below the B8x32 sentinels"
     pairs = b.astype(np.uint64) * np.uint64(1 << 32) + s.astype(np.uint64)
     assert len(np.unique(pairs)) == len(codes)
+
+
+def test_buckets_are_uniform_over_minimizers(native_shim):
+    # k-mers of one sequence cluster by minimizer; the clusters must spread
+    # evenly over the buckets (a minimizer's hash is biased towards 0)
+    k, nb = 25, 1 << 18
+    rng = np.random.default_rng(7)
+    seq = rng.integers(0, 4, 1_000_000).astype(np.uint8)
+    qb, _ = query(native_shim, seq, k, nb)
+    lines = qb >> np.uint64(2)  # four 32-byte sectors per line
+    keys = np.unique(lines)  # lines touched, one per distinct minimizer (mostly)
+    frac_low = (keys < nb // 8).mean()
+    assert 0.47 < frac_low < 0.53
+    counts = np.bincount(lines.astype(np.int64), minlength=nb // 4)
+    # load of the first and last eighths of the lines agree within 5%
+    a, b = counts[: nb // 32].sum(), counts[-nb // 32:].sum()
+    assert abs(a - b) / max(a, b) < 0.05
+    # the sector inside a line comes from the k-mer: a run of positions sharing
+    # a minimizer spreads over the line's four sectors
+    sectors = np.bincount((qb & np.uint64(3)).astype(np.int64), minlength=4) / len(qb)
+    assert (abs(sectors - 0.25) < 0.01).all()
