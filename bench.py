@@ -394,7 +394,8 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
                   "table": {"format": int(info.format), "buckets": int(info.n_buckets),
                             "fp_bits": int(info.fp_bits), "stash_keys": int(info.stash_keys),
                             "device_gb": info.device_bytes / 1e9, "build_s": t_build},
-                  "rows_checksum_observed": checksum, "gen_s": t_gen},
+                  "rows_checksum_observed": checksum, "gen_s": t_gen,
+                  "tuning": getattr(args, "tuning_used", None)},
     }
     if cpu is not None:
         out["cpu_baseline"] = cpu
@@ -545,17 +546,20 @@ def panel_arm(args, rank: int):
 
 
 def served_arm(args, rank: int):
-    """Served scan stream: the 4.2 Gbp panel reference and a pool of 16
-    resident samples; Poisson arrivals; each request one sample and a region
-    log-uniform from 1 Mbp to a whole contig. The batching server over joint
+    """Served scan stream: a reference and a pool of 16 resident samples
+    (served_2gbp by default); Poisson arrivals; each request one sample and a
+    region log-uniform from 1 Mbp to a whole contig. The batching server over joint
     panel tables (requests sharing windows are scanned together) against the
     plain path (per-sample tables, one request per launch) on the same GPU.
     Every result is checked against its sample's full-scan rows."""
     import torch
     import ibs_b200 as ib
     from ibs_b200 import configs
-    w = configs.panel_4gbp(n_samples=args.serve_samples, scale=args.serve_scale,
-                           sample_scale=args.serve_sample_scale)
+    if args.serve_workload == "served_2gbp":
+        w = configs.served_2gbp(n_samples=args.serve_samples, scale=args.serve_scale)
+    else:
+        w = configs.panel_4gbp(n_samples=args.serve_samples, scale=args.serve_scale,
+                               sample_scale=args.serve_sample_scale)
     k, W = w.k, w.window
     lens = w.ref.lens
     sw, mw = w.ref.packed_words()
@@ -653,9 +657,11 @@ def served_arm(args, rank: int):
            "arrival_rate_per_s": args.serve_rate, "region": "log-uniform 1 Mbp .. whole contig",
            "setup_s": setup_s}
 
-    # plain path: per-sample tables, one request per launch
+    # plain path: per-sample tables, one request per launch. The budget
+    # leaves room for registering a sample (its codes and a transient table)
     free, _ = torch.cuda.mem_get_info()
-    srv = ib.Server(ref, W, k, memory_budget=int(free * 0.85), one_request_per_launch=True)
+    transient = max_bound * 8 + ib.table_bytes_for(max(n_keys), k) * 2 + (4 << 30)
+    srv = ib.Server(ref, W, k, memory_budget=int(free - transient), one_request_per_launch=True)
     for i in range(n_samples):
         buf, n = codes(i)
         srv.add_codes(buf.data_ptr(), n, on_device=True)
@@ -686,7 +692,7 @@ def served_arm(args, rank: int):
         cur.append(i)
     groups.append(cur)
     del sampled
-    srv = ib.Server(ref, W, k, memory_budget=int(free * 0.85))
+    srv = ib.Server(ref, W, k, memory_budget=int(free - max_bound * 8 - (8 << 30)))
     id_of = {}
     for members in groups:
         pt = ib.PanelTable(k, union_of[tuple(members)], keys_per_bucket=kpb)
@@ -759,6 +765,25 @@ def reference_arm(args, w):
     }
 
 
+def apply_tuning(args):
+    """The scan's launch shape and table layout: the committed autotuner
+    result (or a given file), then any explicit flag on top."""
+    import ibs_b200 as ib
+    from ibs_b200 import autotune
+    applied = None
+    if args.tuning != "none":
+        path = None if args.tuning == "auto" else args.tuning
+        applied = autotune.apply(path)
+    t = ib.get_tuning()
+    for name in ("span_len", "blocks_in_flight", "block_threads", "ctas_per_sm"):
+        v = getattr(args, name)
+        if v:
+            setattr(t, name, v)
+    ib.set_tuning(t)
+    args.tuning_used = {**t.as_dict(), "source": "flags over " + (args.tuning if applied else "library defaults")}
+    log(f"[bench] tuning {args.tuning_used}")
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -773,6 +798,13 @@ def main():
     ap.add_argument("--table-format", type=int, default=0,
                     help="sample table layout: 0 library default, 1 B8x32, 2 B6x40, 4 minimizer-bucketed")
     ap.add_argument("--keys-per-bucket", type=float, default=0.0, help="table load (0: library default)")
+    ap.add_argument("--tuning", default="auto",
+                    help="launch shape: 'auto' = the committed gpu-ibs_b200/tuning/b200.json when present, "
+                         "'none' = library defaults, or a path")
+    ap.add_argument("--span-len", type=int, default=0)
+    ap.add_argument("--blocks-in-flight", type=int, default=0)
+    ap.add_argument("--block-threads", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--panel", action="store_true", help="also measure the 16-sample batched panel")
     ap.add_argument("--panel-only", action="store_true")
     ap.add_argument("--panel-samples", type=int, default=16)
@@ -784,8 +816,11 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=50.0)
     ap.add_argument("--serve-scale", type=float, default=1.0, help="reference length scale")
+    ap.add_argument("--serve-workload", choices=["served_2gbp", "panel_4gbp"], default="served_2gbp",
+                    help="the pool: the 2 Gbp reference with 16 samples, or the 4.2 Gbp panel's")
     ap.add_argument("--serve-sample-scale", type=float, default=0.5,
-                    help="sample size scale (the 16 full-size samples do not fit on one GPU together)")
+                    help="panel_4gbp pool: sample size scale (its 16 full-size samples do not fit "
+                         "on one GPU together)")
     args = ap.parse_args()
 
     from ibs_b200 import configs
@@ -803,6 +838,7 @@ def main():
         print(json.dumps(reference_arm(args, w)), flush=True)
         return 0
 
+    apply_tuning(args)
     if world > 1:
         import datetime
         import torch

@@ -814,11 +814,14 @@ ibs_status add_group(ibs_server *s, bool joint, uint32_t nSamples, const TableGe
     s->groups.push_back(std::move(g));
     Group &ref = *s->groups.back();
     if (s->resident + ref.bytes() <= s->budget) {
-        ibs_status st = make_resident(s, ref);
-        if (st != IBS_OK)
-            return st;
-        s->st.reloads--; // the first load is not a reload
-        s->st.reload_bytes -= ref.bytes();
+        // resident now if the device has room; otherwise on its first request
+        if (make_resident(s, ref) == IBS_OK) {
+            s->st.reloads--; // the first load is not a reload
+            s->st.reload_bytes -= ref.bytes();
+        } else {
+            cudaGetLastError();
+            clear_error();
+        }
     }
     return IBS_OK;
 }

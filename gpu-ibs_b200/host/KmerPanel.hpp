@@ -1,10 +1,12 @@
 // KmerPanel: N sample databases scanned against a reference in one pass
 // (the reference's panel mode, src/KmerPanel.hpp): the reference is read and
-// packed once and uploaded once, the databases are taken in rounds of as many
-// as fit the device (or --resident=N), and each round is one ibs_scan_panel
-// call over the resident tables. Every database's TSV is the file a single
-// run writes (the same Window records through the same writer). A single
-// round stays resident for the next reference, as the reference does
+// packed once and uploaded once, the databases are taken in rounds of up to
+// 16 that fit the device (or --resident=N), and each round is ONE joint
+// table (ibs_panel_table: every key once, with a mask of the samples that
+// hold it) scanned in one pass: one bucket load per position serves the
+// whole round. Every database's TSV is the file a single run writes (the
+// same Window records through the same writer). A single round stays
+// resident for the next reference, as the reference does
 // (src/KmerPanel.hpp:122-135, :213-222).
 #pragma once
 
@@ -99,21 +101,17 @@ public:
         for (size_t r = 0; r < rounds.size(); r++) {
             const std::vector<size_t> &round = rounds[r];
             auto t0 = std::chrono::steady_clock::now();
-            std::vector<ibs_table *> tables;
-            for (size_t i : round) {
-                members[i].db->initGpuIndex();
-                tables.push_back(members[i].db->gpuTable());
-            }
+            if (!joint)
+                buildJoint(round);
             const double setupSec = since(t0);
             setupTotal += setupSec;
 
             t0 = std::chrono::steady_clock::now();
             std::cout << "Calculating stats" << std::endl;
             std::vector<ibs_window> rows(std::max<uint64_t>(1, nWin * round.size()));
-            KmerDatabase::check(ibs_scan_panel(tables.data(), (uint32_t)tables.size(), dref,
-                                               (uint32_t)windowSize, rows.data(),
-                                               nWin * round.size()),
-                                "ibs_scan_panel");
+            KmerDatabase::check(ibs_panel_table_scan(joint, dref, (uint32_t)windowSize, rows.data(),
+                                                     nWin * round.size()),
+                                "ibs_panel_table_scan");
             const double statsSec = since(t0);
             statsTotal += statsSec;
 
@@ -131,8 +129,7 @@ public:
             const double writeSec = since(t0);
             writeTotal += writeSec;
             if (rounds.size() > 1)
-                for (size_t i : round)
-                    members[i].db->releaseGpuIndex();
+                releaseAll();
             std::cout << "[panel] round " << r + 1 << "/" << rounds.size() << ": " << round.size()
                       << " databases, setup " << setupSec << " s, stats " << statsSec
                       << " s, write " << writeSec << " s" << std::endl;
@@ -157,12 +154,50 @@ private:
     std::vector<Member> members;
     int residentCap = 0;
     std::vector<size_t> keptResident;
+    ibs_panel_table *joint = nullptr; // the current round's table
+    static constexpr double kKeysPerBucket = 3.0;
 
+public:
+    ~KmerPanel() { releaseAll(); }
+
+private:
     void releaseAll()
     {
-        for (auto &m : members)
-            m.db->releaseGpuIndex();
+        if (joint) {
+            ibs_panel_table_close(joint);
+            joint = nullptr;
+        }
         keptResident.clear();
+    }
+
+    // Upper bound of a member's share of a joint table: its keys at the
+    // table's load in 32-byte buckets, plus the overflow stash.
+    static uint64_t jointBytes(uint64_t keys) { return (uint64_t)(keys / kKeysPerBucket * 32 * 1.15); }
+
+    // One joint table of the round's databases. Its size is planned for the
+    // sum of their key counts (the union is at most that; the stash grows
+    // if the planning is short).
+    void buildJoint(const std::vector<size_t> &round)
+    {
+        uint64_t keys = 0;
+        for (size_t i : round)
+            keys += members[i].db->kmcInfo().totalKmers;
+        ibs_table_opts o{};
+        o.device = KmerDatabase::gpuOptions().device;
+        o.keys_per_bucket = kKeysPerBucket;
+        const auto t0 = std::chrono::steady_clock::now();
+        KmerDatabase::check(ibs_panel_table_create(kmerSize(), keys, &o, &joint), "ibs_panel_table_create");
+        for (size_t i : round)
+            KmerDatabase::check(ibs_panel_table_add_kmc(joint, members[i].prefix.c_str()),
+                                "ibs_panel_table_add_kmc");
+        ibs_table_info ti{};
+        uint32_t ns = 0;
+        ibs_panel_table_info_get(joint, &ti, &ns);
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        char msg[200];
+        snprintf(msg, sizeof msg, "[gpu] joint table of %u databases: %.3f s (%llu k-mers, %.2f GB on device %d)",
+                 ns, sec, (unsigned long long)ti.n_keys, ti.device_bytes / 1e9, o.device);
+        std::cout << msg << std::endl;
     }
 
     // Resident sets in order: the longest run of what is left whose tables
@@ -171,7 +206,7 @@ private:
     // reports the shortfall (src/KmerPanel.hpp:282-363).
     std::vector<std::vector<size_t>> planRounds(const std::vector<size_t> &active) const
     {
-        size_t cap = active.size();
+        size_t cap = std::min<size_t>(active.size(), IBS_PANEL_MAX_SAMPLES);
         if (residentCap > 0)
             cap = std::min<size_t>(cap, (size_t)residentCap);
         uint64_t freeBytes = 0, totalBytes = 0;
@@ -183,9 +218,8 @@ private:
         uint64_t curBytes = 0;
         for (size_t i : active) {
             const auto &info = members[i].db->kmcInfo();
-            // the table plus ~2% stash, and the build's transient decode buffer
-            const uint64_t bytes =
-                ibs_table_bytes_for(info.totalKmers, info.kmerLength, nullptr) * 102 / 100;
+            // its share of the joint table, and the build's transient decode buffer
+            const uint64_t bytes = jointBytes(info.totalKmers);
             bool fits = cur.size() < cap;
             if (fits && known)
                 fits = curBytes + bytes + margin + info.totalKmers * 8 <= freeBytes || cur.empty();

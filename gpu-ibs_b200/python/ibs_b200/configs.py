@@ -16,6 +16,9 @@ reference and sample is generated from a seed (see include/ibs_tools.h):
                   16 samples of 0.3e9-2.1e9 k=31 k-mers (log-uniform sizes via
                   block presence), own seeds, 2-5 introgression blocks of
                   1-20 Mbp at 0.01%; KMC p=7.
+* served_2gbp  -- the plain_2gbp reference and 16 samples of its block model
+                  with their own seeds, log-uniform 0.15e9-1.0e9 k=25 k-mers:
+                  the served stream's resident pool.
 """
 from __future__ import annotations
 
@@ -97,3 +100,22 @@ def panel_4gbp(n_samples: int = 16, scale: float = 1.0, sample_scale: float = 1.
     return Workload(name, ref, samples, dict(k=31, p=7, sig_len=9, n_bins=512, counter_size=1),
                     description=f"4.2 Gbp x {n_samples} samples of {0.3 * sample_scale:g}e9-"
                                 f"{2.1 * sample_scale:g}e9 k=31 k-mers, W=50 kbp")
+
+
+def served_2gbp(n_samples: int = 16, scale: float = 1.0) -> Workload:
+    """The served stream's pool: the plain_2gbp reference and n samples made
+    by its block-divergence model with their own seeds, sized log-uniform
+    0.15e9-1.0e9 k=25 k-mers (panel_4gbp's 0.3e9-2.1e9 scaled to the 2 Gbp
+    reference), so that all of them stay resident on one GPU."""
+    base = plain_2gbp(scale)
+    rng = np.random.default_rng(404)
+    positions = sum(base.ref.lens)
+    samples = []
+    for s in range(n_samples):
+        target = math.exp(rng.uniform(math.log(0.15e9), math.log(1.0e9))) * scale
+        samples.append(SampleSpec(seed=4000 + s, k=25, class_rate=BLOCK_RATES, class_prob=BLOCK_PROBS,
+                                  block_len=1 * MB, present_frac=min(1.0, target / (positions * 1.10)),
+                                  random_frac=0.10))
+    return Workload("served_2gbp" if scale == 1.0 else f"served_2gbp_x{scale:g}", base.ref, samples,
+                    base.kmc, description=f"{sum(base.ref.lens) / 1e9:.3g} Gbp x {n_samples} samples of "
+                                          f"0.15e9-1.0e9 k=25 k-mers, W=50 kbp")
