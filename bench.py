@@ -412,7 +412,10 @@ def panel_arm(args, rank: int):
     import torch
     import ibs_b200 as ib
     from ibs_b200 import configs
-    w = configs.panel_4gbp(n_samples=args.panel_samples, scale=args.panel_scale)
+    if args.panel_workload == "served_2gbp":
+        w = configs.served_2gbp(n_samples=args.panel_samples, scale=args.panel_scale)
+    else:
+        w = configs.panel_4gbp(n_samples=args.panel_samples, scale=args.panel_scale)
     k, W = w.k, w.window
     lens = w.ref.lens
     runs = w.ref.n_runs()
@@ -810,6 +813,8 @@ def main():
     ap.add_argument("--panel-samples", type=int, default=16)
     ap.add_argument("--panel-scale", type=float, default=1.0)
     ap.add_argument("--panel-keys-per-bucket", type=float, default=3.0)
+    ap.add_argument("--panel-workload", choices=["panel_4gbp", "served_2gbp"], default="panel_4gbp",
+                    help="panel_4gbp (k=31); served_2gbp's 16 k=25 samples make small profiling cases")
     ap.add_argument("--serve", action="store_true", help="also measure the served request stream")
     ap.add_argument("--serve-only", action="store_true")
     ap.add_argument("--serve-samples", type=int, default=16)

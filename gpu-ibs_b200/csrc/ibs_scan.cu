@@ -167,25 +167,30 @@ __global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t 
     }
 }
 
-// 16-mer hash at packed base G (its canonical form's 32-bit bijective hash).
-__device__ __forceinline__ uint32_t mmer_hash_at(const uint64_t *__restrict__ seq, uint64_t G)
+// The m-mer starting at packed base G: its rank key, and its line hash with
+// its orientation bits on top (bit 62: the forward m-mer is not canonical,
+// bit 63: its reverse complement is not; 2m <= 42 leaves them free).
+__device__ __forceinline__ uint32_t mmer_at_base(const uint64_t *__restrict__ seq, uint64_t G, uint32_t m,
+                                                 uint64_t &gs)
 {
     const uint64_t wi = G >> 5;
     const uint32_t sh = (uint32_t)(G & 31) * 2;
     const uint64_t x = (__ldg(seq + wi) >> sh) | ((__ldg(seq + wi + 1) << (63 - sh)) << 1);
-    const uint32_t lo = (uint32_t)x; // 16 bases, first at the low bits
-    uint32_t f = __brev(lo);
-    f = ((f >> 1) & 0x55555555u) | ((f & 0x55555555u) << 1); // first base high
-    const uint32_t r = ~lo;
-    return mz::hash16(f < r ? f : r);
+    uint64_t y = __brevll(x);
+    y = ((y >> 1) & 0x5555555555555555ull) | ((y & 0x5555555555555555ull) << 1);
+    const uint64_t f = y >> (64 - 2 * m);     // first base high
+    const uint64_t r = ~x & key_mask(2 * m);  // its reverse complement
+    const uint64_t c = f < r ? f : r;
+    gs = mz::line_hash(c, m) | (f > r ? 1ull << 62 : 0ull) | (r > f ? 1ull << 63 : 0ull);
+    return mz::rank_key(c, m);
 }
 
-// The scan over a minimizer-bucketed table (format MZ8). Each lane hashes the
-// 16-mer starting at its position one block ahead; a k-mer's minimizer is
-// the minimum over the next w lanes' hashes (shuffles across the block
+// The scan over a minimizer-bucketed table (format MZ8). Each lane keys the
+// m-mer starting at its position one block ahead; a k-mer's minimizer is
+// the minimum over the next w lanes' keys (shuffles across the block
 // boundary), tracked with its leftmost and rightmost offsets so the
 // leftmost-in-the-canonical-k-mer rule holds on either strand. Lanes whose
-// k-mers share a minimizer load the same bucket; the hardware merges them.
+// k-mers share a minimizer load sectors of one line.
 template <int NB>
 __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64_t *__restrict__ seq,
                                                        const uint64_t *__restrict__ mask,
@@ -199,6 +204,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
     const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const uint32_t k = t.g.k;
     const uint32_t w = mz::w_of(k);
+    const uint32_t m = mz::m_of(k);
     const uint64_t kmask = key_mask(2 * k);
     const uint64_t kbits = (1ull << k) - 1;
     for (uint64_t s = s0 + warp; s < s1; s += nWarps) {
@@ -207,16 +213,20 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
         const uint32_t nPos = win[wIdx].nPos;
         const uint32_t p0 = (uint32_t)(s - __ldg(span0 + wIdx)) * spanLen;
         const uint32_t p1 = min(p0 + spanLen, nPos);
-        const uint32_t lastM = nPos - 1 + (w - 1); // last 16-mer start the window's k-mers use
+        const uint32_t lastM = nPos - 1 + (w - 1); // last m-mer start the window's k-mers use
         SegStats acc = seg_empty();
-        uint32_t hNext = mmer_hash_at(seq, base + min(p0 + lane, lastM));
+        uint64_t gNext;
+        uint32_t hNext = mmer_at_base(seq, base + min(p0 + lane, lastM), m, gNext);
         for (uint32_t p = p0; p < p1; p += 32 * NB) {
             uint32_t hb[NB + 1];
+            uint64_t hg[NB + 1];
             hb[0] = hNext;
+            hg[0] = gNext;
 #pragma unroll
             for (int b = 1; b <= NB; ++b)
-                hb[b] = mmer_hash_at(seq, base + min(p + 32 * b + lane, lastM));
+                hb[b] = mmer_at_base(seq, base + min(p + 32 * b + lane, lastM), m, hg[b]);
             hNext = hb[NB];
+            gNext = hg[NB];
             uint4 v0[NB], v1[NB];
             uint64_t code[NB];
             uint32_t slot[NB];
@@ -240,10 +250,10 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                 const bool isFwd = fwd <= rc;
                 code[b] = isFwd ? fwd : rc;
                 valid[b] = inSpan && (mm & kbits) == 0;
-                // minimizer over the w 16-mers starting at q .. q+w-1
+                // minimizer over the w (<= 8) m-mers starting at q .. q+w-1
                 uint32_t mn = 0xffffffffu, jl = 0, jr = 0;
 #pragma unroll
-                for (uint32_t j = 0; j < 16; ++j) {
+                for (uint32_t j = 0; j < 8; ++j) {
                     if (j < w) {
                         const uint32_t src = lane + j;
                         const uint32_t a = __shfl_sync(FULL, hb[b], src & 31);
@@ -256,9 +266,16 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                             jr = j;
                     }
                 }
+                // the minimizer's line hash and orientation from the lane that
+                // keyed it: position q + jl (forward k-mer) or q + jr (reverse)
+                const uint32_t src = lane + (isFwd ? jl : jr);
+                const uint64_t ga = __shfl_sync(FULL, hg[b], src & 31);
+                const uint64_t gc = __shfl_sync(FULL, hg[b + 1], src & 31);
+                const uint64_t gs = src < 32 ? ga : gc;
+                const uint32_t sm = isFwd ? (uint32_t)(gs >> 62) & 1u : (uint32_t)(gs >> 63);
                 const uint32_t o = isFwd ? jl : (w - 1 - jr);
-                const uint64_t r = mz::bucket_of_h(mn, code[b], t.g.nBuckets);
-                slot[b] = mz::slot_value(mz::slot_high(code[b], k, o), mn, t.g.fpBits);
+                uint64_t r;
+                mz::place(code[b], k, o, sm, gs & ((1ull << 62) - 1), t.g.nBuckets, t.g.fpBits, r, slot[b]);
                 if (valid[b]) {
                     v0[b] = __ldg(t.buckets + 2 * r);
                     v1[b] = __ldg(t.buckets + 2 * r + 1);

@@ -75,14 +75,15 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
     if (fmt == FMT_AUTO_HASH)
         fmt = 0;
     if (fmt == FMT_MZ8) {
-        // minimizer lines of four sectors: the slot value needs nLines >= 2^(2k-26)
+        // minimizer lines of four sectors: the slot value needs nLines >= 2^(2k-27)
         g.format = FMT_MZ8;
-        const uint64_t minLines = g.bits > 26 ? (1ull << (g.bits - 26)) : 1;
+        const uint32_t m = mz::m_of(k);
+        const uint64_t minLines = g.bits > 27 ? (1ull << (g.bits - 27)) : 1;
         const uint64_t nLines =
             std::min<uint64_t>(std::max((n8 + mz::kSectorsPerLine - 1) / mz::kSectorsPerLine, minLines),
-                               1ull << 32);
+                               1ull << std::min<uint32_t>(2 * m, 40));
         g.nBuckets = nLines * mz::kSectorsPerLine;
-        g.fpBits = (uint32_t)std::max<int>(1, 32 - (int)floor_log2(nLines));
+        g.fpBits = 2 * m - floor_log2(nLines);
         g.stashBuckets = 0;
         return g;
     }

@@ -1,24 +1,29 @@
 // Minimizer-bucketed table (format MZ8): the key -> (bucket, slot) map.
 //
-// A canonical k-mer C is filed under its minimizer: among C's w = k - 15
-// 16-mers, the one whose canonical form has the smallest bijective 32-bit
-// hash h (ties: the leftmost in C). Consecutive reference positions mostly
-// share their minimizer (runs of up to w positions), so their probes fall in
-// one place of the table.
+// A canonical k-mer C is filed under its minimizer: among C's w = k - m + 1
+// m-mers (m = k - 6 from k = 22, else 16), the one whose canonical form has
+// the smallest rank key -- the top 32 bits of a bijective multiplicative mix
+// of the 2m-bit code -- ties going to the leftmost in C. Consecutive
+// reference positions mostly share their minimizer (runs of up to w
+// positions), so their probes fall in one place of the table. m grows with k so that a minimizer rarely occurs at
+// two loci of a large genome (4^19 19-mers against 2e9 positions), which
+// would pile two runs into one place.
 //
 // The table is an array of 128-byte lines of four 32-byte sectors; a sector
 // is a B8x32 bucket. The minimizer picks the line and C itself picks one of
-// its four sectors, so a minimizer's k-mers (up to w of them, too many for
-// one 8-slot sector) spread over the line, and a warp's loads for a run of
-// positions touch one DRAM line.
+// its four sectors, so a minimizer's k-mers spread over the line and a
+// warp's loads for a run of positions touch one DRAM line.
 //
-// The slot value identifies C exactly inside its line: with g = spread(h)
-// (a bijection of 32-bit values), line = floor(g * nLines / 2^32), so the
-// low hbits of g single out g, hence h and the canonical minimizer M, among
-// the line's interval; C is then M at offset o, in orientation s (M or its
-// reverse complement), with the other k-16 bases around it:
-//   slot = ((o << 1 | s) << 2(k-16) | C-without-the-16-mer) << hbits | (g mod 2^hbits)
-// which must fit 31 bits (B8x32 sentinels): nLines >= 2^(2k-26).
+// The slot value identifies C exactly inside its line: with g = line_hash(M)
+// (a second bijection of the 2m-bit canonical minimizer M, independent of the
+// rank key, whose minimum over w m-mers is biased towards 0), line =
+// floor(g * nLines / 2^2m), so the low hbits = 2m - log2(nLines) bits of g
+// single out g, hence M, among the line's interval; C is then M at offset
+// o (< w <= 8), in orientation s (M or its reverse complement), with the
+// other k - m bases around it:
+//   slot = ((o << 1 | s) << 2(k-m) | C-without-the-m-mer) << hbits | (g mod 2^hbits)
+// which has 2k + 4 - log2(nLines) bits and must fit 31 (B8x32 sentinels):
+// nLines >= 2^(2k-27).
 #pragma once
 
 #include "ibs_core.cuh"
@@ -26,105 +31,121 @@
 namespace ibs {
 namespace mz {
 
-constexpr uint32_t M = 16; // minimizer length: a 16-mer is one 32-bit word
+constexpr uint32_t kSectorsPerLine = 4;
 
-IBS_HD uint32_t w_of(uint32_t k) { return k - M + 1; }
+IBS_HD uint32_t m_of(uint32_t k) { return k >= 22 ? k - 6 : 16; }
+IBS_HD uint32_t w_of(uint32_t k) { return k - m_of(k) + 1; }
 
-IBS_HD uint32_t brev32(uint32_t x)
+IBS_HD uint64_t brev64(uint64_t x)
 {
 #if defined(__CUDA_ARCH__)
-    return __brev(x);
+    return __brevll(x);
 #else
-    x = ((x >> 1) & 0x55555555u) | ((x & 0x55555555u) << 1);
-    x = ((x >> 2) & 0x33333333u) | ((x & 0x33333333u) << 2);
-    x = ((x >> 4) & 0x0f0f0f0fu) | ((x & 0x0f0f0f0fu) << 4);
-    x = ((x >> 8) & 0x00ff00ffu) | ((x & 0x00ff00ffu) << 8);
-    return (x >> 16) | (x << 16);
+    x = ((x >> 1) & 0x5555555555555555ull) | ((x & 0x5555555555555555ull) << 1);
+    x = ((x >> 2) & 0x3333333333333333ull) | ((x & 0x3333333333333333ull) << 2);
+    x = ((x >> 4) & 0x0f0f0f0f0f0f0f0full) | ((x & 0x0f0f0f0f0f0f0f0full) << 4);
+    x = ((x >> 8) & 0x00ff00ff00ff00ffull) | ((x & 0x00ff00ff00ff00ffull) << 8);
+    x = ((x >> 16) & 0x0000ffff0000ffffull) | ((x & 0x0000ffff0000ffffull) << 16);
+    return (x >> 32) | (x << 32);
 #endif
 }
 
-// Reverse complement of a 16-mer code (first base in the high bits).
-IBS_HD uint32_t rc16(uint32_t v)
+// Reverse complement of an m-mer code (first base in the high bits).
+IBS_HD uint64_t rc_m(uint64_t v, uint32_t m)
 {
-    uint32_t y = brev32(v);
-    y = ((y >> 1) & 0x55555555u) | ((y & 0x55555555u) << 1);
-    return ~y;
+    uint64_t y = brev64(v);
+    y = ((y >> 1) & 0x5555555555555555ull) | ((y & 0x5555555555555555ull) << 1);
+    return ~y >> (64 - 2 * m);
 }
 
-IBS_HD uint32_t canon16(uint32_t v)
+IBS_HD uint64_t canon_m(uint64_t v, uint32_t m)
 {
-    const uint32_t r = rc16(v);
+    const uint64_t r = rc_m(v, m);
     return v < r ? v : r;
 }
 
-IBS_HD uint32_t hash16(uint32_t canonical) { return (uint32_t)perm_hash(canonical, 32); }
-
-// The 16-mer of C (2k-bit code, first base high) at offset o.
-IBS_HD uint32_t mmer_at(uint64_t C, uint32_t k, uint32_t o)
+// The 32-bit key minimizers are chosen by: the top bits of a bijective mix
+// (odd multiply, xorshift) of the canonical m-mer. Cheap on purpose: the scan
+// computes one per reference position.
+IBS_HD uint32_t rank_key(uint64_t canonical, uint32_t m)
 {
-    return (uint32_t)(C >> (2 * (k - M - o)));
+    uint64_t x = (canonical * 0x9e3779b97f4a7c15ull) & key_mask(2 * m);
+    x ^= x >> m;
+    return (uint32_t)(x >> (2 * m - 32));
 }
 
-// (o, s, C without the 16-mer) part of the slot value, given the offset.
-IBS_HD uint32_t slot_high(uint64_t C, uint32_t k, uint32_t o)
+// The line hash of a canonical m-mer: a second bijection of the 2m-bit
+// values, two multiply-xorshift rounds, so the lines stay uniform over the
+// (low-key-biased) minimizers.
+IBS_HD uint64_t line_hash(uint64_t canonical, uint32_t m)
 {
-    const uint32_t mm = mmer_at(C, k, o);
-    const uint32_t s = mm != canon16(mm) ? 1u : 0u;
-    const uint32_t rbits = 2 * (k - M - o);                    // bases right of the 16-mer
+    const uint64_t mask = key_mask(2 * m);
+    uint64_t x = (canonical * 0xd6e8feb86659fd93ull) & mask;
+    x ^= x >> m;
+    x = (x * 0xbf58476d1ce4e5b9ull) & mask;
+    x ^= x >> m;
+    return x;
+}
+
+// The m-mer of C (2k-bit code, first base high) at offset o.
+IBS_HD uint64_t mmer_at(uint64_t C, uint32_t k, uint32_t o, uint32_t m)
+{
+    return (C >> (2 * (k - m - o))) & key_mask(2 * m);
+}
+
+// (o, s, C without the m-mer) part of the slot value: the minimizer's
+// offset o in C and its orientation s there (1 when it reads as the reverse
+// complement of its canonical form).
+IBS_HD uint32_t slot_high(uint64_t C, uint32_t k, uint32_t o, uint32_t s)
+{
+    const uint32_t m = m_of(k);
+    const uint32_t rbits = 2 * (k - m - o);                    // bases right of the m-mer
     const uint64_t right = rbits ? (C & ((1ull << rbits) - 1)) : 0;
     const uint64_t left = C >> (2 * (k - o));                  // bases left of it (2o bits)
-    const uint64_t rest = (left << rbits) | right;             // 2(k-16) bits
-    return (uint32_t)((((uint64_t)o << 1 | s) << (2 * (k - M))) | rest);
+    const uint64_t rest = (left << rbits) | right;             // 2(k-m) bits
+    return (uint32_t)((((uint64_t)o << 1 | s) << (2 * (k - m))) | rest);
 }
 
-// Minimizer of C by brute force (table build, single probes): hash and
-// leftmost offset.
-IBS_HD void minimizer(uint64_t C, uint32_t k, uint32_t &h, uint32_t &o)
+// Minimizer offset of C by brute force (table build, single probes): the
+// leftmost m-mer with the smallest rank key.
+IBS_HD uint32_t minimizer_offset(uint64_t C, uint32_t k)
 {
-    h = 0xffffffffu;
-    o = 0;
-    bool first = true;
+    const uint32_t m = m_of(k);
+    uint32_t best = 0xffffffffu, o = 0;
     for (uint32_t j = 0; j < w_of(k); ++j) {
-        const uint32_t v = hash16(canon16(mmer_at(C, k, j)));
-        if (first || v < h) {
-            h = v;
+        const uint32_t v = rank_key(canon_m(mmer_at(C, k, j, m), m), m);
+        if (j == 0 || v < best) {
+            best = v;
             o = j;
-            first = false;
         }
     }
+    return o;
 }
-
-// A minimizer's hash is the smallest of w hashes, so minimizer hashes crowd
-// towards 0; the line is taken from a bijective remix of it, which is
-// uniform over the minimizers again. Being a bijection, the remix (hence h)
-// is still identified by (line, its low hbits).
-IBS_HD uint32_t spread(uint32_t h) { return (uint32_t)perm_hash(h ^ 0x6a09e667u, 32); }
-
-constexpr uint32_t kSectorsPerLine = 4;
-
-IBS_HD uint64_t line_of_h(uint32_t h, uint64_t nLines) { return ((uint64_t)spread(h) * nLines) >> 32; }
 
 // Sector of C inside its line: two well-mixed bits of the code.
 IBS_HD uint32_t sector_of(uint64_t C) { return (uint32_t)((C * 0x9e3779b97f4a7c15ull) >> 62); }
 
-// Bucket (32-byte sector index) of canonical k-mer C with minimizer hash h.
-IBS_HD uint64_t bucket_of_h(uint32_t h, uint64_t C, uint64_t nBuckets)
+// Bucket (32-byte sector index) and slot value of canonical k-mer C whose
+// minimizer sits at offset o with orientation s and line hash g.
+// hbits = 2m - log2(nLines).
+IBS_HD void place(uint64_t C, uint32_t k, uint32_t o, uint32_t s, uint64_t g, uint64_t nBuckets,
+                  uint32_t hbits, uint64_t &bucket, uint32_t &slot)
 {
-    return line_of_h(h, nBuckets / kSectorsPerLine) * kSectorsPerLine + sector_of(C);
+    const uint32_t m = m_of(k);
+    const uint64_t line = mulhi64(g << (64 - 2 * m), nBuckets / kSectorsPerLine);
+    bucket = line * kSectorsPerLine + sector_of(C);
+    slot = (slot_high(C, k, o, s) << hbits) | (uint32_t)(g & key_mask(hbits));
 }
 
-IBS_HD uint32_t slot_value(uint32_t high, uint32_t h, uint32_t hbits)
-{
-    return (high << hbits) | (spread(h) & (uint32_t)key_mask(hbits));
-}
-
-// Slot value and bucket of a canonical k-mer.
+// Slot value and bucket of a canonical k-mer (the build side, and single
+// probes): everything from C itself.
 IBS_HD void locate(uint64_t C, const TableGeom &g, uint64_t &bucket, uint32_t &slot)
 {
-    uint32_t h, o;
-    minimizer(C, g.k, h, o);
-    bucket = bucket_of_h(h, C, g.nBuckets);
-    slot = slot_value(slot_high(C, g.k, o), h, g.fpBits);
+    const uint32_t m = m_of(g.k);
+    const uint32_t o = minimizer_offset(C, g.k);
+    const uint64_t mm = mmer_at(C, g.k, o, m);
+    const uint64_t cm = canon_m(mm, m);
+    place(C, g.k, o, mm != cm ? 1u : 0u, line_hash(cm, m), g.nBuckets, g.fpBits, bucket, slot);
 }
 
 } // namespace mz

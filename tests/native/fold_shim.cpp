@@ -63,7 +63,7 @@ static TableGeom mz_geom(uint32_t k, uint64_t nBuckets)
     g.bits = 2 * k;
     g.format = FMT_MZ8;
     g.nBuckets = nBuckets; // a multiple of the four sectors of a line
-    g.fpBits = 32 - (63 - __builtin_clzll(nBuckets / mz::kSectorsPerLine));
+    g.fpBits = 2 * mz::m_of(k) - (63 - __builtin_clzll(nBuckets / mz::kSectorsPerLine));
     return g;
 }
 
@@ -77,23 +77,31 @@ extern "C" void mz_locate(const uint64_t *codes, uint64_t n, uint32_t k, uint64_
 }
 
 // Query side as the scan kernel computes it: along the forward strand of
-// `bases` (values 0-3), 16-mer hashes per position, the window minimum over
-// the next w hashes with its leftmost/rightmost offsets, the strand of the
+// `bases` (values 0-3), m-mer rank keys per position, the window minimum over
+// the next w keys with its leftmost/rightmost offsets, the strand of the
 // canonical k-mer, then bucket and slot. Positions 0..n-k.
 extern "C" void mz_query(const uint8_t *bases, uint64_t n, uint32_t k, uint64_t nBuckets,
                          uint64_t *bucket, uint32_t *slot)
 {
     const TableGeom g = mz_geom(k, nBuckets);
-    const uint32_t w = mz::w_of(k);
+    const uint32_t w = mz::w_of(k), m = mz::m_of(k);
     if (n < k)
         return;
-    const uint64_t nm = n - mz::M + 1;
-    uint32_t *h = new uint32_t[nm];
+    const uint64_t nm = n - m + 1;
+    uint32_t *key = new uint32_t[nm];
+    uint64_t *lg = new uint64_t[nm];   // line hash of the canonical m-mer
+    uint8_t *fnc = new uint8_t[nm], *rnc = new uint8_t[nm]; // forward / its rc not canonical
     for (uint64_t q = 0; q < nm; ++q) {
-        uint32_t f = 0;
-        for (uint32_t t = 0; t < mz::M; ++t)
+        uint64_t f = 0, r = 0;
+        for (uint32_t t = 0; t < m; ++t) {
             f = (f << 2) | bases[q + t];
-        h[q] = mz::hash16(mz::canon16(f));
+            r |= (uint64_t)(3 - bases[q + t]) << (2 * t);
+        }
+        const uint64_t c = f < r ? f : r;
+        key[q] = mz::rank_key(c, m);
+        lg[q] = mz::line_hash(c, m);
+        fnc[q] = f > r;
+        rnc[q] = r > f;
     }
     const uint64_t kmask = key_mask(2 * k);
     for (uint64_t q = 0; q + k <= n; ++q) {
@@ -107,16 +115,19 @@ extern "C" void mz_query(const uint8_t *bases, uint64_t n, uint32_t k, uint64_t 
         const uint64_t C = isFwd ? fwd : rc;
         uint32_t mn = 0xffffffffu, jl = 0, jr = 0;
         for (uint32_t j = 0; j < w; ++j) {
-            const uint32_t v = h[q + j];
+            const uint32_t v = key[q + j];
             if (v < mn || j == 0) {
                 mn = v;
                 jl = jr = j;
             } else if (v == mn)
                 jr = j;
         }
+        const uint64_t src = q + (isFwd ? jl : jr);
         const uint32_t o = isFwd ? jl : (w - 1 - jr);
-        bucket[q] = mz::bucket_of_h(mn, C, g.nBuckets);
-        slot[q] = mz::slot_value(mz::slot_high(C, k, o), mn, g.fpBits);
+        mz::place(C, k, o, isFwd ? fnc[src] : rnc[src], lg[src], g.nBuckets, g.fpBits, bucket[q], slot[q]);
     }
-    delete[] h;
+    delete[] key;
+    delete[] lg;
+    delete[] fnc;
+    delete[] rnc;
 }

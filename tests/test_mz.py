@@ -38,7 +38,7 @@ def query(shim, bases, k, nb):
 @pytest.mark.parametrize("k", [16, 21, 25, 27])
 def test_query_side_equals_build_side(native_shim, k):
     rng = np.random.default_rng(k)
-    nb = 4 << max(2 * k - 26, 20)  # four sectors per line, nLines >= 2^(2k-26)
+    nb = 4 << max(2 * k - 27, 20)  # four sectors per line, nLines >= 2^(2k-27)
     # random sequence plus repeats that force minimizer ties
     seq = rng.integers(0, 4, 200_000).astype(np.uint8)
     unit = rng.integers(0, 4, 17).astype(np.uint8)
@@ -56,7 +56,7 @@ def test_query_side_equals_build_side(native_shim, k):
 @pytest.mark.parametrize("k", [20, 25, 27])
 def test_bucket_and_slot_identify_the_kmer(native_shim, k):
     rng = np.random.default_rng(100 + k)
-    nb = 4 << max(2 * k - 26, 18)
+    nb = 4 << max(2 * k - 27, 18)
     codes = np.unique(corpus.random_codes(rng, 400_000, k))
     b, s = locate(native_shim, codes, k, nb)
     assert (b < nb).all()
