@@ -154,9 +154,11 @@ def measured_peaks():
     return 6650.0, "of fallback"
 
 
-def profiled_traffic(workload: str):
-    """DRAM bytes per scan-kernel launch from the committed ncu summary, if any."""
-    p = REPO / "profiles" / f"scan_spans_{workload}.json"
+def profiled_traffic(workload: str, table_format: int):
+    """DRAM bytes per scan-kernel launch from the committed ncu summary of
+    the kernel this table format runs, if any."""
+    kernel = "scan_spans_mz" if table_format == 4 else "scan_spans"
+    p = REPO / "profiles" / f"{kernel}_{workload}.json"
     if p.exists():
         try:
             return json.loads(p.read_text()).get("dram_bytes_per_launch")
@@ -379,12 +381,15 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
                          f"{(sw + mw) * 8 / 1e9:.2f} GB packed reference"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": profiled_traffic(w.name),
+                     "traffic": profiled_traffic(w.name, int(info.format)),
                      "bytes_per_probe": BYTES_PER_PROBE,
                      "random_sector_peak": sector_rate * BYTES_PER_PROBE / 1e9,
                      "random_sector_frac": (probes_per_scan / (ms_step * 1e-3)) / sector_rate,
                      "note": "achieved = probes/s x (32 B bucket sector + 0.375 B streamed reference); "
-                             "random_sector_peak = live GUPS-style random 32 B reads x the same bytes"},
+                             "random_sector_peak = live GUPS-style random 32 B reads x the same bytes; "
+                             "with the minimizer table (format 4) consecutive probes share 128-byte "
+                             "lines, so traffic (DRAM bytes per launch, ncu) sits below the algorithmic "
+                             "bytes"},
         "e2e": {"value": total_probes / e2e_s, "unit": "probes/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3,
                 "call": "ibs_scan_packed (pinned host 2-bit reference -> host rows)"},
@@ -723,6 +728,154 @@ def served_arm(args, rank: int):
     return out
 
 
+def admitted_arm(args, rank: int):
+    """Memory-admitted serving beyond the device's share: 48 samples whose
+    tables total about 3x the server's byte budget, Zipf(1.1) popularity,
+    whole-genome (every contig) and regional requests. The batching server
+    against one request per launch, both evicting least-recently-used tables
+    and reloading them from pinned host images on a side stream. Every row
+    is checked against its sample's full-scan rows."""
+    import torch
+    import ibs_b200 as ib
+    from ibs_b200 import configs
+    w = configs.admitted_4gbp(n_samples=args.admit_samples, scale=args.admit_scale,
+                              sample_scale=args.admit_sample_scale)
+    k, W = w.k, w.window
+    lens = w.ref.lens
+    sw, mw = w.ref.packed_words()
+    dseq = torch.empty(sw, dtype=torch.int64, device="cuda")
+    dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
+    w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
+    ref = ib.Reference(dseq.data_ptr(), dmask.data_ptr(), lens, on_device=True)
+    n_samples = len(w.samples)
+    win_start = np.concatenate([[0], np.cumsum([ib.window_count(lens[c:c + 1], W, k) for c in range(len(lens))])])
+    n_win = int(win_start[-1])
+    t0 = time.time()
+
+    def codes(i):
+        sp = w.samples[i]
+        bound = sp.codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
+        buf = torch.empty(bound, dtype=torch.int64, device="cuda")
+        n = sp.codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), buf.data_ptr(), bound)
+        return buf, n
+
+    full, n_keys, table_bytes = [], [], []
+    rows_dev = torch.empty(n_win * 6, dtype=torch.int32, device="cuda")
+    for i in range(n_samples):
+        buf, n = codes(i)
+        n_keys.append(n)
+        t = ib.Table.from_codes(buf.data_ptr(), n, k, on_device=True, force_format=5)
+        table_bytes.append(int(t.info().device_bytes))
+        del buf
+        torch.cuda.empty_cache()
+        ib.scan_async(t, ref, W, rows_dev.data_ptr(), n_win, 0)
+        torch.cuda.synchronize()
+        full.append(rows_dev.cpu().numpy().view(ib.WINDOW_DTYPE).copy())
+        t.close()
+    del rows_dev
+    torch.cuda.empty_cache()
+    setup_s = time.time() - t0
+    budget = int(sum(table_bytes) / args.admit_overcommit)
+
+    # requests: Zipf(1.1) over the samples; whole-genome (one request per
+    # contig, timed as a group) or regional (log-uniform 1 Mbp .. a contig)
+    rng = np.random.default_rng(606)
+    pop = 1.0 / np.arange(1, n_samples + 1) ** 1.1
+    pop /= pop.sum()
+    order = rng.permutation(n_samples)
+    reqs, group = [], []
+    step = W - k
+    for g in range(args.admit_requests):
+        s_ = int(order[rng.choice(n_samples, p=pop)])
+        if rng.random() < args.admit_whole_frac:
+            for c in range(len(lens)):
+                reqs.append((s_, c, 0, 0))
+                group.append(g)
+        else:
+            c = int(rng.integers(0, len(lens)))
+            L = int(lens[c])
+            ln = int(np.exp(rng.uniform(np.log(1e6), np.log(max(L, 1e6 + 1)))))
+            nw_c = int(win_start[c + 1] - win_start[c])
+            first = min(int(rng.integers(0, max(1, (L - ln) // step + 1))), nw_c - 1)
+            reqs.append((s_, c, first, max(1, min(nw_c - first, ln // step))))
+            group.append(g)
+    group = np.array(group)
+    gaps = rng.exponential(1.0 / args.admit_rate, args.admit_requests)
+
+    def run(srv, paced: bool):
+        done = {}
+        stats0 = srv.stats()
+        t_start = srv.now()
+        submit_t = {}
+        i = 0
+        if paced:
+            t_next = time.perf_counter()
+            for g in range(args.admit_requests):
+                t_next += gaps[g]
+                while time.perf_counter() < t_next:
+                    for r in srv.poll(256, timeout_ms=0):
+                        done[r["request_id"]] = r
+                    time.sleep(0.0002)
+                while i < len(reqs) and group[i] == g:
+                    submit_t[srv.submit(*reqs[i])] = i
+                    i += 1
+        else:
+            for req in reqs:
+                submit_t[srv.submit(*req)] = len(submit_t)
+        deadline = time.time() + 3600
+        while len(done) < len(reqs) and time.time() < deadline:
+            for r in srv.poll(256, timeout_ms=1000):
+                done[r["request_id"]] = r
+        assert len(done) == len(reqs), f"admitted requests unfinished: {srv.stats()}"
+        makespan = srv.now() - t_start
+        st = srv.stats()
+        first_submit = np.full(args.admit_requests, np.inf)
+        last_done = np.zeros(args.admit_requests)
+        for rid, r in done.items():
+            assert r["status"] == 0, "an admitted request failed"
+            a = int(win_start[r["contig"]] + r["first_window"])
+            assert np.array_equal(r["rows"], full[r["sample"]][a:a + int(r["n_windows"])]), "admitted rows differ"
+            g = group[submit_t[rid]]
+            first_submit[g] = min(first_submit[g], r["submit_time"])
+            last_done[g] = max(last_done[g], r["done_time"])
+        lat = last_done - first_submit
+        probes = st["probes"] - stats0["probes"]
+        return {"requests": args.admit_requests, "server_requests": len(reqs), "probes": int(probes),
+                "scanned": int(st["scanned"] - stats0["scanned"]), "makespan_s": makespan,
+                "probes_per_s": probes / makespan,
+                "device_busy_s": st["busy_seconds"] - stats0["busy_seconds"],
+                "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                "latency_max_s": float(lat.max()), "launches": int(st["launches"] - stats0["launches"]),
+                "reloads": int(st["reloads"] - stats0["reloads"]),
+                "reload_bytes": int(st["reload_bytes"] - stats0["reload_bytes"]),
+                "evictions": int(st["evictions"] - stats0["evictions"])}
+
+    out = {"workload": f"{w.name} reference x {n_samples} samples, tables {sum(table_bytes) / 1e9:.1f} GB "
+                       f"against a {budget / 1e9:.1f} GB budget",
+           "k": k, "window": W, "reference_bp": int(sum(map(int, lens))), "sample_kmers": n_keys,
+           "table_gb_total": sum(table_bytes) / 1e9, "budget_gb": budget / 1e9,
+           "requests": args.admit_requests, "whole_genome_frac": args.admit_whole_frac,
+           "popularity": "Zipf(1.1)", "arrival_rate_per_s": args.admit_rate, "setup_s": setup_s}
+    for mode in ("plain", "batched"):
+        srv = ib.Server(ref, W, k, memory_budget=budget, one_request_per_launch=(mode == "plain"))
+        for i in range(n_samples):
+            buf, n = codes(i)
+            srv.add_codes(buf.data_ptr(), n, on_device=True)
+            del buf
+            torch.cuda.empty_cache()
+        out[f"{mode}_saturated"] = run(srv, False)
+        out[f"{mode}_poisson"] = run(srv, True)
+        srv.close()
+        torch.cuda.empty_cache()
+    out["saturated_speedup_vs_plain"] = (out["batched_saturated"]["probes_per_s"] /
+                                         out["plain_saturated"]["probes_per_s"])
+    out["rows_equal_full_scan"] = True
+    out["note"] = ("latency of a whole-genome request = its last contig's completion - its submission; "
+                   "both modes use per-sample tables under the same budget")
+    ref.free()
+    return out
+
+
 def reference_arm(args, w):
     """--impl reference: the reference's CPU-BATCHED scan on bounded slices."""
     import torch
@@ -821,6 +974,17 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=50.0)
     ap.add_argument("--serve-scale", type=float, default=1.0, help="reference length scale")
+    ap.add_argument("--admitted-only", action="store_true",
+                    help="memory-admitted serving: 48 samples, tables ~3x the server's budget")
+    ap.add_argument("--admit-samples", type=int, default=48)
+    ap.add_argument("--admit-scale", type=float, default=1.0, help="reference length scale")
+    ap.add_argument("--admit-sample-scale", type=float, default=0.2,
+                    help="sample size scale (keeps the pinned host images within host memory)")
+    ap.add_argument("--admit-overcommit", type=float, default=3.0,
+                    help="sum of the tables / the server's byte budget")
+    ap.add_argument("--admit-requests", type=int, default=5000)
+    ap.add_argument("--admit-whole-frac", type=float, default=0.1)
+    ap.add_argument("--admit-rate", type=float, default=100.0)
     ap.add_argument("--serve-workload", choices=["served_2gbp", "panel_4gbp"], default="served_2gbp",
                     help="the pool: the 2 Gbp reference with 16 samples, or the 4.2 Gbp panel's")
     ap.add_argument("--serve-sample-scale", type=float, default=0.5,
@@ -860,6 +1024,11 @@ def main():
         import torch
         torch.cuda.set_device(local)
         print(json.dumps({"panel": panel_arm(args, rank)}), flush=True)
+        return 0
+    if args.admitted_only:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"admitted": admitted_arm(args, rank)}), flush=True)
         return 0
     out = gpu_arm(args, w, rank, world, local)
     if args.panel and world == 1:

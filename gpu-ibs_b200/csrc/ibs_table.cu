@@ -56,7 +56,24 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
     TableGeom g{};
     g.k = k;
     g.bits = 2 * k;
-    const double lam = (o && o->keys_per_bucket > 0) ? o->keys_per_bucket : tuning().keys_per_bucket;
+    uint32_t fmt = o ? o->force_format : 0;
+    const bool tunedMz = tuning().table_format == FMT_MZ8;
+    if (fmt == 0 && tunedMz && k >= 16 && k <= 27) {
+        // the tuned default, where the minimizer layout applies and its
+        // minimum line count (2^(2k-27)) does not oversize the table
+        const double want = (double)nKeys / tuning().keys_per_bucket / mz::kSectorsPerLine;
+        if (2 * k <= 27 || want >= (double)(1ull << (2 * k - 27)))
+            fmt = FMT_MZ8;
+    }
+    if (fmt == FMT_AUTO_HASH)
+        fmt = 0;
+    // the tuned load belongs to the tuned layout; hash tables under a tuned
+    // minimizer default keep the hash layout's default of 4 keys per bucket
+    double lam = tuning().keys_per_bucket;
+    if (tunedMz && fmt != FMT_MZ8)
+        lam = 4.0;
+    if (o && o->keys_per_bucket > 0)
+        lam = o->keys_per_bucket;
     const uint64_t space = g.bits >= 64 ? ~0ull : (1ull << g.bits);
     auto clampN = [&](uint64_t n) {
         if (n < 1)
@@ -69,11 +86,6 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
     const uint64_t min8 = g.bits > 31 ? (1ull << (g.bits - 31)) : 1;
     const uint64_t n6 = clampN((uint64_t)((double)nKeys / (lam * 6.0 / 8.0)) + 1);
     const uint64_t min6 = g.bits > 40 ? (1ull << (g.bits - 40)) : 1;
-    uint32_t fmt = o ? o->force_format : 0;
-    if (fmt == 0 && tuning().table_format == FMT_MZ8 && k >= 16 && k <= 27)
-        fmt = FMT_MZ8; // the tuned default, where the minimizer layout applies
-    if (fmt == FMT_AUTO_HASH)
-        fmt = 0;
     if (fmt == FMT_MZ8) {
         // minimizer lines of four sectors: the slot value needs nLines >= 2^(2k-27)
         g.format = FMT_MZ8;

@@ -19,6 +19,9 @@ reference and sample is generated from a seed (see include/ibs_tools.h):
 * served_2gbp  -- the plain_2gbp reference and 16 samples of its block model
                   with their own seeds, log-uniform 0.15e9-1.0e9 k=25 k-mers:
                   the served stream's resident pool.
+* admitted_4gbp -- the panel_4gbp reference and 48 samples of 0.5e9-2.1e9
+                  k=31 k-mers (optionally scaled): the memory-admitted pool,
+                  several times the memory the server may use.
 """
 from __future__ import annotations
 
@@ -119,3 +122,23 @@ def served_2gbp(n_samples: int = 16, scale: float = 1.0) -> Workload:
     return Workload("served_2gbp" if scale == 1.0 else f"served_2gbp_x{scale:g}", base.ref, samples,
                     base.kmc, description=f"{sum(base.ref.lens) / 1e9:.3g} Gbp x {n_samples} samples of "
                                           f"0.15e9-1.0e9 k=25 k-mers, W=50 kbp")
+
+
+def admitted_4gbp(n_samples: int = 48, scale: float = 1.0, sample_scale: float = 1.0) -> Workload:
+    """Memory-admitted serving pool: the panel_4gbp reference and n samples of
+    0.5e9-2.1e9 k=31 k-mers (log-uniform, times sample_scale), made by the
+    block-divergence model with their own seeds; together several times the
+    device memory a server is given."""
+    base = panel_4gbp(n_samples=1, scale=scale)
+    rng = np.random.default_rng(505)
+    positions = sum(base.ref.lens)
+    samples = []
+    for s in range(n_samples):
+        target = math.exp(rng.uniform(math.log(0.5e9), math.log(2.1e9))) * scale * sample_scale
+        samples.append(SampleSpec(seed=5000 + s, k=31, class_rate=BLOCK_RATES, class_prob=BLOCK_PROBS,
+                                  block_len=1 * MB, present_frac=min(1.0, target / (positions * 1.10)),
+                                  random_frac=0.10))
+    name = "admitted_4gbp" + ("" if sample_scale == 1.0 else f"_samples_x{sample_scale:g}")
+    return Workload(name, base.ref, samples, base.kmc,
+                    description=f"4.2 Gbp x {n_samples} samples of {0.5 * sample_scale:g}e9-"
+                                f"{2.1 * sample_scale:g}e9 k=31 k-mers, W=50 kbp")

@@ -138,3 +138,14 @@ def test_sort_unique_host():
     rng = np.random.default_rng(1)
     x = rng.integers(0, 1000, 200_000).astype(np.uint64)
     assert np.array_equal(ib.sort_unique_host(x.copy(), threads=4), np.unique(x))
+
+
+def test_library_defaults_are_the_committed_tuning():
+    import json
+    import ibs_b200 as ib
+    best = json.loads((ib.PKG_DIR / "tuning" / "b200.json").read_text())["best"]
+    t = ib.get_tuning().as_dict()
+    for key in ("span_len", "blocks_in_flight", "block_threads", "ctas_per_sm", "keys_per_bucket",
+                "table_format"):
+        assert t[key] == best[key], key
+    assert best["rows_equal"]
