@@ -250,6 +250,22 @@ __global__ void k_probe(TableView t, const uint64_t *__restrict__ codes, uint64_
         hits[i] = table_lookup<FMT>(t, codes[i]) ? 1 : 0;
 }
 
+// Number of codes present in the table: each thread counts its share, each
+// warp adds its lanes' counts and one lane adds the warp's to the total.
+template <uint32_t FMT>
+__global__ void k_count_present(TableView t, const uint64_t *__restrict__ codes, uint64_t n,
+                                unsigned long long *__restrict__ count)
+{
+    unsigned long long local = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        local += table_lookup<FMT>(t, codes[i]) ? 1 : 0;
+    for (int o = 16; o; o >>= 1)
+        local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local)
+        atomicAdd(count, local);
+}
+
 static int grid_for(uint64_t n, int threads)
 {
     int dev = 0, sms = 148;
@@ -797,6 +813,70 @@ extern "C" ibs_status ibs_probe(ibs_table *t, const uint64_t *codes, uint64_t n,
     if (e != cudaSuccess)
         return cuda_fail(e, "probe");
     return IBS_OK;
+}
+
+// Codes on the device -> how many the table holds.
+static ibs_status count_present_device(ibs_table *t, const uint64_t *dCodes, uint64_t n, uint64_t *count)
+{
+    *count = 0;
+    if (!n)
+        return IBS_OK;
+    unsigned long long *dCount = nullptr;
+    IBS_CUDA(cudaMalloc(&dCount, sizeof *dCount), "count alloc");
+    std::unique_ptr<unsigned long long, cudaError_t (*)(void *)> guard(dCount, cudaFree);
+    IBS_CUDA(cudaMemset(dCount, 0, sizeof *dCount), "count init");
+    const int grid = grid_for(n, 256);
+    if (t->geom.format == FMT_B8X32)
+        k_count_present<FMT_B8X32><<<grid, 256>>>(t->view(), dCodes, n, dCount);
+    else if (t->geom.format == FMT_MZ8)
+        k_count_present<FMT_MZ8><<<grid, 256>>>(t->view(), dCodes, n, dCount);
+    else
+        k_count_present<FMT_B6X40><<<grid, 256>>>(t->view(), dCodes, n, dCount);
+    IBS_LAUNCHED();
+    IBS_CUDA(cudaGetLastError(), "count launch");
+    unsigned long long c = 0;
+    IBS_CUDA(cudaMemcpy(&c, dCount, sizeof c, cudaMemcpyDeviceToHost), "count read");
+    *count = c;
+    return IBS_OK;
+}
+
+extern "C" ibs_status ibs_count_present(ibs_table *t, const uint64_t *codes, uint64_t n, int codes_on_device,
+                                        uint64_t *count)
+{
+    clear_error();
+    if (!t || !count || (n && !codes)) {
+        set_error("ibs_count_present: bad argument");
+        return IBS_ERR_ARG;
+    }
+    DeviceGuard guard(t->device);
+    if (codes_on_device || !n)
+        return count_present_device(t, codes, n, count);
+    uint64_t *d = nullptr;
+    IBS_CUDA(cudaMalloc(&d, n * 8), "codes alloc");
+    std::unique_ptr<uint64_t, cudaError_t (*)(void *)> guard2(d, cudaFree);
+    IBS_CUDA(cudaMemcpy(d, codes, n * 8, cudaMemcpyHostToDevice), "codes upload");
+    return count_present_device(t, d, n, count);
+}
+
+extern "C" ibs_status ibs_count_present_kmc(ibs_table *t, const char *kmc_prefix, uint64_t *count)
+{
+    clear_error();
+    if (!t || !kmc_prefix || !count) {
+        set_error("ibs_count_present_kmc: bad argument");
+        return IBS_ERR_ARG;
+    }
+    DeviceGuard guard(t->device);
+    uint64_t *d = nullptr, n = 0;
+    uint32_t k = 0;
+    ibs_status s = decode_kmc(kmc_prefix, t->device, &d, &n, &k);
+    if (s != IBS_OK)
+        return s;
+    std::unique_ptr<uint64_t, cudaError_t (*)(void *)> guard2(d, cudaFree);
+    if (k != t->geom.k) {
+        set_error("K-mer lengths do not match");
+        return IBS_ERR_ARG;
+    }
+    return count_present_device(t, d, n, count);
 }
 
 extern "C" uint64_t ibs_table_bytes_for(uint64_t n_keys, uint32_t k, const ibs_table_opts *opts)

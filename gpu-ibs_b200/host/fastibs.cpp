@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "CliInput.hpp"
 #include "KmerDatabase.hpp"
 #include "KmerPanel.hpp"
 
@@ -36,6 +37,9 @@ using std::vector;
 #endif
 
 namespace {
+
+using ibs_cli::resolve_database;
+using ibs_cli::trim_slash;
 
 struct PanelOptions {
     vector<string> dbs;
@@ -61,12 +65,6 @@ string reference_name(const string &filename)
     return pos == string::npos ? filename : filename.substr(0, pos);
 }
 
-void trim_slash(string &p)
-{
-    if (!p.empty() && p.back() == '/')
-        p.pop_back();
-}
-
 void log_reference_error(const string &refName, const std::exception &e)
 {
     cerr << "Error processing reference " << refName << ": " << e.what() << " (also in log.txt)"
@@ -76,39 +74,6 @@ void log_reference_error(const string &refName, const std::exception &e)
         log << "Error processing reference: " << refName << endl << e.what() << endl;
     else
         cout << "Unable to open log file." << endl;
-}
-
-string find_prefix(const string &dir)
-{
-    std::error_code ec;
-    for (fs::directory_iterator it(dir, ec), end; !ec && it != end; it.increment(ec)) {
-        const string f = it->path().filename().string();
-        const size_t pos = f.find(".kmc_");
-        if (pos != string::npos)
-            return f.substr(0, pos);
-    }
-    return "";
-}
-
-bool resolve_database(const string &dir, string &prefixPath)
-{
-    std::error_code ec;
-    if (!fs::is_directory(dir, ec)) {
-        cerr << "Error: KMC database folder not found: " << dir;
-        if (fs::exists(dir + ".kmc_pre", ec))
-            cerr << " (this is a KMC prefix; pass the folder that holds "
-                 << fs::path(dir).filename().string() << ".kmc_pre / .kmc_suf)";
-        cerr << endl;
-        return false;
-    }
-    const string prefix = find_prefix(dir);
-    const string path = dir + "/" + prefix;
-    if (prefix.empty() || !fs::exists(path + ".kmc_pre", ec) || !fs::exists(path + ".kmc_suf", ec)) {
-        cerr << "Error: no KMC database (<prefix>.kmc_pre and <prefix>.kmc_suf) in " << dir << endl;
-        return false;
-    }
-    prefixPath = path;
-    return true;
 }
 
 string strip_gz(const string &f)

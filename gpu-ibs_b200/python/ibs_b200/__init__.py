@@ -124,6 +124,8 @@ _ibs_from_codes = _sig(_lib, "ibs_table_from_codes", C.c_int,
 _ibs_info = _sig(_lib, "ibs_table_info_get", C.c_int, [vp, C.POINTER(TableInfo)])
 _ibs_probe = _sig(_lib, "ibs_probe", C.c_int, [vp, vp, C.c_uint64, vp])
 _ibs_close = _sig(_lib, "ibs_close", None, [vp])
+_ibs_count_present = _sig(_lib, "ibs_count_present", C.c_int, [vp, vp, C.c_uint64, C.c_int, u64p])
+_ibs_count_present_kmc = _sig(_lib, "ibs_count_present_kmc", C.c_int, [vp, C.c_char_p, u64p])
 _ibs_packed_words = _sig(_lib, "ibs_packed_words", None, [vp, C.c_uint32, u64p, u64p])
 _ibs_pack_ascii = _sig(_lib, "ibs_pack_ascii", C.c_int,
                        [C.POINTER(C.c_char_p), vp, C.c_uint32, vp, vp, C.c_int])
@@ -265,6 +267,21 @@ class Table:
         i = TableInfo()
         _check(_ibs_info(self._h, C.byref(i)))
         return i
+
+    def count_present(self, codes, n: int | None = None, on_device: bool = False) -> int:
+        """How many of the codes the table holds (ibs_count_present)."""
+        if not on_device:
+            codes = np.ascontiguousarray(codes, dtype=np.uint64)
+            n = len(codes)
+        c = C.c_uint64()
+        _check(_ibs_count_present(self._h, _ptr(codes), n, int(on_device), C.byref(c)))
+        return c.value
+
+    def count_present_kmc(self, prefix: str) -> int:
+        """Size of the intersection with a KMC database's k-mers (ibs_count_present_kmc)."""
+        c = C.c_uint64()
+        _check(_ibs_count_present_kmc(self._h, str(prefix).encode(), C.byref(c)))
+        return c.value
 
     def probe(self, codes: np.ndarray) -> np.ndarray:
         codes = np.ascontiguousarray(codes, dtype=np.uint64)

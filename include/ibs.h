@@ -94,6 +94,18 @@ ibs_status ibs_table_info_get(const ibs_table *t, ibs_table_info *info);
  * The probe of KmcRaIndex::probe (src/gpu/KmcRaIndex.hpp:227-235). */
 ibs_status ibs_probe(ibs_table *t, const uint64_t *codes, uint64_t n, uint8_t *hits);
 
+/* How many of n canonical codes (host or device array) the table holds.
+ * With codes = one database's k-mers and t = another's table this is the
+ * intersection size KDBIntersect prints (src/KDBIntersect.cpp:134-233, the
+ * probe-and-count of DeviceKmerIndex::probeCountHost). */
+ibs_status ibs_count_present(ibs_table *t, const uint64_t *codes, uint64_t n, int codes_on_device,
+                             uint64_t *count);
+
+/* The same for every k-mer of a KMC 3 database, decoded on the device: the
+ * size of its intersection with the table's k-mer set. IBS_ERR_ARG ("K-mer
+ * lengths do not match") when the k differs. */
+ibs_status ibs_count_present_kmc(ibs_table *t, const char *kmc_prefix, uint64_t *count);
+
 void ibs_close(ibs_table *t);
 
 /* Device bytes a table of n_keys k-mers takes (its buckets; the stash of

@@ -230,3 +230,46 @@ def build_case(name: str, root: Path):
 
 
 GOLDEN_CASES = list(EDGE_CASES) + ["plain_1mbp"]
+
+
+# ---------------------------------------------------------------------------
+# intersection cases: two samples of one reference, in different KMC layouts
+# ---------------------------------------------------------------------------
+INTERSECT_CASES = {
+    # name: k, and the KMC layouts of sample A and sample B
+    "x_k25": dict(k=25, a=dict(p=5, version=0x200, counter_size=1), b=dict(p=9, version=0, counter_size=2)),
+    "x_k31": dict(k=31, a=dict(p=7, version=0x200, counter_size=1), b=dict(p=3, version=0x200, counter_size=0)),
+    "x_k15": dict(k=15, a=dict(p=7, version=0, counter_size=1), b=dict(p=3, version=0x200, counter_size=1)),
+    "x_k32": dict(k=32, a=dict(p=8, version=0x200, counter_size=1), b=dict(p=4, version=0x200, counter_size=1)),
+}
+
+
+def build_intersect_case(name: str, root: Path):
+    """Writes <root>/<name>/{a,b}/sample.kmc_*: two samples of one seeded
+    400 kbp reference (1% and 3% SNP copies, each with random extra k-mers,
+    B keeping 60% of its blocks); returns their folders and prefixes."""
+    spec = INTERSECT_CASES[name]
+    k = spec["k"]
+    seed = 900 + k
+    ref = ib.RefSpec(seed=seed, lens=[300_000, 100_000], n_frac=0.002, n_run=(1, 200))
+    seq, mask = ref.reference_host()
+    out = dict(k=k)
+    for side, rate, present, extra in (("a", 0.01, 1.0, 0.05), ("b", 0.03, 0.6, 0.10)):
+        smp = ib.SampleSpec(seed=seed * 10 + ord(side), k=k, class_rate=(rate,), class_prob=(1.0,),
+                            block_len=20_000, present_frac=present, random_frac=extra)
+        codes = smp.codes_host(ref, seq, mask)
+        lay = spec[side]
+        d = root / name / side
+        d.mkdir(parents=True, exist_ok=True)
+        ib.kmc_write(str(d / "sample"), codes, len(codes), k=k, p=lay["p"], sig_len=9, n_bins=64,
+                     counter_size=lay["counter_size"], version=lay["version"],
+                     min_count=2 if lay["counter_size"] else 0,
+                     max_count=255 if lay["counter_size"] == 1 else 65535)
+        out[side] = d
+        out["prefix_" + side] = d / "sample"
+    return out
+
+
+def intersect_hashes(case) -> dict:
+    return {s + ext: sha256_file(str(case["prefix_" + s]) + ext) for s in ("a", "b")
+            for ext in (".kmc_pre", ".kmc_suf")}
