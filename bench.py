@@ -776,6 +776,8 @@ def admitted_arm(args, rank: int):
     torch.cuda.empty_cache()
     setup_s = time.time() - t0
     budget = int(sum(table_bytes) / args.admit_overcommit)
+    log(f"[admitted] {n_samples} samples, {sum(n_keys) / 1e9:.2f}e9 k-mers, tables {sum(table_bytes) / 1e9:.1f} GB "
+        f"(pinned host images of that size per server), budget {budget / 1e9:.1f} GB, setup {setup_s:.0f} s")
 
     # requests: Zipf(1.1) over the samples; whole-genome (one request per
     # contig, timed as a group) or regional (log-uniform 1 Mbp .. a contig)
@@ -863,6 +865,7 @@ def admitted_arm(args, rank: int):
             srv.add_codes(buf.data_ptr(), n, on_device=True)
             del buf
             torch.cuda.empty_cache()
+        log(f"[admitted] {mode}: {n_samples} samples registered")
         out[f"{mode}_saturated"] = run(srv, False)
         out[f"{mode}_poisson"] = run(srv, True)
         srv.close()
@@ -978,7 +981,7 @@ def main():
                     help="memory-admitted serving: 48 samples, tables ~3x the server's budget")
     ap.add_argument("--admit-samples", type=int, default=48)
     ap.add_argument("--admit-scale", type=float, default=1.0, help="reference length scale")
-    ap.add_argument("--admit-sample-scale", type=float, default=0.12,
+    ap.add_argument("--admit-sample-scale", type=float, default=0.08,
                     help="sample size scale: the pinned host images of all 48 tables must fit the "
                          "host's memory (196 GB on the B200 boxes here)")
     ap.add_argument("--admit-overcommit", type=float, default=3.0,

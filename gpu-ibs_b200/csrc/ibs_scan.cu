@@ -171,31 +171,54 @@ __global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t 
     }
 }
 
-// The m-mer starting at packed base G: its rank key, and its line hash with
-// its orientation bits on top (bit 62: the forward m-mer is not canonical,
-// bit 63: its reverse complement is not; 2m <= 42 leaves them free).
-__device__ __forceinline__ uint32_t mmer_at_base(const uint64_t *__restrict__ seq, uint64_t G, uint32_t m,
-                                                 uint64_t &gs)
+// Everything the minimizer scan needs about reference position G, from one
+// read of its packed words: the canonical k-mer starting there (its code,
+// strand and whether its k bases are all ACGT) and the m-mer starting there
+// (its rank key, and its line hash with the orientation bits on top: bit 62
+// set when the forward m-mer is not canonical, bit 63 when its reverse
+// complement is not; 2m <= 42 leaves them free).
+struct MzPos {
+    uint64_t code, gs;
+    uint32_t key;
+    bool isFwd, acgt;
+};
+
+__device__ __forceinline__ MzPos mz_pos(const uint64_t *__restrict__ seq, const uint64_t *__restrict__ mask,
+                                        uint64_t G, uint32_t k, uint32_t m)
 {
+    MzPos r;
     const uint64_t wi = G >> 5;
     const uint32_t sh = (uint32_t)(G & 31) * 2;
     const uint64_t x = (__ldg(seq + wi) >> sh) | ((__ldg(seq + wi + 1) << (63 - sh)) << 1);
+    const uint64_t mi = G >> 6;
+    const uint32_t ms = (uint32_t)(G & 63);
+    const uint64_t mm = (__ldg(mask + mi) >> ms) | ((__ldg(mask + mi + 1) << (63 - ms)) << 1);
+    r.acgt = (mm & key_mask(k)) == 0;
     uint64_t y = __brevll(x);
-    y = ((y >> 1) & 0x5555555555555555ull) | ((y & 0x5555555555555555ull) << 1);
-    const uint64_t f = y >> (64 - 2 * m);     // first base high
-    const uint64_t r = ~x & key_mask(2 * m);  // its reverse complement
-    const uint64_t c = f < r ? f : r;
-    gs = mz::line_hash(c, m) | (f > r ? 1ull << 62 : 0ull) | (r > f ? 1ull << 63 : 0ull);
-    return mz::rank_key(c, m);
+    y = ((y >> 1) & 0x5555555555555555ull) | ((y & 0x5555555555555555ull) << 1); // first base high
+    const uint64_t fwd = y >> (64 - 2 * k);
+    const uint64_t rc = ~x & key_mask(2 * k);
+    r.isFwd = fwd <= rc;
+    r.code = r.isFwd ? fwd : rc;
+    const uint64_t f = y >> (64 - 2 * m);
+    const uint64_t mr = ~x & key_mask(2 * m);
+    const uint64_t c = f < mr ? f : mr;
+    r.gs = mz::line_hash(c, m) | (f > mr ? 1ull << 62 : 0ull) | (mr > f ? 1ull << 63 : 0ull);
+    r.key = mz::rank_key(c, m);
+    return r;
 }
 
-// The scan over a minimizer-bucketed table (format MZ8). Each lane keys the
-// m-mer starting at its position one block ahead; a k-mer's minimizer is
+// The scan over a minimizer-bucketed table (format MZ8). Each position's
+// words are read once, one block ahead: the m-mer keys of the next block are
+// needed by the current block's minimizer windows, and the same read gives
+// the k-mer that block probes when its turn comes. A k-mer's minimizer is
 // the minimum over the next w lanes' keys (shuffles across the block
 // boundary), tracked with its leftmost and rightmost offsets so the
-// leftmost-in-the-canonical-k-mer rule holds on either strand. Lanes whose
-// k-mers share a minimizer load sectors of one line.
-template <int NB>
+// leftmost-in-the-canonical-k-mer rule holds on either strand; its line hash
+// comes from the keying lane by shuffle. Lanes whose k-mers share a
+// minimizer load sectors of one line. K > 0 fixes k at compile time (the
+// shifts and masks fold); K = 0 reads it from the table.
+template <int NB, uint32_t K>
 __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64_t *__restrict__ seq,
                                                        const uint64_t *__restrict__ mask,
                                                        const WinDesc *__restrict__ win,
@@ -206,62 +229,44 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    const uint32_t k = t.g.k;
+    const uint32_t k = K ? K : t.g.k;
     const uint32_t w = mz::w_of(k);
     const uint32_t m = mz::m_of(k);
-    const uint64_t kmask = key_mask(2 * k);
-    const uint64_t kbits = (1ull << k) - 1;
     for (uint64_t s = s0 + warp; s < s1; s += nWarps) {
         const uint32_t wIdx = window_of_span(span0, nWin, s);
         const uint64_t base = win[wIdx].base;
         const uint32_t nPos = win[wIdx].nPos;
         const uint32_t p0 = (uint32_t)(s - __ldg(span0 + wIdx)) * spanLen;
         const uint32_t p1 = min(p0 + spanLen, nPos);
-        const uint32_t lastM = nPos - 1 + (w - 1); // last m-mer start the window's k-mers use
+        // last position read: the last m-mer start the window's k-mers use.
+        // Lanes past the span read positions up to it (inside the window's
+        // bases) and are masked out.
+        const uint32_t lastM = nPos - 1 + (w - 1);
         SegStats acc = seg_empty();
-        uint64_t gNext;
-        uint32_t hNext = mmer_at_base(seq, base + min(p0 + lane, lastM), m, gNext);
+        MzPos next = mz_pos(seq, mask, base + min(p0 + lane, lastM), k, m);
         for (uint32_t p = p0; p < p1; p += 32 * NB) {
-            uint32_t hb[NB + 1];
-            uint64_t hg[NB + 1];
-            hb[0] = hNext;
-            hg[0] = gNext;
+            MzPos ps[NB + 1];
+            ps[0] = next;
 #pragma unroll
             for (int b = 1; b <= NB; ++b)
-                hb[b] = mmer_at_base(seq, base + min(p + 32 * b + lane, lastM), m, hg[b]);
-            hNext = hb[NB];
-            gNext = hg[NB];
+                ps[b] = mz_pos(seq, mask, base + min(p + 32 * b + lane, lastM), k, m);
+            next = ps[NB];
             uint4 v0[NB], v1[NB];
-            uint64_t code[NB];
             uint32_t slot[NB];
             bool valid[NB];
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
                 const uint32_t q = p + 32 * b + lane;
-                const bool inSpan = q < p1;
-                const uint64_t G = base + (inSpan ? q : p0);
-                // k-mer and strand
-                const uint64_t wi = G >> 5;
-                const uint32_t sh = (uint32_t)(G & 31) * 2;
-                const uint64_t x = (__ldg(seq + wi) >> sh) | ((__ldg(seq + wi + 1) << (63 - sh)) << 1);
-                const uint64_t mi = G >> 6;
-                const uint32_t ms = (uint32_t)(G & 63);
-                const uint64_t mm = (__ldg(mask + mi) >> ms) | ((__ldg(mask + mi + 1) << (63 - ms)) << 1);
-                uint64_t y = __brevll(x);
-                y = ((y >> 1) & 0x5555555555555555ull) | ((y & 0x5555555555555555ull) << 1);
-                const uint64_t fwd = y >> (64 - 2 * k);
-                const uint64_t rc = ~x & kmask;
-                const bool isFwd = fwd <= rc;
-                code[b] = isFwd ? fwd : rc;
-                valid[b] = inSpan && (mm & kbits) == 0;
+                valid[b] = q < p1 && ps[b].acgt;
+                const bool isFwd = ps[b].isFwd;
                 // minimizer over the w (<= 8) m-mers starting at q .. q+w-1
                 uint32_t mn = 0xffffffffu, jl = 0, jr = 0;
 #pragma unroll
                 for (uint32_t j = 0; j < 8; ++j) {
                     if (j < w) {
                         const uint32_t src = lane + j;
-                        const uint32_t a = __shfl_sync(FULL, hb[b], src & 31);
-                        const uint32_t c = __shfl_sync(FULL, hb[b + 1], src & 31);
+                        const uint32_t a = __shfl_sync(FULL, ps[b].key, src & 31);
+                        const uint32_t c = __shfl_sync(FULL, ps[b + 1].key, src & 31);
                         const uint32_t v = src < 32 ? a : c;
                         if (v < mn || j == 0) {
                             mn = v;
@@ -273,13 +278,13 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                 // the minimizer's line hash and orientation from the lane that
                 // keyed it: position q + jl (forward k-mer) or q + jr (reverse)
                 const uint32_t src = lane + (isFwd ? jl : jr);
-                const uint64_t ga = __shfl_sync(FULL, hg[b], src & 31);
-                const uint64_t gc = __shfl_sync(FULL, hg[b + 1], src & 31);
+                const uint64_t ga = __shfl_sync(FULL, ps[b].gs, src & 31);
+                const uint64_t gc = __shfl_sync(FULL, ps[b + 1].gs, src & 31);
                 const uint64_t gs = src < 32 ? ga : gc;
                 const uint32_t sm = isFwd ? (uint32_t)(gs >> 62) & 1u : (uint32_t)(gs >> 63);
                 const uint32_t o = isFwd ? jl : (w - 1 - jr);
                 uint64_t r;
-                mz::place(code[b], k, o, sm, gs & ((1ull << 62) - 1), t.g.nBuckets, t.g.fpBits, r, slot[b]);
+                mz::place(ps[b].code, k, o, sm, gs & ((1ull << 62) - 1), t.g.nBuckets, t.g.fpBits, r, slot[b]);
                 if (valid[b]) {
                     v0[b] = __ldg(t.buckets + 2 * r);
                     v1[b] = __ldg(t.buckets + 2 * r + 1);
@@ -292,8 +297,8 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
             for (int b = 0; b < NB; ++b) {
                 bool hit = false;
                 if (valid[b]) {
-                    const uint32_t m = bucket_match<FMT_B8X32>(v0[b], v1[b], slot[b]);
-                    hit = m == 1u || (m == 2u && stash_lookup(t, code[b]));
+                    const uint32_t mt = bucket_match<FMT_B8X32>(v0[b], v1[b], slot[b]);
+                    hit = mt == 1u || (mt == 2u && stash_lookup(t, ps[b].code));
                 }
                 const uint32_t V = __ballot_sync(FULL, valid[b]);
                 const uint32_t H = __ballot_sync(FULL, hit);
@@ -386,9 +391,12 @@ template <uint32_t FMT, int NB>
 static void launch_nb(const ibs_table *t, const uint64_t *dSeq, const uint64_t *dMask, const ScanPlan &p,
                       uint64_t s0, uint64_t s1, SegStats *dSpans, cudaStream_t st, int grid, int threads)
 {
-    if (FMT == FMT_MZ8)
-        k_scan_spans_mz<NB><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
-                                                      (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
+    if (FMT == FMT_MZ8 && t->geom.k == 25)
+        k_scan_spans_mz<NB, 25><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
+                                                          (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
+    else if (FMT == FMT_MZ8)
+        k_scan_spans_mz<NB, 0><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
+                                                         (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
     else
         k_scan_spans<FMT, NB><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
                                                         (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);

@@ -202,3 +202,26 @@ def test_minimizer_format_rejects_unsupported_k(build_case):
     with pytest.raises(ib.IbsError) as e:
         ib.Table.open(str(case["prefix"]), force_format=4)
     assert e.value.status == 6
+
+
+@pytest.mark.parametrize("k", [16, 21, 22, 24])
+def test_minimizer_table_at_other_k_equals_hash_table(k):
+    # the minimizer kernel's generic-k instance (k = 25 has its own), with
+    # minimizer lengths 16 (k <= 22) and k - 6; rows equal the hash table's,
+    # which the goldens pin to the reference
+    spec = ib.RefSpec(seed=40 + k, lens=[250_000, 70_000, 23, 5_000], n_frac=0.003, n_run=(1, 150))
+    seq, mask = spec.reference_host()
+    smp = ib.SampleSpec(seed=400 + k, k=k, class_rate=(0.0001, 0.01, 0.03), class_prob=(0.3, 0.5, 0.2),
+                        block_len=10_000, present_frac=0.8, random_frac=0.05)
+    codes = smp.codes_host(spec, seq, mask)
+    ref = ib.Reference(seq, mask, spec.lens)
+    th = ib.Table.from_codes(codes, len(codes), k, on_device=False, force_format=5)
+    tm = ib.Table.from_codes(codes, len(codes), k, on_device=False, force_format=4)
+    assert tm.info().format == 4
+    for W in (1000, 5000):
+        assert np.array_equal(ib.scan(tm, ref, W), ib.scan(th, ref, W)), (k, W)
+    q = np.concatenate([codes[:20_000], corpus.random_codes(np.random.default_rng(k), 20_000, k)])
+    assert np.array_equal(tm.probe(q), th.probe(q))
+    th.close()
+    tm.close()
+    ref.free()
