@@ -366,6 +366,31 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
     h2d = (sw + mw) * 8 + n_win * 32 + (n_win + 1) * 4
     d2h = n_win * 24
 
+    # from FASTA text in host memory: parse + pack on the device, scan, rows
+    # back (the fastibs CLI's path for a plain .fasta reference)
+    fasta = None
+    if world == 1 and not args.no_fasta_e2e:
+        fpath = cache_dir(w) / "reference.fasta"
+        fpath.parent.mkdir(parents=True, exist_ok=True)
+        if not fpath.exists():
+            w.ref.write_fasta(str(fpath) + ".partial")
+            os.replace(str(fpath) + ".partial", fpath)
+        text = fpath.read_bytes()
+        secs = []
+        for it in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fref = ib.Reference.from_fasta(text, device=dev)
+            frows = ib.scan(table, fref, W)
+            secs.append(time.perf_counter() - t0)
+            fref.free()
+            assert np.array_equal(frows, rows), "rows from the device-parsed FASTA differ"
+        best = min(secs[1:])
+        fasta = {"value": total_probes / best, "unit": "probes/s", "seconds": best,
+                 "fasta_bytes": len(text), "h2d_bytes_per_step": len(text), "d2h_bytes_per_step": int(d2h),
+                 "call": "ibs_reference_from_fasta (FASTA bytes in host memory) + ibs_scan (rows to host)"}
+        del text
+
     peak, peak_kind = measured_peaks()
     achieved = probes_per_scan / (ms_step * 1e-3) * BYTES_PER_PROBE / 1e9
     checksum = int(rows["observed_kmers"].astype(np.int64).sum())
@@ -393,6 +418,7 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
         "e2e": {"value": total_probes / e2e_s, "unit": "probes/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3,
                 "call": "ibs_scan_packed (pinned host 2-bit reference -> host rows)"},
+        "e2e_from_fasta": fasta,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "extra": {"gbp_x_samples_per_s": sum(map(int, lens)) * world / (ms_step * 1e-3) / 1e9,
@@ -954,6 +980,7 @@ def main():
     ap.add_argument("--cpu-slice", type=int, default=50_000_000, help="bases per CPU-baseline slice")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fasta-e2e", action="store_true", help="skip the from-FASTA end-to-end measurement")
     ap.add_argument("--table-format", type=int, default=0,
                     help="sample table layout: 0 library default, 1 B8x32, 2 B6x40, 4 minimizer-bucketed")
     ap.add_argument("--keys-per-bucket", type=float, default=0.0, help="table load (0: library default)")

@@ -35,6 +35,14 @@ ibs_status cuda_fail(cudaError_t e, const char *what);
 ibs_status check_device_ordinal(int dev);
 // Decodes a KMC 3 database into canonical codes in device memory (caller frees).
 ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodes, uint64_t *n, uint32_t *k);
+// Packed base offset of each contig (roundup64 of the lengths before it) and
+// the seq / mask word counts with their tail padding.
+void packed_offsets(const uint64_t *lens, uint32_t n, std::vector<uint64_t> &off, uint64_t &seqWords,
+                    uint64_t &maskWords);
+// A reference around device arrays already in the packed layout; it takes
+// ownership of dSeq / dMask (freed by ibs_reference_free, also on failure).
+ibs_status reference_adopt(const std::vector<uint64_t> &lens, int device, uint64_t *dSeq, uint64_t *dMask,
+                           ibs_reference **out);
 
 #define IBS_LAUNCHED() (::ibs::launch_counter().fetch_add(1, std::memory_order_relaxed))
 
@@ -179,6 +187,7 @@ ibs_status launch_panel(ibs_table *const *tables, uint32_t nTables, const uint64
 struct ibs_reference {
     int device = 0;
     std::vector<uint64_t> lens, baseOff;
+    std::vector<std::string> ids;       // contig ids when parsed from FASTA by the library
     uint64_t seqWords = 0, maskWords = 0;
     uint64_t *dSeq = nullptr, *dMask = nullptr;
     ibs::ScanPlan plan;                 // cached for the last (W, k)

@@ -498,8 +498,8 @@ static ibs_status upload_plan(ScanPlan &p, cudaStream_t st)
 // ---------------------------------------------------------------------------
 // host packing
 // ---------------------------------------------------------------------------
-static void packed_offsets(const uint64_t *lens, uint32_t n, std::vector<uint64_t> &off,
-                           uint64_t &seqWords, uint64_t &maskWords)
+void packed_offsets(const uint64_t *lens, uint32_t n, std::vector<uint64_t> &off, uint64_t &seqWords,
+                    uint64_t &maskWords)
 {
     off.resize(n);
     uint64_t b = 0;
@@ -695,6 +695,25 @@ extern "C" ibs_status ibs_reference_create(const uint64_t *seq2bit, const uint64
     if (s != IBS_OK) {
         ibs_reference_free(r.release());
         return s;
+    }
+    *out = r.release();
+    return IBS_OK;
+}
+
+ibs_status ibs::reference_adopt(const std::vector<uint64_t> &lens, int device, uint64_t *dSeq, uint64_t *dMask,
+                                ibs_reference **out)
+{
+    std::unique_ptr<ibs_reference> r(new ibs_reference);
+    r->device = device;
+    r->lens = lens;
+    packed_offsets(lens.data(), (uint32_t)lens.size(), r->baseOff, r->seqWords, r->maskWords);
+    r->dSeq = dSeq;
+    r->dMask = dMask;
+    DeviceGuard guard(device);
+    const cudaError_t e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        ibs_reference_free(r.release());
+        return cuda_fail(e, "stream create");
     }
     *out = r.release();
     return IBS_OK;

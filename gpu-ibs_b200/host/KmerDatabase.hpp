@@ -131,13 +131,55 @@ public:
 
     static PackedReference readReference(const std::string &refPath)
     {
-        PackedReference r;
         const auto t0 = std::chrono::steady_clock::now();
         std::cout << "Reading sequences" << std::endl;
         const bool compressed = refPath.find(".gz") != std::string::npos;
-        ibs_host::SequenceFile f = ibs_host::read_sequence_file(refPath, compressed);
+        PackedReference r = packText(ibs_host::read_file_text(refPath, compressed));
+        r.readSec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() - r.packSec;
+        return r;
+    }
+
+    // A reference on the device: FASTA text (plain or gunzipped) is parsed
+    // and packed there (ibs_reference_from_fasta); FASTQ is read and packed
+    // on the host and uploaded. meta gets the ids and lengths.
+    static ibs_reference *loadReference(const std::string &refPath, PackedReference &meta)
+    {
+        const auto t0 = std::chrono::steady_clock::now();
+        std::cout << "Reading sequences" << std::endl;
+        const bool compressed = refPath.find(".gz") != std::string::npos;
+        std::string text = ibs_host::read_file_text(refPath, compressed);
         const auto t1 = std::chrono::steady_clock::now();
-        r.readSec = std::chrono::duration<double>(t1 - t0).count();
+        ibs_reference *dref = nullptr;
+        if (!text.empty() && text[0] == '>') {
+            meta = PackedReference();
+            check(ibs_reference_from_fasta(text.data(), text.size(), gpuOptions().device, &dref),
+                  "ibs_reference_from_fasta");
+            const uint32_t n = ibs_reference_contig_count(dref);
+            for (uint32_t c = 0; c < n; ++c) {
+                uint64_t len = 0;
+                const char *id = nullptr;
+                ibs_reference_contig(dref, c, &len, &id);
+                meta.lens.push_back(len);
+                meta.ids.emplace_back(id);
+            }
+            meta.readSec = std::chrono::duration<double>(t1 - t0).count();
+            meta.packSec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+            return dref;
+        }
+        meta = packText(text);
+        meta.readSec = std::chrono::duration<double>(t1 - t0).count();
+        check(ibs_reference_create(meta.seq.data(), meta.mask.data(), meta.lens.data(),
+                                   (uint32_t)meta.lens.size(), gpuOptions().device, &dref),
+              "ibs_reference_create");
+        return dref;
+    }
+
+    // Host reader and packer (FASTQ, and the arrays when a caller wants them).
+    static PackedReference packText(const std::string &text)
+    {
+        PackedReference r;
+        const auto t1 = std::chrono::steady_clock::now();
+        ibs_host::SequenceFile f = ibs_host::parse_sequence_text(text);
         r.ids = std::move(f.ids);
         std::vector<const char *> ptrs;
         for (const auto &s : f.sequences) {
@@ -202,16 +244,16 @@ public:
         std::cout << "K-mer path: fused GPU encode+probe, sector-bucket table (sm_100a)" << std::endl;
         checkWindow(windowSize, kmerSize);
         const double setupSec = lap();
-        PackedReference ref = readReference(refPath);
+        PackedReference ref;
+        std::unique_ptr<ibs_reference, void (*)(ibs_reference *)> dref(loadReference(refPath, ref),
+                                                                        ibs_reference_free);
         lap();
         const uint64_t n = ibs_window_count(ref.lens.data(), (uint32_t)ref.lens.size(),
                                             (uint32_t)windowSize, kmerSize);
         std::cout << "Number of chunks: " << n << std::endl;
         std::cout << "Calculating stats" << std::endl;
         std::vector<ibs_window> rows(n ? n : 1);
-        check(ibs_scan_packed(table, ref.seq.data(), ref.mask.data(), ref.lens.data(),
-                              (uint32_t)ref.lens.size(), (uint32_t)windowSize, rows.data(), n),
-              "ibs_scan_packed");
+        check(ibs_scan(table, dref.get(), (uint32_t)windowSize, rows.data(), n), "ibs_scan");
         const std::vector<Window> stats = toWindows(ref, rows.data(), windowSize, kmerSize);
         const double statsSec = lap();
         std::cout << "Writing stats to file" << std::endl;

@@ -75,16 +75,12 @@ public:
                   << " databases per reference pass" << std::endl;
         KmerDatabase::checkWindow(windowSize, k);
 
-        KmerDatabase::PackedReference ref = KmerDatabase::readReference(refPath);
+        KmerDatabase::PackedReference ref;
+        ibs_reference *dref = KmerDatabase::loadReference(refPath, ref);
+        std::unique_ptr<ibs_reference, void (*)(ibs_reference *)> refGuard(dref, ibs_reference_free);
         const uint64_t nWin = ibs_window_count(ref.lens.data(), (uint32_t)ref.lens.size(),
                                                (uint32_t)windowSize, k);
         std::cout << "Number of chunks: " << nWin << std::endl;
-        ibs_reference *dref = nullptr;
-        KmerDatabase::check(ibs_reference_create(ref.seq.data(), ref.mask.data(), ref.lens.data(),
-                                                 (uint32_t)ref.lens.size(),
-                                                 KmerDatabase::gpuOptions().device, &dref),
-                            "ibs_reference_create");
-        std::unique_ptr<ibs_reference, void (*)(ibs_reference *)> refGuard(dref, ibs_reference_free);
 
         std::vector<std::vector<size_t>> rounds;
         if (!keptResident.empty() && keptResident == active)

@@ -65,9 +65,13 @@ inline std::string read_plain(const std::string &path)
     return data;
 }
 
-inline SequenceFile read_sequence_file(const std::string &path, bool compressed)
+inline std::string read_file_text(const std::string &path, bool compressed)
 {
-    const std::string data = compressed ? read_gzip(path) : read_plain(path);
+    return compressed ? read_gzip(path) : read_plain(path);
+}
+
+inline SequenceFile parse_sequence_text(const std::string &data)
+{
     if (data.empty())
         throw std::runtime_error("Empty file");
     bool fastq;
@@ -114,6 +118,11 @@ inline SequenceFile read_sequence_file(const std::string &path, bool compressed)
         out.sequences.push_back(std::move(seq));
     }
     return out;
+}
+
+inline SequenceFile read_sequence_file(const std::string &path, bool compressed)
+{
+    return parse_sequence_text(read_file_text(path, compressed));
 }
 
 } // namespace ibs_host

@@ -134,6 +134,10 @@ _ibs_ref_create = _sig(_lib, "ibs_reference_create", C.c_int,
 _ibs_ref_create_dev = _sig(_lib, "ibs_reference_create_device", C.c_int,
                            [vp, vp, vp, C.c_uint32, C.c_int, C.POINTER(vp)])
 _ibs_ref_free = _sig(_lib, "ibs_reference_free", None, [vp])
+_ibs_ref_from_fasta = _sig(_lib, "ibs_reference_from_fasta", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.POINTER(vp)])
+_ibs_ref_ncontigs = _sig(_lib, "ibs_reference_contig_count", C.c_uint32, [vp])
+_ibs_ref_contig = _sig(_lib, "ibs_reference_contig", C.c_int, [vp, C.c_uint32, u64p, C.POINTER(C.c_char_p)])
+_ibs_ref_copy = _sig(_lib, "ibs_reference_copy_packed", C.c_int, [vp, vp, vp])
 _ibs_window_count = _sig(_lib, "ibs_window_count", C.c_uint64, [vp, C.c_uint32, C.c_uint32, C.c_uint32])
 _ibs_window_bounds = _sig(_lib, "ibs_window_bounds", C.c_int,
                           [vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint64])
@@ -396,6 +400,31 @@ class Reference:
         fn = _ibs_ref_create_dev if on_device else _ibs_ref_create
         _check(fn(_ptr(seq2bit), _ptr(nmask), _ptr(self.lens), len(self.lens), device, C.byref(h)))
         self._h = h.value
+
+    @classmethod
+    def from_fasta(cls, text: bytes, device: int = 0) -> "Reference":
+        """Parses and packs FASTA text on the device (ibs_reference_from_fasta);
+        `ids` and `lens` are its contigs."""
+        h = vp()
+        _check(_ibs_ref_from_fasta(text, len(text), device, C.byref(h)))
+        r = cls.__new__(cls)
+        r._h = h.value
+        n = _ibs_ref_ncontigs(r._h)
+        lens, ids = np.zeros(n, dtype=np.uint64), []
+        for i in range(n):
+            ln, idp = C.c_uint64(), C.c_char_p()
+            _check(_ibs_ref_contig(r._h, i, C.byref(ln), C.byref(idp)))
+            lens[i] = ln.value
+            ids.append(idp.value)
+        r.lens, r.ids = lens, ids
+        return r
+
+    def copy_packed(self):
+        """The packed (seq2bit, nmask) arrays back on the host."""
+        sw, mw = packed_words(self.lens)
+        seq, mask = np.zeros(sw, np.uint64), np.zeros(mw, np.uint64)
+        _check(_ibs_ref_copy(self._h, _ptr(seq), _ptr(mask)))
+        return seq, mask
 
     @property
     def handle(self) -> int:

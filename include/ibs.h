@@ -143,6 +143,22 @@ ibs_status ibs_reference_create_device(const uint64_t *seq2bit_dev, const uint64
                                        ibs_reference **out);
 void ibs_reference_free(ibs_reference *r);
 
+/* A reference straight from FASTA text in host memory (a whole file's bytes;
+ * decompress .gz first): the reference's readSequenceFile for FASTA
+ * (src/Utils.hpp:170-255) -- lines split on '\n' only, so a '\r' stays
+ * and packs as a non-ACGT base; the id is the header line after '>'; a
+ * record without sequence is dropped -- with the line-break removal and
+ * the packing (packWindow, src/gpu/EncodeProbeCore.hpp:157-186) done on the
+ * device. FASTQ text returns IBS_ERR_UNSUPPORTED (pack it with
+ * ibs_pack_ascii); text not starting with '>' or '@' IBS_ERR_FORMAT. */
+ibs_status ibs_reference_from_fasta(const char *text, uint64_t n_bytes, int device, ibs_reference **out);
+/* Contigs of a reference: count, and each one's length and id (the id
+ * string lives as long as the reference; "" when it was built from arrays). */
+uint32_t ibs_reference_contig_count(const ibs_reference *r);
+ibs_status ibs_reference_contig(const ibs_reference *r, uint32_t i, uint64_t *len, const char **id);
+/* The packed arrays back on the host (ibs_packed_words gives the sizes). */
+ibs_status ibs_reference_copy_packed(const ibs_reference *r, uint64_t *seq2bit, uint64_t *nmask);
+
 /* Windows chunkSequences cuts (src/Utils.hpp:296-327): sum over contigs of
  * ceil(len / (W - k)). 0 when W <= k. */
 uint64_t ibs_window_count(const uint64_t *lens, uint32_t n_contigs, uint32_t W, uint32_t k);
