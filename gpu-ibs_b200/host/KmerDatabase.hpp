@@ -264,6 +264,42 @@ public:
                   << writeSec << " s" << std::endl;
     }
 
+    // fastibsmapper: the coverage track of every contig (per base, how many
+    // of the sample's k-mers cover it) written as "<id>\n<c0,c1,...>\n" per
+    // contig (KmerDatabase::produceMapping, src/KmerDatabase.hpp:1067-1204).
+    // Probing, the coverage counts and the text are all made on the device.
+    void produceMapping(const std::string &refPath, const std::string &outPath)
+    {
+        auto clock = std::chrono::steady_clock::now();
+        auto lap = [&clock]() {
+            const auto now = std::chrono::steady_clock::now();
+            const double s = std::chrono::duration<double>(now - clock).count();
+            clock = now;
+            return s;
+        };
+        initGpuIndex();
+        std::cout << "Kmer size: " << kmerSize << std::endl;
+        std::cout << "K-mer path: fused GPU encode+probe, coverage and text on the device (sm_100a)"
+                  << std::endl;
+        PackedReference ref;
+        std::unique_ptr<ibs_reference, void (*)(ibs_reference *)> dref(loadReference(refPath, ref),
+                                                                        ibs_reference_free);
+        lap();
+        std::cout << "Calculating mapping" << std::endl;
+        std::vector<const char *> ids;
+        for (const auto &id : ref.ids)
+            ids.push_back(id.c_str());
+        char *text = nullptr;
+        uint64_t n = 0;
+        check(ibs_map_text(table, dref.get(), ids.data(), &text, &n), "ibs_map_text");
+        std::unique_ptr<char, void (*)(char *)> textGuard(text, ibs_map_text_free);
+        const double probeSec = lap();
+        std::cout << "Writing mapping to file" << std::endl;
+        writeOutputFile(outPath, [&](std::ofstream &f) { f.write(text, (std::streamsize)n); });
+        std::cout << "Mapping phases: read " << ref.readSec << " s, pack " << ref.packSec << " s, probe+serialize "
+                  << probeSec << " s, write " << lap() << " s" << std::endl;
+    }
+
     // Output written as "<outPath>.partial" and renamed once complete; a
     // failed open, write or rename throws and leaves no file under the final
     // name (src/KmerDatabase.hpp:899-931).

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "CliInput.hpp"
+#include "GpuCli.hpp"
 #include "KmerDatabase.hpp"
 #include "KmerPanel.hpp"
 
@@ -38,7 +39,12 @@ using std::vector;
 
 namespace {
 
+using ibs_cli::list_references;
+using ibs_cli::parse_int;
+using ibs_cli::log_reference_error;
+using ibs_cli::prepare_results;
 using ibs_cli::resolve_database;
+using ibs_cli::strip_gz;
 using ibs_cli::trim_slash;
 
 struct PanelOptions {
@@ -47,17 +53,6 @@ struct PanelOptions {
     int resident = 0;
 };
 
-bool parse_int(const string &text, int lo, int &out)
-{
-    const char *s = text.c_str();
-    char *end = nullptr;
-    errno = 0;
-    const long long v = std::strtoll(s, &end, 10);
-    if (end == s || *end != '\0' || errno == ERANGE || v < lo || v > INT_MAX)
-        return false;
-    out = (int)v;
-    return true;
-}
 
 string reference_name(const string &filename)
 {
@@ -65,72 +60,6 @@ string reference_name(const string &filename)
     return pos == string::npos ? filename : filename.substr(0, pos);
 }
 
-void log_reference_error(const string &refName, const std::exception &e)
-{
-    cerr << "Error processing reference " << refName << ": " << e.what() << " (also in log.txt)"
-         << endl;
-    std::ofstream log("log.txt", std::ios::app);
-    if (log.is_open())
-        log << "Error processing reference: " << refName << endl << e.what() << endl;
-    else
-        cout << "Unable to open log file." << endl;
-}
-
-string strip_gz(const string &f)
-{
-    return f.size() > 3 && f.compare(f.size() - 3, 3, ".gz") == 0 ? f.substr(0, f.size() - 3) : f;
-}
-
-bool is_reference_file(const string &f)
-{
-    const string ext = fs::path(strip_gz(f)).extension().string();
-    return ext == ".fasta" || ext == ".fa" || ext == ".fna";
-}
-
-bool list_references(const string &dir, vector<fs::path> &out)
-{
-    std::error_code ec;
-    if (!fs::is_directory(dir, ec)) {
-        cerr << "Error: reference folder not found: " << dir << endl;
-        return false;
-    }
-    fs::directory_iterator it(dir, ec), end;
-    for (; !ec && it != end; it.increment(ec)) {
-        const string name = it->path().filename().string();
-        if (is_reference_file(name))
-            out.push_back(it->path());
-        else
-            cout << "Skipping " << name << " (not a reference file: .fasta, .fa or .fna, optionally .gz)"
-                 << endl;
-    }
-    if (ec) {
-        cerr << "Error: cannot list the reference folder " << dir << ": " << ec.message() << endl;
-        return false;
-    }
-    if (out.empty()) {
-        cerr << "Error: no reference files (.fasta, .fa or .fna, optionally .gz) in " << dir << endl;
-        return false;
-    }
-    return true;
-}
-
-bool prepare_results(const string &dir)
-{
-    std::error_code ec;
-    if (fs::is_directory(dir, ec))
-        return true;
-    if (fs::exists(dir, ec)) {
-        cerr << "Error: results path exists and is not a folder: " << dir << endl;
-        return false;
-    }
-    fs::create_directories(dir, ec);
-    if (ec || !fs::is_directory(dir)) {
-        cerr << "Error: cannot create the results folder " << dir << ": "
-             << (ec ? ec.message() : "not a folder") << endl;
-        return false;
-    }
-    return true;
-}
 
 void window_too_small(int W, unsigned k)
 {
@@ -172,71 +101,20 @@ void usage(const char *argv0)
 
 bool parse_options(int argc, char **argv, int first, PanelOptions &panel)
 {
-    auto &o = KmerDatabase::gpuOptions();
-    auto intOpt = [](const string &arg, size_t n, int &out, int lo = 1) {
-        if (parse_int(arg.substr(n), lo, out))
-            return true;
-        cerr << "Invalid value for option: " << arg << " (expected an integer >= " << lo << ")" << endl;
-        return false;
-    };
     for (int a = first; a < argc; a++) {
         const string arg = argv[a];
-        if (arg == "--gpu")
-            o.enable = 1;
-        else if (arg == "--cpu" || arg == "--probe=batched") {
-            o.enable = 0;
-            cerr << "Warning: " << arg << " selects the reference's CPU path, which this build does "
-                 << "not have; scanning on the GPU (identical rows)" << endl;
-        } else if (arg == "--sync")
-            o.sync = true;
-        else if (arg.rfind("--batch-mb=", 0) == 0) {
-            if (!intOpt(arg, 11, o.batchMB))
-                return false;
-        } else if (arg.rfind("--streams=", 0) == 0) {
-            if (!intOpt(arg, 10, o.streams))
-                return false;
-        } else if (arg == "--gpus=all")
-            o.gpus = 0;
-        else if (arg == "--gpus=0") {
-            cerr << "Invalid value for option: --gpus=0 (use --gpus=all for every device, --cpu for none)"
-                 << endl;
+        const int g = ibs_cli::parse_gpu_flag(arg);
+        if (g < 0)
             return false;
-        } else if (arg.rfind("--gpus=", 0) == 0) {
-            if (!intOpt(arg, 7, o.gpus))
-                return false;
-        } else if (arg.rfind("--device=", 0) == 0) {
-            if (!intOpt(arg, 9, o.device, 0))
-                return false;
-        } else if (arg == "--no-peer")
-            o.noPeer = true;
-        else if (arg.rfind("--db=", 0) == 0 && arg.size() > 5)
+        if (g > 0)
+            continue;
+        if (arg.rfind("--db=", 0) == 0 && arg.size() > 5)
             panel.dbs.push_back(arg.substr(5));
         else if (arg.rfind("--db-list=", 0) == 0 && arg.size() > 10)
             panel.listFile = arg.substr(10);
         else if (arg.rfind("--resident=", 0) == 0) {
-            if (!intOpt(arg, 11, panel.resident, 0))
+            if (!ibs_cli::int_option(arg, 11, panel.resident, 0))
                 return false;
-        } else if (arg == "--sort-queries")
-            o.sortQueries = true;
-        else if (arg == "--probe=bs" || arg == "--probe=hash")
-            o.probeHash = arg == "--probe=hash";
-        else if (arg == "--pin-lut")
-            o.pinLut = true;
-        else if (arg.rfind("--hash-lf=", 0) == 0) {
-            double v = 0;
-            try {
-                size_t used = 0;
-                v = std::stod(arg.substr(10), &used);
-                if (used != arg.size() - 10)
-                    v = 0;
-            } catch (const std::exception &) {
-                v = 0;
-            }
-            if (v < 0.1 || v > 0.95) {
-                cerr << "Invalid value for option: " << arg << " (expected 0.1 .. 0.95)" << endl;
-                return false;
-            }
-            o.hashLoadFactor = v;
         } else {
             cerr << "Unknown option: " << arg << endl;
             return false;

@@ -138,6 +138,9 @@ _ibs_ref_from_fasta = _sig(_lib, "ibs_reference_from_fasta", C.c_int, [C.c_char_
 _ibs_ref_ncontigs = _sig(_lib, "ibs_reference_contig_count", C.c_uint32, [vp])
 _ibs_ref_contig = _sig(_lib, "ibs_reference_contig", C.c_int, [vp, C.c_uint32, u64p, C.POINTER(C.c_char_p)])
 _ibs_ref_copy = _sig(_lib, "ibs_reference_copy_packed", C.c_int, [vp, vp, vp])
+_ibs_map_cov = _sig(_lib, "ibs_map_coverage", C.c_int, [vp, vp, vp, C.c_uint64])
+_ibs_map_text = _sig(_lib, "ibs_map_text", C.c_int, [vp, vp, vp, C.POINTER(C.c_void_p), u64p])
+_ibs_map_text_free = _sig(_lib, "ibs_map_text_free", None, [vp])
 _ibs_window_count = _sig(_lib, "ibs_window_count", C.c_uint64, [vp, C.c_uint32, C.c_uint32, C.c_uint32])
 _ibs_window_bounds = _sig(_lib, "ibs_window_bounds", C.c_int,
                           [vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint64])
@@ -440,6 +443,25 @@ class Reference:
             self.free()
         except Exception:
             pass
+
+
+def map_coverage(table: "Table", ref: Reference) -> np.ndarray:
+    """Per-base k-mer coverage of every contig, concatenated (ibs_map_coverage)."""
+    n = int(np.sum(ref.lens))
+    cov = np.zeros(max(n, 1), dtype=np.uint8)
+    _check(_ibs_map_cov(table.handle, ref.handle, _ptr(cov), n))
+    return cov[:n]
+
+
+def map_text(table: "Table", ref: Reference, ids: list[bytes] | None = None) -> bytes:
+    """The mapper's output text (ibs_map_text)."""
+    arr = (C.c_char_p * len(ids))(*ids) if ids is not None else None
+    p, n = C.c_void_p(), C.c_uint64()
+    _check(_ibs_map_text(table.handle, ref.handle, arr, C.byref(p), C.byref(n)))
+    try:
+        return C.string_at(p.value, n.value) if n.value else b""
+    finally:
+        _ibs_map_text_free(p.value)
 
 
 def window_count(lens, W: int, k: int) -> int:

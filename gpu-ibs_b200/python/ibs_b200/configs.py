@@ -97,7 +97,7 @@ def panel_4gbp(n_samples: int = 16, scale: float = 1.0, sample_scale: float = 1.
             st = int(rng.integers(0, max(1, lens[c] - ln)))
             intro.append((c, st, ln))
         samples.append(SampleSpec(seed=3000 + s, k=31, class_rate=BLOCK_RATES, class_prob=BLOCK_PROBS,
-                                  block_len=1 * MB, present_frac=present, random_frac=0.10,
+                                  block_len=1 * MB, present_frac=present, random_frac=0.10 * present,
                                   intro=intro, intro_rate=0.0001))
     name = "panel_4gbp" if sample_scale == 1.0 else f"panel_4gbp_samples_x{sample_scale:g}"
     return Workload(name, ref, samples, dict(k=31, p=7, sig_len=9, n_bins=512, counter_size=1),
@@ -118,7 +118,7 @@ def served_2gbp(n_samples: int = 16, scale: float = 1.0) -> Workload:
         target = math.exp(rng.uniform(math.log(0.15e9), math.log(1.0e9))) * scale
         samples.append(SampleSpec(seed=4000 + s, k=25, class_rate=BLOCK_RATES, class_prob=BLOCK_PROBS,
                                   block_len=1 * MB, present_frac=min(1.0, target / (positions * 1.10)),
-                                  random_frac=0.10))
+                                  random_frac=0.10 * min(1.0, target / (positions * 1.10))))
     return Workload("served_2gbp" if scale == 1.0 else f"served_2gbp_x{scale:g}", base.ref, samples,
                     base.kmc, description=f"{sum(base.ref.lens) / 1e9:.3g} Gbp x {n_samples} samples of "
                                           f"0.15e9-1.0e9 k=25 k-mers, W=50 kbp")
@@ -137,7 +137,7 @@ def admitted_4gbp(n_samples: int = 48, scale: float = 1.0, sample_scale: float =
         target = math.exp(rng.uniform(math.log(0.5e9), math.log(2.1e9))) * scale * sample_scale
         samples.append(SampleSpec(seed=5000 + s, k=31, class_rate=BLOCK_RATES, class_prob=BLOCK_PROBS,
                                   block_len=1 * MB, present_frac=min(1.0, target / (positions * 1.10)),
-                                  random_frac=0.10))
+                                  random_frac=0.10 * min(1.0, target / (positions * 1.10))))
     name = "admitted_4gbp" + ("" if sample_scale == 1.0 else f"_samples_x{sample_scale:g}")
     return Workload(name, base.ref, samples, base.kmc,
                     description=f"4.2 Gbp x {n_samples} samples of {0.5 * sample_scale:g}e9-"

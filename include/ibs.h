@@ -159,6 +159,22 @@ ibs_status ibs_reference_contig(const ibs_reference *r, uint32_t i, uint64_t *le
 /* The packed arrays back on the host (ibs_packed_words gives the sizes). */
 ibs_status ibs_reference_copy_packed(const ibs_reference *r, uint64_t *seq2bit, uint64_t *nmask);
 
+/* ---- mapper ----------------------------------------------------------------
+ * fastibsmapper's coverage track (KmerDatabase::produceMapping and
+ * getMappingFromSequence, src/KmerDatabase.hpp:774-801, :1067-1204): for
+ * each base of each contig, the number of k-mer starts s in [i-k+1, i]
+ * whose k bases are ACGT and whose canonical k-mer the table holds.
+ * ibs_map_coverage: one byte per base, contigs concatenated (capacity =
+ * the sum of the lengths). */
+ibs_status ibs_map_coverage(ibs_table *t, ibs_reference *ref, uint8_t *coverage, uint64_t cap);
+/* The mapper's output file as text, built on the device: per contig its id,
+ * a newline, the coverage values joined by commas, a newline. ids = NULL
+ * takes the reference's own ids (ibs_reference_from_fasta); otherwise one
+ * per contig. *text is pinned host memory: free it with ibs_map_text_free. */
+ibs_status ibs_map_text(ibs_table *t, ibs_reference *ref, const char *const *ids, char **text,
+                        uint64_t *n_bytes);
+void ibs_map_text_free(char *text);
+
 /* Windows chunkSequences cuts (src/Utils.hpp:296-327): sum over contigs of
  * ceil(len / (W - k)). 0 when W <= k. */
 uint64_t ibs_window_count(const uint64_t *lens, uint32_t n_contigs, uint32_t W, uint32_t k);

@@ -164,6 +164,54 @@ def tsv_text(ids: list[str], seqs_lens: list[int], rows: np.ndarray, W: int, k: 
     return "".join(out)
 
 
+def position_codes(seq: bytes, k: int):
+    """(canonical code, valid) of every k-mer start of seq, as the reference's
+    KmerCodec::encodePositions gives them (src/KmerCodec.hpp:38-61): a start
+    is valid when its k bases are ACGT/acgt."""
+    s = np.frombuffer(seq, dtype=np.uint8)
+    n = len(s) - k + 1
+    if n <= 0:
+        return np.zeros(0, np.uint64), np.zeros(0, bool)
+    lut = np.full(256, 4, dtype=np.uint8)
+    for i, c in enumerate(b"ACGT"):
+        lut[c] = lut[c + 32] = i
+    v = lut[s]
+    cb = np.concatenate([[0], np.cumsum(v > 3)])
+    valid = (cb[k:] - cb[:-k])[:n] == 0
+    v = np.where(v > 3, 0, v).astype(np.uint64)
+    fwd = np.zeros(n, np.uint64)
+    rc = np.zeros(n, np.uint64)
+    for t in range(k):
+        fwd = (fwd << np.uint64(2)) | v[t:t + n]
+        rc |= (np.uint64(3) - v[t:t + n]) << np.uint64(2 * t)
+    return np.minimum(fwd, rc), valid
+
+
+def coverage(index: Index, seq: bytes, k: int) -> np.ndarray:
+    """Per-base k-mer coverage of one contig: the reference's difference array
+    (+1 at a hit start, -1 k bases on) and its prefix sum
+    (KmerDatabase::getMappingFromSequence, src/KmerDatabase.hpp:774-801)."""
+    codes, valid = position_codes(seq, k)
+    diff = np.zeros(len(seq) + 1, np.int64)
+    if len(codes):
+        hit = valid & (index.probe(codes).astype(bool))
+        idx = np.nonzero(hit)[0]
+        np.add.at(diff, idx, 1)
+        np.add.at(diff, idx + k, -1)
+    return np.cumsum(diff)[: len(seq)]
+
+
+def mapping_text(index: Index, ids: list[str], seqs: list[bytes], k: int) -> bytes:
+    """The mapper's output file: per contig its id, then the coverage values
+    joined by commas (serializeCoverage, src/KmerDatabase.hpp:754-772;
+    the writer, :1195-1203)."""
+    out = []
+    for cid, s in zip(ids, seqs):
+        cov = coverage(index, s, k)
+        out.append(cid.encode(errors="surrogateescape") + b"\n" + ",".join(map(str, cov.tolist())).encode() + b"\n")
+    return b"".join(out)
+
+
 def reference_binary() -> Path | None:
     p = REF_DIR / "fastibs"
     return p if p.exists() else None
