@@ -69,6 +69,43 @@ __device__ __forceinline__ SegStats block_stats(uint32_t V, uint32_t H, uint32_t
     return b;
 }
 
+// The same for 64 positions (two blocks: bit i = position p+i): each lane
+// closes the gaps that end at its hits among positions lane and lane + 32.
+__device__ __forceinline__ SegStats block_stats64(uint64_t V, uint64_t H, uint32_t lane, int k)
+{
+    SegStats b;
+    b.pad = 0;
+    b.total = __popcll(V);
+    b.obs = __popcll(H);
+    if (H == 0) {
+        b.lead = b.trail = b.total;
+        b.gaps = 0;
+        b.dist = 0;
+        return b;
+    }
+    const uint32_t first = __ffsll(H) - 1;
+    const uint32_t last = 63 - __clzll(H);
+    b.lead = __popcll(V & ((1ull << first) - 1ull));
+    b.trail = last == 63 ? 0u : __popcll(V >> (last + 1));
+    uint32_t gc = 0, d = 0;
+#pragma unroll
+    for (uint32_t half = 0; half < 2; ++half) {
+        const uint32_t pos = lane + 32 * half;
+        if (((H >> pos) & 1ull) && pos != first) {
+            const uint64_t below = (1ull << pos) - 1ull;
+            const uint32_t prev = 63 - __clzll(H & below); // a hit before pos: prev <= 62
+            const uint32_t g = __popcll(V & below & ~((2ull << prev) - 1ull));
+            if (g) {
+                gc += 1;
+                d += (uint32_t)gap_distance(g, k);
+            }
+        }
+    }
+    b.gaps = __reduce_add_sync(FULL, gc);
+    b.dist = __reduce_add_sync(FULL, d);
+    return b;
+}
+
 // Canonical code of the k-mer whose first base is packed base G, and whether
 // its k bases are all ACGT.
 __device__ __forceinline__ uint64_t canonical_at(const uint64_t *__restrict__ seq,
@@ -264,10 +301,12 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
 #pragma unroll
                 for (uint32_t j = 0; j < 8; ++j) {
                     if (j < w) {
-                        const uint32_t src = lane + j;
-                        const uint32_t a = __shfl_sync(FULL, ps[b].key, src & 31);
-                        const uint32_t c = __shfl_sync(FULL, ps[b + 1].key, src & 31);
-                        const uint32_t v = src < 32 ? a : c;
+                        // key of position q + j: lanes below 32 - j read lane + j of
+                        // this block, the others lane + j - 32 (< j) of the next, so
+                        // a source lane offers its next-block key exactly when it is
+                        // below j -- one shuffle per offset
+                        const uint32_t offer = lane < j ? ps[b + 1].key : ps[b].key;
+                        const uint32_t v = __shfl_sync(FULL, offer, (lane + j) & 31);
                         if (v < mn || j == 0) {
                             mn = v;
                             jl = jr = j;
@@ -293,6 +332,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                     v1[b] = make_uint4(0, 0, 0, 0);
                 }
             }
+            uint32_t V[NB], H[NB];
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
                 bool hit = false;
@@ -300,9 +340,21 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                     const uint32_t mt = bucket_match<FMT_B8X32>(v0[b], v1[b], slot[b]);
                     hit = mt == 1u || (mt == 2u && stash_lookup(t, ps[b].code));
                 }
-                const uint32_t V = __ballot_sync(FULL, valid[b]);
-                const uint32_t H = __ballot_sync(FULL, hit);
-                acc = seg_combine(acc, block_stats(V, H, lane, (int)k), (int)k);
+                V[b] = __ballot_sync(FULL, valid[b]);
+                H[b] = __ballot_sync(FULL, hit);
+            }
+            if constexpr (NB % 2 == 0) {
+                // two blocks per fold step: one 64-position summary
+#pragma unroll
+                for (int b = 0; b < NB; b += 2)
+                    acc = seg_combine(acc,
+                                      block_stats64((uint64_t)V[b + 1] << 32 | V[b], (uint64_t)H[b + 1] << 32 | H[b],
+                                                    lane, (int)k),
+                                      (int)k);
+            } else {
+#pragma unroll
+                for (int b = 0; b < NB; ++b)
+                    acc = seg_combine(acc, block_stats(V[b], H[b], lane, (int)k), (int)k);
             }
         }
         if (lane == 0)

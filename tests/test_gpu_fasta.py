@@ -49,7 +49,7 @@ def test_device_parse_edge_layouts(tmp_path):
     recs = []
     for i in range(40):
         n = int(rng.integers(0, 30_000)) if i % 7 else 0  # some records without sequence
-        body = bytes(rng.choice(alphabet[:12], n, p=[.22] * 4 + [.02] * 4 + [.02] * 4))
+        body = bytes(rng.choice(alphabet[:12], n, p=[.21] * 4 + [.02] * 8))
         if i % 5 == 1:
             body = body.replace(b"N", b">", 3)  # '>' inside a sequence line is a base
         recs.append((f"contig_{i} desc {i}".encode() + (b"\r" if i % 3 == 0 else b""), body))
