@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(256) k_na_spans(TableView t, const uint64_t *_
                 const uint64_t h = perm_hash(code[b], t.g.bits);
                 const uint64_t r = bucket_of(h, t.g);
                 fp[b] = fp_of(h, t.g);
-                if (valid[b]) {
+                if (valid[b] && FMT != FMT_MZ8) {
                     v0[b] = __ldg(t.buckets + 2 * r);
                     v1[b] = __ldg(t.buckets + 2 * r + 1);
                 } else {
@@ -191,8 +191,13 @@ __global__ void __launch_bounds__(256) k_na_spans(TableView t, const uint64_t *_
             for (int b = 0; b < NB; ++b) {
                 bool hit = false;
                 if (valid[b]) {
-                    const uint32_t m = bucket_match<FMT>(v0[b], v1[b], fp[b]);
-                    hit = m == 1u || (m == 2u && stash_lookup(t, code[b]));
+                    if constexpr (FMT == FMT_MZ8) {
+                        // minimizer table: each lane finds its k-mer's minimizer on its own
+                        hit = table_lookup<FMT_MZ8>(t, code[b]);
+                    } else {
+                        const uint32_t m = bucket_match<FMT>(v0[b], v1[b], fp[b]);
+                        hit = m == 1u || (m == 2u && stash_lookup(t, code[b]));
+                    }
                 }
                 const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
                 const uint32_t H = __ballot_sync(dev::FULL_MASK, hit);
@@ -280,9 +285,8 @@ extern "C" ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev
         set_error("ibs_scan_noalloc: bad argument");
         return IBS_ERR_ARG;
     }
-    if (t->geom.format != FMT_B8X32 && t->geom.format != FMT_B6X40) {
-        set_error("ibs_scan_noalloc: scans tables of the hash-bucket formats (1, 2); build the table "
-                  "with force_format 1, 2 or 5");
+    if (t->geom.format != FMT_B8X32 && t->geom.format != FMT_B6X40 && t->geom.format != FMT_MZ8) {
+        set_error("ibs_scan_noalloc: unknown table format");
         return IBS_ERR_UNSUPPORTED;
     }
     const uint32_t k = t->geom.k;
@@ -340,6 +344,9 @@ extern "C" ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev
         if (t->geom.format == FMT_B8X32)
             k_na_spans<FMT_B8X32, kNB><<<grid, 256, 0, st>>>(t->view(), seq2bit_dev, nmask_dev, dDesc,
                                                              n_contigs, W, nSpans, dSpans);
+        else if (t->geom.format == FMT_MZ8)
+            k_na_spans<FMT_MZ8, kNB><<<grid, 256, 0, st>>>(t->view(), seq2bit_dev, nmask_dev, dDesc,
+                                                           n_contigs, W, nSpans, dSpans);
         else
             k_na_spans<FMT_B6X40, kNB><<<grid, 256, 0, st>>>(t->view(), seq2bit_dev, nmask_dev, dDesc,
                                                              n_contigs, W, nSpans, dSpans);
