@@ -387,7 +387,23 @@ bool table_ready(Group &g)
     return true;
 }
 
-ibs_status make_resident(ibs_server *s, Group &g)
+// Pending work of the groups in one planning pass: whether a group has
+// requests with windows left, and the submission time of its oldest one.
+struct Demand {
+    std::vector<char> busy;
+    std::vector<double> oldest;
+};
+
+// A group whose requests wait for more than this behind newer work may
+// evict a table that still has pending requests.
+constexpr double kEvictSlack = 0.25;
+
+// Makes g resident, evicting least-recently-used idle tables. Tables with
+// pending requests are kept unless g's oldest request is older than all of
+// theirs by kEvictSlack: resident work finishes before its table is swapped
+// out (no thrashing when many requests arrive together), and a long wait
+// still gets its turn. Evicts nothing when g cannot be made to fit.
+ibs_status make_resident(ibs_server *s, Group &g, const Demand *dem = nullptr, double gOldest = 0)
 {
     if (g.dev)
         return IBS_OK;
@@ -396,18 +412,34 @@ ibs_status make_resident(ibs_server *s, Group &g)
     for (auto &o : s->groups)
         if (o->dev && o->loading)
             table_ready(*o);
-    // evict least-recently-used idle tables until this one fits
-    while (s->resident + g.bytes() > s->budget) {
-        Group *victim = nullptr;
-        for (auto &o : s->groups)
-            if (o->dev && !o->inflight && !o->loading && (!victim || o->lastUse < victim->lastUse))
-                victim = o.get();
-        if (!victim)
-            return IBS_ERR_STATE; // everything resident is in use: retry later
-        IBS_CUDA(cudaFreeAsync(victim->dev, s->side), "table eviction");
-        victim->dev = nullptr;
-        s->resident -= victim->bytes();
-        s->st.evictions++;
+    if (s->resident + g.bytes() > s->budget) {
+        const uint64_t need = s->resident + g.bytes() - s->budget;
+        std::vector<Group *> cand;
+        for (auto &o : s->groups) {
+            if (!o->dev || o->inflight || o->loading || o.get() == &g)
+                continue;
+            const bool busy = dem && dem->busy[o->id];
+            if (busy && !(dem->oldest[o->id] > gOldest + kEvictSlack))
+                continue;
+            cand.push_back(o.get());
+        }
+        std::sort(cand.begin(), cand.end(), [dem](const Group *x, const Group *y) {
+            const bool bx = dem && dem->busy[x->id], by = dem && dem->busy[y->id];
+            return bx != by ? !bx : x->lastUse < y->lastUse;
+        });
+        uint64_t freed = 0;
+        size_t take = 0;
+        while (take < cand.size() && freed < need)
+            freed += cand[take++]->bytes();
+        if (freed < need)
+            return IBS_ERR_STATE; // wait for tables in use to finish
+        for (size_t i = 0; i < take; ++i) {
+            Group *victim = cand[i];
+            IBS_CUDA(cudaFreeAsync(victim->dev, s->side), "table eviction");
+            victim->dev = nullptr;
+            s->resident -= victim->bytes();
+            s->st.evictions++;
+        }
     }
     IBS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&g.dev), g.bytes(), s->side), "table reload alloc");
     IBS_CUDA(cudaMemcpyAsync(g.dev, g.host, g.bytes(), cudaMemcpyHostToDevice, s->side), "table reload");
@@ -651,11 +683,26 @@ bool iterate(ibs_server *s)
                 break;
         }
         const double t = s->now();
-        std::vector<uint32_t> ready;
+        // groups in the order of their oldest pending request
+        Demand dem;
+        dem.busy.assign(s->groups.size(), 0);
+        dem.oldest.assign(s->groups.size(), 0.0);
+        std::vector<std::pair<double, uint32_t>> order;
         for (auto &d : demand) {
+            double o = d.second.front()->submitT;
+            for (Request *r : d.second)
+                o = std::min(o, r->submitT);
+            dem.busy[d.first] = 1;
+            dem.oldest[d.first] = o;
+            order.push_back({o, d.first});
+        }
+        std::sort(order.begin(), order.end());
+        std::vector<uint32_t> ready;
+        for (auto &od : order) {
+            auto &d = *demand.find(od.second);
             Group &g = *s->groups[d.first];
             if (!g.dev) {
-                const ibs_status rs = make_resident(s, g);
+                const ibs_status rs = make_resident(s, g, &dem, od.first);
                 if (rs == IBS_ERR_STATE)
                     continue; // every resident table is busy: retry after a retire
                 if (rs != IBS_OK) {
