@@ -147,7 +147,17 @@ __global__ void k_stash_move(const ulonglong2 *old, uint64_t oldEntries, unsigne
     }
 }
 
-template <int NB>
+// The span kernel in three modes. kScan: probe and fold every sample's
+// statistics (one pass). kMaskPass: probe only k-mers whose bucket lies in
+// [bLo, bHi) and store (first pass) or OR in (later passes) their sample
+// masks, 16 bits per position, into `masks`. kStats: fold the statistics
+// from the stored masks. A joint table far larger than the GPU's address
+// translation reach probes much slower at random; cutting its buckets into
+// ranges probed in separate passes keeps each pass's random loads inside
+// one range.
+enum : int { kScan = 0, kMaskPass = 1, kStats = 2 };
+
+template <int NB, int MODE>
 __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__restrict__ seq,
                                                      const uint64_t *__restrict__ mask,
                                                      const WinDesc *__restrict__ win,
@@ -155,7 +165,8 @@ __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__r
                                                      uint64_t nSpans, uint32_t spanLen,
                                                      uint32_t nSamples,
                                                      unsigned long long *__restrict__ work,
-                                                     SegStats *__restrict__ out)
+                                                     SegStats *__restrict__ out, uint16_t *__restrict__ masks,
+                                                     uint64_t bLo, uint64_t bHi, bool firstPass)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t k = t.g.k;
@@ -180,12 +191,13 @@ __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__r
         const uint32_t nPos = win[lo].nPos;
         const uint32_t p0 = (uint32_t)(s - __ldg(span0 + lo)) * spanLen;
         const uint32_t p1 = min(p0 + spanLen, nPos);
+        uint16_t *spanMasks = masks + s * spanLen - p0; // position q of the span at spanMasks[q]
         SegStats acc = seg_empty(); // lane j < nSamples: sample j
         for (uint32_t p = p0; p < p1; p += 32 * NB) {
             uint4 v0[NB], v1[NB];
             uint64_t code[NB];
             uint32_t fp[NB];
-            bool valid[NB];
+            bool valid[NB], mine[NB];
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
                 const uint32_t q = p + 32 * b + lane;
@@ -197,7 +209,8 @@ __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__r
                 const uint64_t h = perm_hash(code[b], t.g.bits);
                 const uint64_t r = bucket_of(h, t.g);
                 fp[b] = (uint32_t)fp_of(h, t.g);
-                if (valid[b]) {
+                mine[b] = valid[b] && (MODE != kMaskPass || (r >= bLo && r < bHi));
+                if (MODE != kStats && mine[b]) {
                     v0[b] = __ldg(t.buckets + 2 * r);
                     v1[b] = __ldg(t.buckets + 2 * r + 1);
                 } else {
@@ -207,11 +220,20 @@ __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__r
             }
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
+                const uint32_t q = p + 32 * b + lane;
                 uint32_t m = 0;
-                if (valid[b]) {
+                if (MODE == kStats) {
+                    if (valid[b])
+                        m = spanMasks[q];
+                } else if (mine[b]) {
                     m = bucket_mask(v0[b], v1[b], fp[b]);
                     if (m & 0x80000000u)
                         m = stash_mask(t, code[b]);
+                }
+                if (MODE == kMaskPass) {
+                    if (q < p1 && (firstPass || m))
+                        spanMasks[q] = (uint16_t)(firstPass ? m : (spanMasks[q] | m));
+                    continue;
                 }
                 const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
                 uint32_t myH = 0;
@@ -224,7 +246,7 @@ __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__r
                     acc = seg_combine(acc, block_stats_serial(V, myH, (int)k), (int)k);
             }
         }
-        if (lane < nSamples)
+        if (MODE != kMaskPass && lane < nSamples)
             out[(uint64_t)lane * nSpans + s] = acc;
     }
 }
@@ -547,10 +569,21 @@ extern "C" ibs_status ibs_panel_table_probe(ibs_panel_table *p, const uint64_t *
     return IBS_OK;
 }
 
+// Bucket-range passes of a scan: one while the bucket array is within the
+// pass size (ibs_tuning.panel_pass_mb, default 48 GiB), else one per pass
+// size of buckets.
+static uint32_t pass_count(const ibs_panel_table *p)
+{
+    const uint64_t passBytes = (tuning().panel_pass_mb ? (uint64_t)tuning().panel_pass_mb : 48ull << 10) << 20;
+    const uint64_t bytes = p->geom.nBuckets * 32;
+    return (uint32_t)std::max<uint64_t>(1, (bytes + passBytes - 1) / passBytes);
+}
+
 // Plan and scratch of (reference, W) for the panel scan.
 static ibs_status panel_plan(ibs_panel_table *p, const ibs_reference *ref, uint32_t W)
 {
-    if (p->planRef == ref && p->plan.W == W && p->plan.dWin && p->planLens == ref->lens)
+    if (p->planRef == ref && p->plan.W == W && p->plan.dWin && p->planLens == ref->lens &&
+        (pass_count(p) <= 1 || p->dMasks))
         return IBS_OK;
     p->plan.release();
     plan_windows(p->plan, ref->lens, ref->baseOff, W, p->geom.k, kSpanLen);
@@ -571,6 +604,12 @@ static ibs_status panel_plan(ibs_panel_table *p, const ibs_reference *ref, uint3
         IBS_CUDA(cudaMalloc(&p->dSpans, need * sizeof(SegStats)), "panel span scratch");
         p->spansCap = need;
     }
+    // per-position sample masks between the passes of a multi-pass scan
+    cudaFree(p->dMasks);
+    p->dMasks = nullptr;
+    if (pass_count(p) > 1)
+        IBS_CUDA(cudaMalloc(&p->dMasks, std::max<uint64_t>(1, p->plan.nSpans * p->plan.spanLen) * 2),
+                 "panel mask scratch");
     p->planRef = ref;
     p->planLens = ref->lens;
     if (p->graph) {
@@ -584,13 +623,33 @@ static ibs_status panel_enqueue(ibs_panel_table *p, const ibs_reference *ref, ib
                                 cudaStream_t st)
 {
     const ScanPlan &pl = p->plan;
-    IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
+    const uint32_t passes = pass_count(p);
     if (pl.nSpans) {
         const int grid = sm_count() * 6;
-        k_panel_spans<kNB><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
-                                                 (uint32_t)pl.nWin, pl.nSpans, pl.spanLen, p->nSamples,
-                                                 p->dCounters + 1, p->dSpans);
-        IBS_LAUNCHED();
+        if (passes <= 1) {
+            IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
+            k_panel_spans<kNB, kScan><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
+                                                            (uint32_t)pl.nWin, pl.nSpans, pl.spanLen,
+                                                            p->nSamples, p->dCounters + 1, p->dSpans, nullptr,
+                                                            0, 0, false);
+            IBS_LAUNCHED();
+        } else {
+            const uint64_t nb = p->geom.nBuckets;
+            for (uint32_t i = 0; i < passes; ++i) {
+                IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
+                k_panel_spans<kNB, kMaskPass><<<grid, 256, 0, st>>>(
+                    p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0, (uint32_t)pl.nWin, pl.nSpans,
+                    pl.spanLen, p->nSamples, p->dCounters + 1, p->dSpans, p->dMasks, nb * i / passes,
+                    nb * (i + 1) / passes, i == 0);
+                IBS_LAUNCHED();
+            }
+            IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
+            k_panel_spans<kNB, kStats><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
+                                                             (uint32_t)pl.nWin, pl.nSpans, pl.spanLen,
+                                                             p->nSamples, p->dCounters + 1, p->dSpans, p->dMasks,
+                                                             0, 0, false);
+            IBS_LAUNCHED();
+        }
     }
     if (pl.nWin && p->nSamples) {
         k_panel_finalize<<<grid_for(pl.nWin * p->nSamples), 256, 0, st>>>(
@@ -725,6 +784,7 @@ extern "C" void ibs_panel_table_close(ibs_panel_table *p)
             cudaGraphExecDestroy(p->graph);
         p->plan.release();
         cudaFree(p->dSpans);
+        cudaFree(p->dMasks);
         cudaFree(p->buckets);
         cudaFree(p->stash);
         cudaFree(p->dErr);

@@ -31,7 +31,7 @@ static std::mutex g_tuneMu;
 // plain 2 Gbp x 2.19e9 k-mers): minimizer table at 2 keys per 32-byte
 // sector, spans of 2048 positions, 2 blocks in flight, 512 threads, 16 CTAs
 // per SM.
-static ibs_tuning g_tune = {2048, 2, 512, 16, 2.0, FMT_MZ8, {0, 0, 0}};
+static ibs_tuning g_tune = {2048, 2, 512, 16, 2.0, FMT_MZ8, 0, {0, 0}};
 
 const ibs_tuning &tuning() { return g_tune; }
 
@@ -1204,6 +1204,8 @@ extern "C" ibs_status ibs_set_tuning(const ibs_tuning *t)
         n.keys_per_bucket = t->keys_per_bucket;
     if (t->table_format)
         n.table_format = t->table_format == 0xffffffffu ? 0 : t->table_format;
+    if (t->panel_pass_mb)
+        n.panel_pass_mb = t->panel_pass_mb == 0xffffffffu ? 0 : t->panel_pass_mb;
     g_tune = n;
     return IBS_OK;
 }

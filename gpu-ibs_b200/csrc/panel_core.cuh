@@ -136,6 +136,7 @@ struct ibs_panel_table {
     std::vector<uint64_t> planLens;
     ibs::ScanPlan plan;
     ibs::SegStats *dSpans = nullptr;
+    uint16_t *dMasks = nullptr; // per-position masks of a multi-pass scan
     uint64_t spansCap = 0;
     // captured scan graph for (reference, W, rows, stream)
     cudaGraphExec_t graph = nullptr;

@@ -71,7 +71,7 @@ class ServerStats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("span_len", C.c_uint32), ("blocks_in_flight", C.c_uint32), ("block_threads", C.c_uint32),
                 ("ctas_per_sm", C.c_uint32), ("keys_per_bucket", C.c_double), ("table_format", C.c_uint32),
-                ("reserved", C.c_uint32 * 3)]
+                ("panel_pass_mb", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}

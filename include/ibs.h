@@ -357,8 +357,12 @@ typedef struct ibs_tuning {
     uint32_t ctas_per_sm;      /* resident CTAs per SM the grid is sized for */
     double keys_per_bucket;    /* default load of new tables */
     uint32_t table_format;     /* default format of new tables (0 = automatic, 4 = minimizer buckets) */
-    uint32_t reserved[3];
+    uint32_t panel_pass_mb;    /* joint-table scans probe bucket ranges of at most this many MiB per
+                                  pass (random loads over a larger range translate slowly); 0 = 48 GiB */
+    uint32_t reserved[2];
 } ibs_tuning;
+/* Fields left 0 keep their value; table_format and panel_pass_mb take
+ * 0xffffffff to go back to 0 (automatic / the default). */
 ibs_status ibs_set_tuning(const ibs_tuning *t);
 void ibs_get_tuning(ibs_tuning *t);
 

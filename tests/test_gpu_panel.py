@@ -107,3 +107,39 @@ def test_panel_stash_grows_when_keys_exceed_the_estimate():
         assert np.array_equal(panel[i], ib.scan(t, ref, 5000)), f"sample {i}"
         t.close()
     pt.close()
+
+
+def test_panel_scan_in_bucket_range_passes_equals_one_pass():
+    # a joint table scanned in several bucket-range passes (the masks of
+    # each pass kept per position) gives the one-pass rows
+    ref_spec = ib.RefSpec(seed=79, lens=[400_000, 90_000, 24], n_frac=0.003, n_run=(1, 200))
+    seq, mask = ref_spec.reference_host()
+    samples = _samples(ref_spec, seq, mask, 16)
+    union = len(np.unique(np.concatenate(samples)))
+    pt = ib.PanelTable(25, union)
+    for c in samples:
+        pt.add_codes(c, len(c), on_device=False)
+    ref = ib.Reference(seq, mask, ref_spec.lens)
+    one = pt.scan(ref, 5000)
+    nbytes = pt.info()[0].n_buckets * 32
+    assert nbytes > 3 << 20
+    t = ib.get_tuning()
+    t.panel_pass_mb = 1  # several passes over this table
+    ib.set_tuning(t)
+    try:
+        many = pt.scan(ref, 5000)
+        import torch
+        n = ib.window_count(ref_spec.lens, 5000, 25)
+        dev = torch.zeros(n * 16 * 6, dtype=torch.int32, device="cuda")
+        st = torch.cuda.Stream()
+        for _ in range(2):  # captured, then replayed
+            pt.scan_async(ref, 5000, dev.data_ptr(), n * 16, st.cuda_stream)
+            st.synchronize()
+            assert np.array_equal(dev.cpu().numpy().view(ib.WINDOW_DTYPE).reshape(16, n), one)
+    finally:
+        t.panel_pass_mb = 0xffffffff
+        ib.set_tuning(t)
+    assert ib.get_tuning().panel_pass_mb == 0
+    assert np.array_equal(many, one)
+    pt.close()
+    ref.free()
