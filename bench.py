@@ -1008,7 +1008,7 @@ def main():
                     help="memory-admitted serving: 48 samples, tables ~3x the server's budget")
     ap.add_argument("--admit-samples", type=int, default=48)
     ap.add_argument("--admit-scale", type=float, default=1.0, help="reference length scale")
-    ap.add_argument("--admit-sample-scale", type=float, default=0.12,
+    ap.add_argument("--admit-sample-scale", type=float, default=0.1,
                     help="sample size scale: the pinned host images of all 48 tables must fit the "
                          "host's memory (196 GB on the B200 boxes here)")
     ap.add_argument("--admit-overcommit", type=float, default=3.0,
