@@ -118,12 +118,12 @@ __device__ __forceinline__ uint32_t bucket_match(const uint4 &v0, const uint4 &v
 template <uint32_t FMT>
 __device__ __forceinline__ bool table_lookup(const TableView &t, uint64_t code)
 {
-    if (FMT == FMT_MZ8) {
-        uint64_t r;
-        uint32_t slot;
+    if (FMT == FMT_MZ8 || FMT == FMT_MZ6) {
+        uint64_t r, slot;
         mz::locate(code, t.g, r, slot);
         const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);
-        const uint32_t m = bucket_match<FMT_B8X32>(v0, v1, slot);
+        const uint32_t m = FMT == FMT_MZ8 ? bucket_match<FMT_B8X32>(v0, v1, slot)
+                                          : bucket_match<FMT_B6X40>(v0, v1, slot);
         return m == 1u || (m == 2u && stash_lookup(t, code));
     }
     const uint64_t h = perm_hash(code, t.g.bits);

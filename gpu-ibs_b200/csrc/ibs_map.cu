@@ -178,6 +178,8 @@ ibs_status coverage_device(ibs_table *t, const ibs_reference *ref, uint8_t *dCov
         k_map_spans<FMT_B8X32><<<grid, 256>>>(v, ref->dSeq, ref->dMask, dSpans, spans.size(), dCov);
     else if (t->geom.format == FMT_MZ8)
         k_map_spans<FMT_MZ8><<<grid, 256>>>(v, ref->dSeq, ref->dMask, dSpans, spans.size(), dCov);
+    else if (t->geom.format == FMT_MZ6)
+        k_map_spans<FMT_MZ6><<<grid, 256>>>(v, ref->dSeq, ref->dMask, dSpans, spans.size(), dCov);
     else
         k_map_spans<FMT_B6X40><<<grid, 256>>>(v, ref->dSeq, ref->dMask, dSpans, spans.size(), dCov);
     IBS_LAUNCHED();

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(256) k_na_spans(TableView t, const uint64_t *_
                 const uint64_t h = perm_hash(code[b], t.g.bits);
                 const uint64_t r = bucket_of(h, t.g);
                 fp[b] = fp_of(h, t.g);
-                if (valid[b] && FMT != FMT_MZ8) {
+                if (valid[b] && !is_mz(FMT)) {
                     v0[b] = __ldg(t.buckets + 2 * r);
                     v1[b] = __ldg(t.buckets + 2 * r + 1);
                 } else {
@@ -191,9 +191,9 @@ __global__ void __launch_bounds__(256) k_na_spans(TableView t, const uint64_t *_
             for (int b = 0; b < NB; ++b) {
                 bool hit = false;
                 if (valid[b]) {
-                    if constexpr (FMT == FMT_MZ8) {
+                    if constexpr (FMT == FMT_MZ8 || FMT == FMT_MZ6) {
                         // minimizer table: each lane finds its k-mer's minimizer on its own
-                        hit = table_lookup<FMT_MZ8>(t, code[b]);
+                        hit = table_lookup<FMT>(t, code[b]);
                     } else {
                         const uint32_t m = bucket_match<FMT>(v0[b], v1[b], fp[b]);
                         hit = m == 1u || (m == 2u && stash_lookup(t, code[b]));
@@ -285,7 +285,7 @@ extern "C" ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev
         set_error("ibs_scan_noalloc: bad argument");
         return IBS_ERR_ARG;
     }
-    if (t->geom.format != FMT_B8X32 && t->geom.format != FMT_B6X40 && t->geom.format != FMT_MZ8) {
+    if (t->geom.format != FMT_B8X32 && t->geom.format != FMT_B6X40 && !is_mz(t->geom.format)) {
         set_error("ibs_scan_noalloc: unknown table format");
         return IBS_ERR_UNSUPPORTED;
     }
@@ -346,6 +346,9 @@ extern "C" ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev
                                                              n_contigs, W, nSpans, dSpans);
         else if (t->geom.format == FMT_MZ8)
             k_na_spans<FMT_MZ8, kNB><<<grid, 256, 0, st>>>(t->view(), seq2bit_dev, nmask_dev, dDesc,
+                                                           n_contigs, W, nSpans, dSpans);
+        else if (t->geom.format == FMT_MZ6)
+            k_na_spans<FMT_MZ6, kNB><<<grid, 256, 0, st>>>(t->view(), seq2bit_dev, nmask_dev, dDesc,
                                                            n_contigs, W, nSpans, dSpans);
         else
             k_na_spans<FMT_B6X40, kNB><<<grid, 256, 0, st>>>(t->view(), seq2bit_dev, nmask_dev, dDesc,

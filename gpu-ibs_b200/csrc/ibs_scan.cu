@@ -254,8 +254,9 @@ __device__ __forceinline__ MzPos mz_pos(const uint64_t *__restrict__ seq, const 
 // leftmost-in-the-canonical-k-mer rule holds on either strand; its line hash
 // comes from the keying lane by shuffle. Lanes whose k-mers share a
 // minimizer load sectors of one line. K > 0 fixes k at compile time (the
-// shifts and masks fold); K = 0 reads it from the table.
-template <int NB, uint32_t K>
+// shifts and masks fold); K = 0 reads it from the table. SEC is the sector
+// layout: FMT_B8X32 (format MZ8) or FMT_B6X40 (format MZ6).
+template <int NB, uint32_t K, uint32_t SEC>
 __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64_t *__restrict__ seq,
                                                        const uint64_t *__restrict__ mask,
                                                        const WinDesc *__restrict__ win,
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                 ps[b] = mz_pos(seq, mask, base + min(p + 32 * b + lane, lastM), k, m);
             next = ps[NB];
             uint4 v0[NB], v1[NB];
-            uint32_t slot[NB];
+            uint64_t slot[NB];
             bool valid[NB];
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
@@ -337,7 +338,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
             for (int b = 0; b < NB; ++b) {
                 bool hit = false;
                 if (valid[b]) {
-                    const uint32_t mt = bucket_match<FMT_B8X32>(v0[b], v1[b], slot[b]);
+                    const uint32_t mt = bucket_match<SEC>(v0[b], v1[b], slot[b]);
                     hit = mt == 1u || (mt == 2u && stash_lookup(t, ps[b].code));
                 }
                 V[b] = __ballot_sync(FULL, valid[b]);
@@ -444,11 +445,17 @@ static void launch_nb(const ibs_table *t, const uint64_t *dSeq, const uint64_t *
                       uint64_t s0, uint64_t s1, SegStats *dSpans, cudaStream_t st, int grid, int threads)
 {
     if (FMT == FMT_MZ8 && t->geom.k == 25)
-        k_scan_spans_mz<NB, 25><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
-                                                          (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
+        k_scan_spans_mz<NB, 25, FMT_B8X32><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
+                                                                     (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
     else if (FMT == FMT_MZ8)
-        k_scan_spans_mz<NB, 0><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
-                                                         (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
+        k_scan_spans_mz<NB, 0, FMT_B8X32><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
+                                                                    (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
+    else if (FMT == FMT_MZ6 && t->geom.k == 31)
+        k_scan_spans_mz<NB, 31, FMT_B6X40><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
+                                                                     (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
+    else if (FMT == FMT_MZ6)
+        k_scan_spans_mz<NB, 0, FMT_B6X40><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
+                                                                    (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
     else
         k_scan_spans<FMT, NB><<<grid, threads, 0, st>>>(t->view(), dSeq, dMask, p.dWin, p.dSpan0,
                                                         (uint32_t)p.nWin, s0, s1, p.spanLen, dSpans);
@@ -483,6 +490,8 @@ static ibs_status launch_spans(const ibs_table *t, const uint64_t *dSeq, const u
         launch_spans_fmt<FMT_B8X32>(t, dSeq, dMask, p, s0, s1, dSpans, st);
     else if (t->geom.format == FMT_MZ8)
         launch_spans_fmt<FMT_MZ8>(t, dSeq, dMask, p, s0, s1, dSpans, st);
+    else if (t->geom.format == FMT_MZ6)
+        launch_spans_fmt<FMT_MZ6>(t, dSeq, dMask, p, s0, s1, dSpans, st);
     else
         launch_spans_fmt<FMT_B6X40>(t, dSeq, dMask, p, s0, s1, dSpans, st);
     IBS_LAUNCHED();

@@ -58,19 +58,23 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
     g.bits = 2 * k;
     uint32_t fmt = o ? o->force_format : 0;
     const bool tunedMz = tuning().table_format == FMT_MZ8;
-    if (fmt == 0 && tunedMz && k >= 16 && k <= 27) {
+    // minimum line count of a minimizer table: its slot values must fit 31
+    // bits (B8x32 sectors, k <= 27) or 40 bits (B6x40 sectors, k <= 31)
+    auto mzMinLog2 = [&](uint32_t f) { return (int)(2 * k) - (f == FMT_MZ8 ? 27 : 36); };
+    if (fmt == 0 && tunedMz && k >= 16 && k <= 31) {
         // the tuned default, where the minimizer layout applies and its
-        // minimum line count (2^(2k-27)) does not oversize the table
+        // minimum line count does not oversize the table
+        const uint32_t f = k <= 27 ? FMT_MZ8 : FMT_MZ6;
         const double want = (double)nKeys / tuning().keys_per_bucket / mz::kSectorsPerLine;
-        if (2 * k <= 27 || want >= (double)(1ull << (2 * k - 27)))
-            fmt = FMT_MZ8;
+        if (mzMinLog2(f) <= 0 || want >= (double)(1ull << mzMinLog2(f)))
+            fmt = f;
     }
     if (fmt == FMT_AUTO_HASH)
         fmt = 0;
     // the tuned load belongs to the tuned layout; hash tables under a tuned
     // minimizer default keep the hash layout's default of 4 keys per bucket
     double lam = tuning().keys_per_bucket;
-    if (tunedMz && fmt != FMT_MZ8)
+    if (tunedMz && !is_mz(fmt))
         lam = 4.0;
     if (o && o->keys_per_bucket > 0)
         lam = o->keys_per_bucket;
@@ -86,13 +90,14 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
     const uint64_t min8 = g.bits > 31 ? (1ull << (g.bits - 31)) : 1;
     const uint64_t n6 = clampN((uint64_t)((double)nKeys / (lam * 6.0 / 8.0)) + 1);
     const uint64_t min6 = g.bits > 40 ? (1ull << (g.bits - 40)) : 1;
-    if (fmt == FMT_MZ8) {
-        // minimizer lines of four sectors: the slot value needs nLines >= 2^(2k-27)
-        g.format = FMT_MZ8;
+    if (is_mz(fmt)) {
+        // minimizer lines of four sectors, at least 2^mzMinLog2 of them
+        g.format = fmt;
         const uint32_t m = mz::m_of(k);
-        const uint64_t minLines = g.bits > 27 ? (1ull << (g.bits - 27)) : 1;
+        const uint64_t minLines = mzMinLog2(fmt) > 0 ? (1ull << mzMinLog2(fmt)) : 1;
+        const uint64_t want = fmt == FMT_MZ8 ? n8 : n6; // sectors at the load
         const uint64_t nLines =
-            std::min<uint64_t>(std::max((n8 + mz::kSectorsPerLine - 1) / mz::kSectorsPerLine, minLines),
+            std::min<uint64_t>(std::max((want + mz::kSectorsPerLine - 1) / mz::kSectorsPerLine, minLines),
                                1ull << std::min<uint32_t>(2 * m, 40));
         g.nBuckets = nLines * mz::kSectorsPerLine;
         g.fpBits = 2 * m - floor_log2(nLines);
@@ -116,10 +121,8 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
 // Bucket and stored fingerprint of a key in either table family.
 __device__ __forceinline__ void locate_key(uint64_t code, const TableGeom &g, uint64_t &r, uint64_t &fp)
 {
-    if (g.format == FMT_MZ8) {
-        uint32_t slot;
-        mz::locate(code, g, r, slot);
-        fp = slot;
+    if (is_mz(g.format)) {
+        mz::locate(code, g, r, fp);
         return;
     }
     const uint64_t h = perm_hash(code, g.bits);
@@ -286,7 +289,8 @@ static ibs_status build_from_device_codes(ibs_table *t, const uint64_t *dCodes, 
     const uint64_t nb = g.nBuckets;
     IBS_CUDA(cudaMalloc(&t->buckets, nb * 32), "table alloc");
     t->deviceBytes = nb * 32;
-    IBS_CUDA(cudaMemset(t->buckets, g.format == FMT_B6X40 ? 0x00 : 0xff, nb * 32), "table init");
+    IBS_CUDA(cudaMemset(t->buckets, g.format == FMT_B6X40 || g.format == FMT_MZ6 ? 0x00 : 0xff, nb * 32),
+             "table init");
     uint32_t *cnt = nullptr;
     unsigned long long *dOverflow = nullptr;
     int *dErr = nullptr;
@@ -507,7 +511,11 @@ static ibs_status check_format(uint32_t k, const ibs_table_opts *o)
         set_error("minimizer-bucketed tables (format 4) need 16 <= k <= 27");
         return IBS_ERR_UNSUPPORTED;
     }
-    if (o && o->force_format > FMT_AUTO_HASH) {
+    if (o && o->force_format == FMT_MZ6 && (k < 16 || k > 31)) {
+        set_error("minimizer-bucketed tables with 40-bit slots (format 6) need 16 <= k <= 31");
+        return IBS_ERR_UNSUPPORTED;
+    }
+    if (o && (o->force_format > FMT_MZ6 || o->force_format == FMT_PANEL)) {
         set_error("unknown table format " + std::to_string(o->force_format));
         return IBS_ERR_ARG;
     }
@@ -801,6 +809,8 @@ extern "C" ibs_status ibs_probe(ibs_table *t, const uint64_t *codes, uint64_t n,
             k_probe<FMT_B8X32><<<grid_for(n, 256), 256>>>(t->view(), dCodes, n, dHits);
         else if (t->geom.format == FMT_MZ8)
             k_probe<FMT_MZ8><<<grid_for(n, 256), 256>>>(t->view(), dCodes, n, dHits);
+        else if (t->geom.format == FMT_MZ6)
+            k_probe<FMT_MZ6><<<grid_for(n, 256), 256>>>(t->view(), dCodes, n, dHits);
         else
             k_probe<FMT_B6X40><<<grid_for(n, 256), 256>>>(t->view(), dCodes, n, dHits);
         IBS_LAUNCHED();
@@ -830,6 +840,8 @@ static ibs_status count_present_device(ibs_table *t, const uint64_t *dCodes, uin
         k_count_present<FMT_B8X32><<<grid, 256>>>(t->view(), dCodes, n, dCount);
     else if (t->geom.format == FMT_MZ8)
         k_count_present<FMT_MZ8><<<grid, 256>>>(t->view(), dCodes, n, dCount);
+    else if (t->geom.format == FMT_MZ6)
+        k_count_present<FMT_MZ6><<<grid, 256>>>(t->view(), dCodes, n, dCount);
     else
         k_count_present<FMT_B6X40><<<grid, 256>>>(t->view(), dCodes, n, dCount);
     IBS_LAUNCHED();

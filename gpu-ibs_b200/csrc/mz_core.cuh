@@ -10,7 +10,7 @@
 // would pile two runs into one place.
 //
 // The table is an array of 128-byte lines of four 32-byte sectors; a sector
-// is a B8x32 bucket. The minimizer picks the line and C itself picks one of
+// is a B8x32 bucket (format MZ8) or a B6x40 bucket (format MZ6). The minimizer picks the line and C itself picks one of
 // its four sectors, so a minimizer's k-mers spread over the line and a
 // warp's loads for a run of positions touch one DRAM line.
 //
@@ -22,8 +22,10 @@
 // o (< w <= 8), in orientation s (M or its reverse complement), with the
 // other k - m bases around it:
 //   slot = ((o << 1 | s) << 2(k-m) | C-without-the-m-mer) << hbits | (g mod 2^hbits)
-// which has 2k + 4 - log2(nLines) bits and must fit 31 (B8x32 sentinels):
-// nLines >= 2^(2k-27).
+// which has 2k + 4 - log2(nLines) bits and must fit the sector's slots: 31
+// bits in B8x32 sectors (format MZ8, the sentinels above), nLines >=
+// 2^(2k-27); 40 bits in B6x40 sectors (format MZ6, for k up to 31), nLines
+// >= 2^(2k-36).
 #pragma once
 
 #include "ibs_core.cuh"
@@ -96,14 +98,14 @@ IBS_HD uint64_t mmer_at(uint64_t C, uint32_t k, uint32_t o, uint32_t m)
 // (o, s, C without the m-mer) part of the slot value: the minimizer's
 // offset o in C and its orientation s there (1 when it reads as the reverse
 // complement of its canonical form).
-IBS_HD uint32_t slot_high(uint64_t C, uint32_t k, uint32_t o, uint32_t s)
+IBS_HD uint64_t slot_high(uint64_t C, uint32_t k, uint32_t o, uint32_t s)
 {
     const uint32_t m = m_of(k);
     const uint32_t rbits = 2 * (k - m - o);                    // bases right of the m-mer
     const uint64_t right = rbits ? (C & ((1ull << rbits) - 1)) : 0;
     const uint64_t left = C >> (2 * (k - o));                  // bases left of it (2o bits)
     const uint64_t rest = (left << rbits) | right;             // 2(k-m) bits
-    return (uint32_t)((((uint64_t)o << 1 | s) << (2 * (k - m))) | rest);
+    return (((uint64_t)o << 1 | s) << (2 * (k - m))) | rest;
 }
 
 // Minimizer offset of C by brute force (table build, single probes): the
@@ -129,17 +131,17 @@ IBS_HD uint32_t sector_of(uint64_t C) { return (uint32_t)((C * 0x9e3779b97f4a7c1
 // minimizer sits at offset o with orientation s and line hash g.
 // hbits = 2m - log2(nLines).
 IBS_HD void place(uint64_t C, uint32_t k, uint32_t o, uint32_t s, uint64_t g, uint64_t nBuckets,
-                  uint32_t hbits, uint64_t &bucket, uint32_t &slot)
+                  uint32_t hbits, uint64_t &bucket, uint64_t &slot)
 {
     const uint32_t m = m_of(k);
     const uint64_t line = mulhi64(g << (64 - 2 * m), nBuckets / kSectorsPerLine);
     bucket = line * kSectorsPerLine + sector_of(C);
-    slot = (slot_high(C, k, o, s) << hbits) | (uint32_t)(g & key_mask(hbits));
+    slot = (slot_high(C, k, o, s) << hbits) | (g & key_mask(hbits));
 }
 
 // Slot value and bucket of a canonical k-mer (the build side, and single
 // probes): everything from C itself.
-IBS_HD void locate(uint64_t C, const TableGeom &g, uint64_t &bucket, uint32_t &slot)
+IBS_HD void locate(uint64_t C, const TableGeom &g, uint64_t &bucket, uint64_t &slot)
 {
     const uint32_t m = m_of(g.k);
     const uint32_t o = minimizer_offset(C, g.k);

@@ -60,8 +60,9 @@ typedef struct ibs_table_opts {
     int device;             /* CUDA device ordinal (default 0) */
     double keys_per_bucket; /* target mean keys per 32 B bucket (0 = default 4.0) */
     uint32_t force_format;  /* 0 = the tuned default (ibs_tuning.table_format), 1 = B8x32,
-                               2 = B6x40, 4 = minimizer buckets (16 <= k <= 27),
-                               5 = hash buckets, B8x32 or B6x40 by size */
+                               2 = B6x40, 4 = minimizer lines of B8x32 sectors (16 <= k <= 27),
+                               5 = hash buckets, B8x32 or B6x40 by size,
+                               6 = minimizer lines of B6x40 sectors (16 <= k <= 31) */
     uint32_t reserved[5];
 } ibs_table_opts;
 

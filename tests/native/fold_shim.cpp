@@ -69,7 +69,7 @@ static TableGeom mz_geom(uint32_t k, uint64_t nBuckets)
 
 // Build side: bucket and slot of canonical codes.
 extern "C" void mz_locate(const uint64_t *codes, uint64_t n, uint32_t k, uint64_t nBuckets,
-                          uint64_t *bucket, uint32_t *slot)
+                          uint64_t *bucket, uint64_t *slot)
 {
     const TableGeom g = mz_geom(k, nBuckets);
     for (uint64_t i = 0; i < n; ++i)
@@ -81,7 +81,7 @@ extern "C" void mz_locate(const uint64_t *codes, uint64_t n, uint32_t k, uint64_
 // the next w keys with its leftmost/rightmost offsets, the strand of the
 // canonical k-mer, then bucket and slot. Positions 0..n-k.
 extern "C" void mz_query(const uint8_t *bases, uint64_t n, uint32_t k, uint64_t nBuckets,
-                         uint64_t *bucket, uint32_t *slot)
+                         uint64_t *bucket, uint64_t *slot)
 {
     const TableGeom g = mz_geom(k, nBuckets);
     const uint32_t w = mz::w_of(k), m = mz::m_of(k);

@@ -162,13 +162,15 @@ def test_scan_argument_errors(build_case):
     assert len(ib.scan(t, empty, 1000)) == 0
 
 
-@pytest.mark.parametrize("name", ["edge_k25", "edge_k25_kmc1", "edge_k25_crlf", "plain_1mbp", "edge_k25_gz"])
-def test_minimizer_table_matches_reference_golden(name, build_case):
+@pytest.mark.parametrize("name,fmt", [("edge_k25", 4), ("edge_k25_kmc1", 4), ("edge_k25_crlf", 4), ("plain_1mbp", 4),
+                                      ("edge_k25_gz", 4), ("edge_k31", 6), ("edge_k25", 6), ("plain_1mbp", 6)])
+def test_minimizer_table_matches_reference_golden(name, fmt, build_case):
+    # format 4: B8x32 sectors (k <= 27); format 6: B6x40 sectors (k <= 31)
     gold = corpus.load_golden(name)
     case = build_case(name)
-    t = ib.Table.open(str(case["prefix"]), force_format=4)
+    t = ib.Table.open(str(case["prefix"]), force_format=fmt)
     info = t.info()
-    assert info.format == 4
+    assert info.format == fmt
     ix = orc.Index(str(case["prefix"]))
     assert t.probe(ix.list_codes()).all()
     q = corpus.random_codes(np.random.default_rng(6), 100_000, case["k"])
@@ -197,18 +199,20 @@ def test_minimizer_table_40mbp_and_overflow(tmp_path):
         t.close()
 
 
-def test_minimizer_format_rejects_unsupported_k(build_case):
-    case = build_case("edge_k31")
+@pytest.mark.parametrize("name,fmt", [("edge_k31", 4), ("edge_k32", 6), ("edge_k15", 4), ("edge_k15", 6)])
+def test_minimizer_format_rejects_unsupported_k(name, fmt, build_case):
+    case = build_case(name)
     with pytest.raises(ib.IbsError) as e:
-        ib.Table.open(str(case["prefix"]), force_format=4)
+        ib.Table.open(str(case["prefix"]), force_format=fmt)
     assert e.value.status == 6
 
 
-@pytest.mark.parametrize("k", [16, 21, 22, 24])
-def test_minimizer_table_at_other_k_equals_hash_table(k):
-    # the minimizer kernel's generic-k instance (k = 25 has its own), with
-    # minimizer lengths 16 (k <= 22) and k - 6; rows equal the hash table's,
-    # which the goldens pin to the reference
+@pytest.mark.parametrize("k,fmt", [(16, 4), (21, 4), (22, 4), (24, 4), (16, 6), (25, 6), (28, 6), (31, 6)])
+def test_minimizer_table_at_other_k_equals_hash_table(k, fmt):
+    # the minimizer kernel's generic-k instances (k = 25 in B8x32 sectors and
+    # k = 31 in B6x40 sectors have their own), with minimizer lengths 16
+    # (k <= 22) and k - 6; rows equal the hash table's, which the goldens pin
+    # to the reference
     spec = ib.RefSpec(seed=40 + k, lens=[250_000, 70_000, 23, 5_000], n_frac=0.003, n_run=(1, 150))
     seq, mask = spec.reference_host()
     smp = ib.SampleSpec(seed=400 + k, k=k, class_rate=(0.0001, 0.01, 0.03), class_prob=(0.3, 0.5, 0.2),
@@ -216,8 +220,8 @@ def test_minimizer_table_at_other_k_equals_hash_table(k):
     codes = smp.codes_host(spec, seq, mask)
     ref = ib.Reference(seq, mask, spec.lens)
     th = ib.Table.from_codes(codes, len(codes), k, on_device=False, force_format=5)
-    tm = ib.Table.from_codes(codes, len(codes), k, on_device=False, force_format=4)
-    assert tm.info().format == 4
+    tm = ib.Table.from_codes(codes, len(codes), k, on_device=False, force_format=fmt)
+    assert tm.info().format == fmt
     for W in (1000, 5000):
         assert np.array_equal(ib.scan(tm, ref, W), ib.scan(th, ref, W)), (k, W)
     q = np.concatenate([codes[:20_000], corpus.random_codes(np.random.default_rng(k), 20_000, k)])

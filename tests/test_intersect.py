@@ -57,7 +57,7 @@ def test_device_count_matches_reference(cases, name):
     import ibs_b200 as ib
     c = cases[name]
     want = GOLD["cases"][name]
-    formats = [0, 1, 2] + ([4] if 16 <= c["k"] <= 27 else [])
+    formats = [0, 1, 2] + ([4] if 16 <= c["k"] <= 27 else []) + ([6] if 16 <= c["k"] <= 31 else [])
     for fmt in formats:
         if fmt == 1 and c["k"] > 25:
             continue  # B8x32 needs 2^(2k-31) buckets

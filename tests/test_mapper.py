@@ -49,7 +49,8 @@ def test_device_mapping_matches_reference(name, build_case):
     ref = ib.Reference(seq, mask, lens)
     ix = orc.Index(str(case["prefix"]))
     want_cov = np.concatenate([orc.coverage(ix, s, case["k"]) for s in seqs])
-    formats = [0, 2] + ([1] if case["k"] <= 25 else []) + ([4] if 16 <= case["k"] <= 25 else [])
+    formats = ([0, 2] + ([1] if case["k"] <= 25 else []) + ([4] if 16 <= case["k"] <= 27 else [])
+               + ([6] if 16 <= case["k"] <= 31 else []))
     for fmt in formats:
         t = ib.Table.open(str(case["prefix"]), force_format=fmt)
         assert np.array_equal(ib.map_coverage(t, ref).astype(np.int64), want_cov), (name, fmt)

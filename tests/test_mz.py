@@ -19,7 +19,7 @@ def _ptr(a):
 def locate(shim, codes, k, nb):
     codes = np.ascontiguousarray(codes, np.uint64)
     b = np.zeros(len(codes), np.uint64)
-    s = np.zeros(len(codes), np.uint32)
+    s = np.zeros(len(codes), np.uint64)
     shim.mz_locate(_ptr(codes), ctypes.c_uint64(len(codes)), ctypes.c_uint32(k), ctypes.c_uint64(nb),
                    _ptr(b), _ptr(s))
     return b, s
@@ -29,16 +29,27 @@ def query(shim, bases, k, nb):
     bases = np.ascontiguousarray(bases, np.uint8)
     n = max(len(bases) - k + 1, 0)
     b = np.zeros(n, np.uint64)
-    s = np.zeros(n, np.uint32)
+    s = np.zeros(n, np.uint64)
     shim.mz_query(_ptr(bases), ctypes.c_uint64(len(bases)), ctypes.c_uint32(k), ctypes.c_uint64(nb),
                   _ptr(b), _ptr(s))
     return b, s
 
 
-@pytest.mark.parametrize("k", [16, 21, 25, 27])
+def min_lines_log2(k):
+    """log2 of the fewest lines whose slots fit the sector: 31-bit slots of
+    B8x32 sectors (format MZ8) up to k = 27, 40-bit slots of B6x40 sectors
+    (format MZ6) above."""
+    return 2 * k - 27 if k <= 27 else 2 * k - 36
+
+
+def slot_bits(k):
+    return 31 if k <= 27 else 40
+
+
+@pytest.mark.parametrize("k", [16, 21, 25, 27, 28, 31])
 def test_query_side_equals_build_side(native_shim, k):
     rng = np.random.default_rng(k)
-    nb = 4 << max(2 * k - 27, 20)  # four sectors per line, nLines >= 2^(2k-27)
+    nb = 4 << max(min_lines_log2(k), 20)  # four sectors per line
     # random sequence plus repeats that force minimizer ties
     seq = rng.integers(0, 4, 200_000).astype(np.uint8)
     unit = rng.integers(0, 4, 17).astype(np.uint8)
@@ -53,16 +64,16 @@ def test_query_side_equals_build_side(native_shim, k):
         assert np.array_equal(qb, lb) and np.array_equal(qs, ls)
 
 
-@pytest.mark.parametrize("k", [20, 25, 27])
+@pytest.mark.parametrize("k", [20, 25, 27, 28, 31])
 def test_bucket_and_slot_identify_the_kmer(native_shim, k):
     rng = np.random.default_rng(100 + k)
-    nb = 4 << max(2 * k - 27, 18)
+    nb = 4 << max(min_lines_log2(k), 18)
     codes = np.unique(corpus.random_codes(rng, 400_000, k))
     b, s = locate(native_shim, codes, k, nb)
     assert (b < nb).all()
-    assert (s < (1 << 31)).all(), "slot values must stay below the B8x32 sentinels"
-    pairs = b.astype(np.uint64) * np.uint64(1 << 32) + s.astype(np.uint64)
-    assert len(np.unique(pairs)) == len(codes)
+    assert (s < (1 << slot_bits(k))).all(), "slot values must stay below the sector's sentinels"
+    pairs = np.unique(np.stack([b, s], axis=1), axis=0)
+    assert len(pairs) == len(codes)
 
 
 def test_buckets_are_uniform_over_minimizers(native_shim):

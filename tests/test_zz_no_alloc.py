@@ -28,11 +28,11 @@ def _device_inputs(seqs):
 
 
 @pytest.mark.parametrize("name,W,fmt", [("plain_1mbp", 50000, 0), ("edge_k25", 5000, 0), ("edge_k15", 100, 0),
-                                        ("edge_k32", 1000, 0), ("edge_k25", 5000, 4)])
+                                        ("edge_k32", 1000, 0), ("edge_k25", 5000, 4), ("edge_k31", 5000, 6)])
 def test_noalloc_matches_scan_twice(name, W, fmt, build_case):
     import torch
     case = build_case(name)
-    table = ib.Table.open(str(case["prefix"]), force_format=fmt)  # 4: the minimizer table
+    table = ib.Table.open(str(case["prefix"]), force_format=fmt)  # 4, 6: minimizer tables
     ids, seqs = orc.read_sequence_file(str(case["ref"]))
     seq, mask, lens, dseq, dmask = _device_inputs(seqs)
     ref = ib.Reference(seq, mask, lens)
