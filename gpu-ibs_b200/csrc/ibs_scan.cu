@@ -220,17 +220,23 @@ struct MzPos {
     bool isFwd, acgt;
 };
 
+// The 32 bases from packed base G (bits 2t) and the N bits of the k from G,
+// read as 32-bit words (base b at bits 2(b % 16) of word b / 16, N bit b at
+// bit b % 32 of word b / 32) and joined by funnel shifts. The words read lie
+// inside the 64-bit words G / 32 .. G / 32 + 1 and G / 64 .. G / 64 + 1.
 __device__ __forceinline__ MzPos mz_pos(const uint64_t *__restrict__ seq, const uint64_t *__restrict__ mask,
                                         uint64_t G, uint32_t k, uint32_t m)
 {
     MzPos r;
-    const uint64_t wi = G >> 5;
-    const uint32_t sh = (uint32_t)(G & 31) * 2;
-    const uint64_t x = (__ldg(seq + wi) >> sh) | ((__ldg(seq + wi + 1) << (63 - sh)) << 1);
-    const uint64_t mi = G >> 6;
-    const uint32_t ms = (uint32_t)(G & 63);
-    const uint64_t mm = (__ldg(mask + mi) >> ms) | ((__ldg(mask + mi + 1) << (63 - ms)) << 1);
-    r.acgt = (mm & key_mask(k)) == 0;
+    const uint32_t *__restrict__ s32 = reinterpret_cast<const uint32_t *>(seq);
+    const uint32_t *__restrict__ m32 = reinterpret_cast<const uint32_t *>(mask);
+    const uint64_t wi = G >> 4;
+    const uint32_t sh = (uint32_t)(G & 15) * 2;
+    const uint32_t w0 = __ldg(s32 + wi), w1 = __ldg(s32 + wi + 1), w2 = __ldg(s32 + wi + 2);
+    const uint64_t x = ((uint64_t)__funnelshift_r(w1, w2, sh) << 32) | __funnelshift_r(w0, w1, sh);
+    const uint64_t mi = G >> 5;
+    const uint32_t mm = __funnelshift_r(__ldg(m32 + mi), __ldg(m32 + mi + 1), (uint32_t)(G & 31));
+    r.acgt = (mm & (uint32_t)key_mask(k)) == 0;
     uint64_t y = __brevll(x);
     y = ((y >> 1) & 0x5555555555555555ull) | ((y & 0x5555555555555555ull) << 1); // first base high
     const uint64_t fwd = y >> (64 - 2 * k);
@@ -240,8 +246,9 @@ __device__ __forceinline__ MzPos mz_pos(const uint64_t *__restrict__ seq, const 
     const uint64_t f = y >> (64 - 2 * m);
     const uint64_t mr = ~x & key_mask(2 * m);
     const uint64_t c = f < mr ? f : mr;
-    r.gs = mz::line_hash(c, m) | (f > mr ? 1ull << 62 : 0ull) | (mr > f ? 1ull << 63 : 0ull);
-    r.key = mz::rank_key(c, m);
+    const uint64_t lh = mz::line_hash(c, m);
+    r.gs = lh | (f > mr ? 1ull << 62 : 0ull) | (mr > f ? 1ull << 63 : 0ull);
+    r.key = mz::rank_key_of(lh);
     return r;
 }
 
@@ -250,9 +257,10 @@ __device__ __forceinline__ MzPos mz_pos(const uint64_t *__restrict__ seq, const 
 // needed by the current block's minimizer windows, and the same read gives
 // the k-mer that block probes when its turn comes. A k-mer's minimizer is
 // the minimum over the next w lanes' keys (shuffles across the block
-// boundary), tracked with its leftmost and rightmost offsets so the
-// leftmost-in-the-canonical-k-mer rule holds on either strand; its line hash
-// comes from the keying lane by shuffle. Lanes whose k-mers share a
+// boundary); each key carries its offset j in its 3 low bits (j for a
+// forward k-mer, 7 - j for a reverse one), so one integer minimum per offset
+// keeps the leftmost-in-the-canonical-k-mer rule on either strand. Its line
+// hash comes from the keying lane by shuffle. Lanes whose k-mers share a
 // minimizer load sectors of one line. K > 0 fixes k at compile time (the
 // shifts and masks fold); K = 0 reads it from the table. SEC is the sector
 // layout: FMT_B8X32 (format MZ8) or FMT_B6X40 (format MZ6).
@@ -297,8 +305,12 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                 const uint32_t q = p + 32 * b + lane;
                 valid[b] = q < p1 && ps[b].acgt;
                 const bool isFwd = ps[b].isFwd;
-                // minimizer over the w (<= 8) m-mers starting at q .. q+w-1
-                uint32_t mn = 0xffffffffu, jl = 0, jr = 0;
+                // minimizer over the w (<= 7) m-mers starting at q .. q+w-1:
+                // keys have their low 3 bits clear; j ^ flip there makes the
+                // smallest packed value the leftmost smallest key (forward
+                // k-mer) or the rightmost (reverse k-mer)
+                const uint32_t flip = isFwd ? 0u : 7u;
+                uint32_t best = 0xffffffffu;
 #pragma unroll
                 for (uint32_t j = 0; j < 8; ++j) {
                     if (j < w) {
@@ -308,21 +320,18 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                         // below j -- one shuffle per offset
                         const uint32_t offer = lane < j ? ps[b + 1].key : ps[b].key;
                         const uint32_t v = __shfl_sync(FULL, offer, (lane + j) & 31);
-                        if (v < mn || j == 0) {
-                            mn = v;
-                            jl = jr = j;
-                        } else if (v == mn)
-                            jr = j;
+                        best = min(best, v ^ j ^ flip);
                     }
                 }
+                const uint32_t jm = (best & 7u) ^ flip;
                 // the minimizer's line hash and orientation from the lane that
-                // keyed it: position q + jl (forward k-mer) or q + jr (reverse)
-                const uint32_t src = lane + (isFwd ? jl : jr);
+                // keyed it: position q + jm
+                const uint32_t src = lane + jm;
                 const uint64_t ga = __shfl_sync(FULL, ps[b].gs, src & 31);
                 const uint64_t gc = __shfl_sync(FULL, ps[b + 1].gs, src & 31);
                 const uint64_t gs = src < 32 ? ga : gc;
                 const uint32_t sm = isFwd ? (uint32_t)(gs >> 62) & 1u : (uint32_t)(gs >> 63);
-                const uint32_t o = isFwd ? jl : (w - 1 - jr);
+                const uint32_t o = isFwd ? jm : (w - 1 - jm);
                 uint64_t r;
                 mz::place(ps[b].code, k, o, sm, gs & ((1ull << 62) - 1), t.g.nBuckets, t.g.fpBits, r, slot[b]);
                 if (valid[b]) {

@@ -2,8 +2,8 @@
 //
 // A canonical k-mer C is filed under its minimizer: among C's w = k - m + 1
 // m-mers (m = k - 6 from k = 22, else 16), the one whose canonical form has
-// the smallest rank key -- the top 32 bits of a bijective multiplicative mix
-// of the 2m-bit code -- ties going to the leftmost in C. Consecutive
+// the smallest rank key (29 bits derived from the m-mer's line hash, below),
+// ties going to the leftmost in C. Consecutive
 // reference positions mostly share their minimizer (runs of up to w
 // positions), so their probes fall in one place of the table. m grows with k so that a minimizer rarely occurs at
 // two loci of a large genome (4^19 19-mers against 2e9 positions), which
@@ -66,19 +66,8 @@ IBS_HD uint64_t canon_m(uint64_t v, uint32_t m)
     return v < r ? v : r;
 }
 
-// The 32-bit key minimizers are chosen by: the top bits of a bijective mix
-// (odd multiply, xorshift) of the canonical m-mer. Cheap on purpose: the scan
-// computes one per reference position.
-IBS_HD uint32_t rank_key(uint64_t canonical, uint32_t m)
-{
-    uint64_t x = (canonical * 0x9e3779b97f4a7c15ull) & key_mask(2 * m);
-    x ^= x >> m;
-    return (uint32_t)(x >> (2 * m - 32));
-}
-
-// The line hash of a canonical m-mer: a second bijection of the 2m-bit
-// values, two multiply-xorshift rounds, so the lines stay uniform over the
-// (low-key-biased) minimizers.
+// The line hash of a canonical m-mer: a bijection of the 2m-bit values, two
+// multiply-xorshift rounds, so the lines stay uniform over the minimizers.
 IBS_HD uint64_t line_hash(uint64_t canonical, uint32_t m)
 {
     const uint64_t mask = key_mask(2 * m);
@@ -88,6 +77,18 @@ IBS_HD uint64_t line_hash(uint64_t canonical, uint32_t m)
     x ^= x >> m;
     return x;
 }
+
+// The key minimizers are chosen by: an odd 32-bit multiple of the line
+// hash's low 32 bits, with its low 3 bits cleared. Cheap on purpose: the scan
+// computes one per reference position, and it packs a window offset into the
+// 3 free bits so that one integer minimum per offset finds the leftmost (or,
+// on the other strand, the rightmost) smallest key. The line index comes
+// from the line hash's high bits; for every fixed line the multiples of its
+// low bits are spread evenly over the key range (a golden-ratio multiplier),
+// so picking small keys does not crowd lines.
+IBS_HD uint32_t rank_key_of(uint64_t lineHash) { return ((uint32_t)lineHash * 0x9e3779b1u) & ~7u; }
+
+IBS_HD uint32_t rank_key(uint64_t canonical, uint32_t m) { return rank_key_of(line_hash(canonical, m)); }
 
 // The m-mer of C (2k-bit code, first base high) at offset o.
 IBS_HD uint64_t mmer_at(uint64_t C, uint32_t k, uint32_t o, uint32_t m)

@@ -1,5 +1,6 @@
 // Host build of the window-statistics fold the scan kernel uses
 // (gpu-ibs_b200/csrc/ibs_core.cuh), for property tests on the CPU.
+#include <algorithm>
 #include <cstdint>
 #include "ibs_core.cuh"
 
@@ -113,17 +114,15 @@ extern "C" void mz_query(const uint8_t *bases, uint64_t n, uint32_t k, uint64_t 
         rc &= kmask;
         const bool isFwd = fwd <= rc;
         const uint64_t C = isFwd ? fwd : rc;
-        uint32_t mn = 0xffffffffu, jl = 0, jr = 0;
-        for (uint32_t j = 0; j < w; ++j) {
-            const uint32_t v = key[q + j];
-            if (v < mn || j == 0) {
-                mn = v;
-                jl = jr = j;
-            } else if (v == mn)
-                jr = j;
-        }
-        const uint64_t src = q + (isFwd ? jl : jr);
-        const uint32_t o = isFwd ? jl : (w - 1 - jr);
+        // the kernel's packed minimum: offset j (forward) or 7 - j (reverse)
+        // in the keys' 3 clear low bits
+        const uint32_t flip = isFwd ? 0u : 7u;
+        uint32_t best = 0xffffffffu;
+        for (uint32_t j = 0; j < w; ++j)
+            best = std::min(best, key[q + j] ^ j ^ flip);
+        const uint32_t jm = (best & 7u) ^ flip;
+        const uint64_t src = q + jm;
+        const uint32_t o = isFwd ? jm : (w - 1 - jm);
         mz::place(C, k, o, isFwd ? fnc[src] : rnc[src], lg[src], g.nBuckets, g.fpBits, bucket[q], slot[q]);
     }
     delete[] key;
