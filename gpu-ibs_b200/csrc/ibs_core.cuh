@@ -174,6 +174,102 @@ struct WindowRow {
     int32_t start, end, total_kmers, observed_kmers, variations, kmer_distance;
 };
 
+IBS_HD uint32_t popc64(uint64_t x)
+{
+#if defined(__CUDA_ARCH__)
+    return __popcll(x);
+#else
+    return (uint32_t)__builtin_popcountll(x);
+#endif
+}
+
+// Index of the lowest / highest set bit of x != 0.
+IBS_HD uint32_t ctz64(uint64_t x)
+{
+#if defined(__CUDA_ARCH__)
+    return __ffsll(x) - 1;
+#else
+    return (uint32_t)__builtin_ctzll(x);
+#endif
+}
+
+IBS_HD uint32_t clz64(uint64_t x)
+{
+#if defined(__CUDA_ARCH__)
+    return __clzll(x);
+#else
+    return (uint32_t)__builtin_clzll(x);
+#endif
+}
+
+// Running statistics of one warp's span, fed 64 positions at a time as
+// valid (V) and hit (H) masks (bit i = the i-th position; H a subset of V).
+// The counts, the misses before the span's first hit (lead) and since its
+// last hit (pending) are warp-uniform. Gaps are closed where they end: a gap
+// that ends at a chunk's first hit by every lane alike (lane 0 counts it), a
+// gap inside a chunk by the lane of the hit that ends it. Each lane keeps its
+// own gap sums; the warp adds them up once at the end of the span. Chunks
+// with no valid miss between their first and last hit skip the per-lane
+// search.
+struct SpanFold {
+    uint32_t total = 0, obs = 0, lead = 0, pending = 0;
+    uint32_t gc = 0, d = 0; // this lane's closed gaps and their distance sum
+
+    IBS_HD void add(uint64_t V, uint64_t H, uint32_t lane, int k)
+    {
+        const uint32_t nV = popc64(V);
+        total += nV;
+        if (H == 0) {
+            if (obs == 0)
+                lead += nV;
+            else
+                pending += nV;
+            return;
+        }
+        const uint32_t first = ctz64(H);
+        const uint32_t last = 63 - clz64(H);
+        const uint32_t c0 = popc64(V & ((1ull << first) - 1ull));
+        if (obs == 0) {
+            lead += c0;
+        } else if (pending + c0 > 0 && lane == 0) {
+            gc += 1;
+            d += (uint32_t)gap_distance(pending + c0, k);
+        }
+        obs += popc64(H);
+        // valid misses strictly between the first and the last hit
+        const uint64_t inner = V & ~H & ~((2ull << first) - 1ull) & ((1ull << last) - 1ull);
+        if (inner) {
+            for (uint32_t half = 0; half < 2; ++half) {
+                const uint32_t pos = lane + 32 * half;
+                if (((H >> pos) & 1ull) && pos != first) {
+                    const uint64_t below = (1ull << pos) - 1ull;
+                    const uint32_t prev = 63 - clz64(H & below); // a hit before pos
+                    const uint32_t g = popc64(V & below & ~((2ull << prev) - 1ull));
+                    if (g) {
+                        gc += 1;
+                        d += (uint32_t)gap_distance(g, k);
+                    }
+                }
+            }
+        }
+        pending = last == 63 ? 0u : popc64(V >> (last + 1));
+    }
+
+    // The span's summary, given the sums of gc and d over the warp's lanes.
+    IBS_HD SegStats summary(uint32_t gaps, uint32_t dist) const
+    {
+        SegStats r;
+        r.pad = 0;
+        r.total = total;
+        r.obs = obs;
+        r.lead = obs ? lead : total;
+        r.trail = obs ? pending : total;
+        r.gaps = gaps;
+        r.dist = dist;
+        return r;
+    }
+};
+
 IBS_HD void seg_finish(const SegStats &s, int k, WindowRow &row)
 {
     int64_t var = s.gaps, dist = s.dist;

@@ -16,6 +16,7 @@
 // (src/Window.hpp:29-36), with the windows of chunkSequences
 // (src/Utils.hpp:296-327).
 #include "ibs_internal.cuh"
+#include "scan_device.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -35,100 +36,21 @@ static ibs_tuning g_tune = {2048, 2, 512, 16, 2.0, FMT_MZ8, 0, {0, 0}};
 
 const ibs_tuning &tuning() { return g_tune; }
 
-// Statistics of one 32-position block from its valid (V) and hit (H) ballots
-// (bit i = position p+i; H is a subset of V). Every lane returns the same
-// value. Gaps between two hits of the block are found lane-parallel: the
-// lane of each hit except the first counts the valid misses since the
-// previous hit.
-__device__ __forceinline__ SegStats block_stats(uint32_t V, uint32_t H, uint32_t lane, int k)
-{
-    SegStats b;
-    b.pad = 0;
-    b.total = __popc(V);
-    b.obs = __popc(H);
-    if (H == 0) {
-        b.lead = b.trail = b.total;
-        b.gaps = 0;
-        b.dist = 0;
-        return b;
-    }
-    const uint32_t first = __ffs(H) - 1;
-    const uint32_t last = 31 - __clz(H);
-    b.lead = __popc(V & ((1u << first) - 1u));
-    b.trail = last == 31 ? 0u : __popc(V >> (last + 1));
-    uint32_t g = 0;
-    if (((H >> lane) & 1u) && lane != first) {
-        const uint32_t below = (1u << lane) - 1u;
-        const uint32_t prev = 31 - __clz(H & below);
-        g = __popc(V & below & ~((2u << prev) - 1u));
-    }
-    const uint32_t gc = g > 0 ? 1u : 0u;
-    const uint32_t d = g > 0 ? (uint32_t)gap_distance(g, k) : 0u;
-    b.gaps = __reduce_add_sync(FULL, gc);
-    b.dist = __reduce_add_sync(FULL, d);
-    return b;
-}
+using dev::canonical_at;
 
-// The same for 64 positions (two blocks: bit i = position p+i): each lane
-// closes the gaps that end at its hits among positions lane and lane + 32.
-__device__ __forceinline__ SegStats block_stats64(uint64_t V, uint64_t H, uint32_t lane, int k)
+// Feeds NB consecutive 32-position blocks' ballots to the span fold, two
+// blocks (64 positions) per step.
+template <int NB>
+__device__ __forceinline__ void fold_blocks(SpanFold &fold, const uint32_t (&V)[NB], const uint32_t (&H)[NB],
+                                            uint32_t lane, int k)
 {
-    SegStats b;
-    b.pad = 0;
-    b.total = __popcll(V);
-    b.obs = __popcll(H);
-    if (H == 0) {
-        b.lead = b.trail = b.total;
-        b.gaps = 0;
-        b.dist = 0;
-        return b;
-    }
-    const uint32_t first = __ffsll(H) - 1;
-    const uint32_t last = 63 - __clzll(H);
-    b.lead = __popcll(V & ((1ull << first) - 1ull));
-    b.trail = last == 63 ? 0u : __popcll(V >> (last + 1));
-    uint32_t gc = 0, d = 0;
 #pragma unroll
-    for (uint32_t half = 0; half < 2; ++half) {
-        const uint32_t pos = lane + 32 * half;
-        if (((H >> pos) & 1ull) && pos != first) {
-            const uint64_t below = (1ull << pos) - 1ull;
-            const uint32_t prev = 63 - __clzll(H & below); // a hit before pos: prev <= 62
-            const uint32_t g = __popcll(V & below & ~((2ull << prev) - 1ull));
-            if (g) {
-                gc += 1;
-                d += (uint32_t)gap_distance(g, k);
-            }
-        }
+    for (int b = 0; b < NB; b += 2) {
+        if (b + 1 < NB)
+            fold.add((uint64_t)V[b + 1] << 32 | V[b], (uint64_t)H[b + 1] << 32 | H[b], lane, k);
+        else
+            fold.add(V[b], H[b], lane, k);
     }
-    b.gaps = __reduce_add_sync(FULL, gc);
-    b.dist = __reduce_add_sync(FULL, d);
-    return b;
-}
-
-// Canonical code of the k-mer whose first base is packed base G, and whether
-// its k bases are all ACGT.
-__device__ __forceinline__ uint64_t canonical_at(const uint64_t *__restrict__ seq,
-                                                 const uint64_t *__restrict__ mask, uint64_t G,
-                                                 uint32_t k, uint64_t kmask, uint64_t kbits,
-                                                 bool &acgt)
-{
-    const uint64_t wi = G >> 5;
-    const uint32_t sh = (uint32_t)(G & 31) * 2;
-    const uint64_t w0 = __ldg(seq + wi), w1 = __ldg(seq + wi + 1);
-    const uint64_t x = (w0 >> sh) | ((w1 << (63 - sh)) << 1); // bases G.. at bits 2t
-    const uint64_t mi = G >> 6;
-    const uint32_t ms = (uint32_t)(G & 63);
-    const uint64_t m0 = __ldg(mask + mi), m1 = __ldg(mask + mi + 1);
-    const uint64_t mm = (m0 >> ms) | ((m1 << (63 - ms)) << 1);
-    acgt = (mm & kbits) == 0;
-    // forward strand: first base in the high bits -> reverse the 2-bit
-    // symbols (bit reversal, then swap the two bits inside each symbol)
-    uint64_t y = __brevll(x);
-    y = ((y >> 1) & 0x5555555555555555ull) | ((y & 0x5555555555555555ull) << 1);
-    const uint64_t fwd = y >> (64 - 2 * k);
-    const uint64_t rc = ~x & kmask; // complement; x already holds the reversed order
-    return fwd < rc ? fwd : rc;
 }
 
 __device__ __forceinline__ uint32_t window_of_span(const uint32_t *__restrict__ span0,
@@ -165,7 +87,7 @@ __global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t 
         const uint32_t nPos = win[w].nPos;
         const uint32_t p0 = (uint32_t)(s - __ldg(span0 + w)) * spanLen;
         const uint32_t p1 = min(p0 + spanLen, nPos);
-        SegStats acc = seg_empty();
+        SpanFold fold;
         for (uint32_t p = p0; p < p1; p += 32 * NB) {
             uint4 v0[NB], v1[NB];
             uint64_t code[NB], fp[NB];
@@ -191,6 +113,7 @@ __global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t 
                     v1[b] = make_uint4(0, 0, 0, 0);
                 }
             }
+            uint32_t V[NB], H[NB];
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
                 bool hit = false;
@@ -198,11 +121,12 @@ __global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t 
                     const uint32_t m = bucket_match<FMT>(v0[b], v1[b], fp[b]);
                     hit = m == 1u || (m == 2u && stash_lookup(t, code[b]));
                 }
-                const uint32_t V = __ballot_sync(FULL, valid[b]);
-                const uint32_t H = __ballot_sync(FULL, hit);
-                acc = seg_combine(acc, block_stats(V, H, lane, (int)k), (int)k);
+                V[b] = __ballot_sync(FULL, valid[b]);
+                H[b] = __ballot_sync(FULL, hit);
             }
+            fold_blocks<NB>(fold, V, H, lane, (int)k);
         }
+        const SegStats acc = dev::span_finish(fold);
         if (lane == 0)
             out[s] = acc;
     }
@@ -288,7 +212,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
         // Lanes past the span read positions up to it (inside the window's
         // bases) and are masked out.
         const uint32_t lastM = nPos - 1 + (w - 1);
-        SegStats acc = seg_empty();
+        SpanFold fold;
         MzPos next = mz_pos(seq, mask, base + min(p0 + lane, lastM), k, m);
         for (uint32_t p = p0; p < p1; p += 32 * NB) {
             MzPos ps[NB + 1];
@@ -353,20 +277,9 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                 V[b] = __ballot_sync(FULL, valid[b]);
                 H[b] = __ballot_sync(FULL, hit);
             }
-            if constexpr (NB % 2 == 0) {
-                // two blocks per fold step: one 64-position summary
-#pragma unroll
-                for (int b = 0; b < NB; b += 2)
-                    acc = seg_combine(acc,
-                                      block_stats64((uint64_t)V[b + 1] << 32 | V[b], (uint64_t)H[b + 1] << 32 | H[b],
-                                                    lane, (int)k),
-                                      (int)k);
-            } else {
-#pragma unroll
-                for (int b = 0; b < NB; ++b)
-                    acc = seg_combine(acc, block_stats(V[b], H[b], lane, (int)k), (int)k);
-            }
+            fold_blocks<NB>(fold, V, H, lane, (int)k);
         }
+        const SegStats acc = dev::span_finish(fold);
         if (lane == 0)
             out[s] = acc;
     }

@@ -44,6 +44,12 @@ __device__ __forceinline__ SegStats block_stats(uint32_t V, uint32_t H, uint32_t
     return b;
 }
 
+// The summary of a warp's span fold; every lane returns the same value.
+__device__ __forceinline__ SegStats span_finish(const SpanFold &f)
+{
+    return f.summary(__reduce_add_sync(FULL_MASK, f.gc), __reduce_add_sync(FULL_MASK, f.d));
+}
+
 // Canonical code of the k-mer whose first base is packed base G, and whether
 // its k bases are all ACGT. Reads two sequence words and two mask words.
 __device__ __forceinline__ uint64_t canonical_at(const uint64_t *__restrict__ seq,

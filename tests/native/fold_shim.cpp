@@ -130,3 +130,31 @@ extern "C" void mz_query(const uint8_t *bases, uint64_t n, uint32_t k, uint64_t 
     delete[] fnc;
     delete[] rnc;
 }
+
+// The scan kernels' running span fold (SpanFold, gpu-ibs_b200/csrc/ibs_core.cuh)
+// with its 32 lanes emulated: positions [0, n) fed in 64-position chunks,
+// each lane's gap sums added up at the end, then the row values as above.
+extern "C" void span_fold(const uint8_t *valid, const uint8_t *hit, uint64_t n, int k, int32_t out[4])
+{
+    SpanFold lanes[32];
+    for (uint64_t a = 0; a < n; a += 64) {
+        uint64_t V = 0, H = 0;
+        for (uint64_t i = a; i < n && i < a + 64; ++i) {
+            V |= (uint64_t)(valid[i] != 0) << (i - a);
+            H |= (uint64_t)(valid[i] && hit[i]) << (i - a);
+        }
+        for (uint32_t lane = 0; lane < 32; ++lane)
+            lanes[lane].add(V, H, lane, k);
+    }
+    uint32_t gaps = 0, dist = 0;
+    for (const SpanFold &f : lanes) {
+        gaps += f.gc;
+        dist += f.d;
+    }
+    WindowRow row{};
+    seg_finish(lanes[0].summary(gaps, dist), k, row);
+    out[0] = row.total_kmers;
+    out[1] = row.observed_kmers;
+    out[2] = row.variations;
+    out[3] = row.kmer_distance;
+}

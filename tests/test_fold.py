@@ -44,3 +44,29 @@ def test_fold_equals_sequential_loop(native_shim, data):
 def test_table_hash_is_a_bijection(native_shim, bits):
     native_shim.hash_collisions.restype = ctypes.c_uint64
     assert native_shim.hash_collisions(ctypes.c_uint32(bits)) == 0
+
+
+def span_fold(shim, valid, hit, k):
+    valid = np.ascontiguousarray(valid, np.uint8)
+    hit = np.ascontiguousarray(hit, np.uint8)
+    out = (ctypes.c_int32 * 4)()
+    shim.span_fold(valid.ctypes.data_as(ctypes.c_void_p), hit.ctypes.data_as(ctypes.c_void_p),
+                   ctypes.c_uint64(len(valid)), ctypes.c_int(k), out)
+    return tuple(out)
+
+
+@settings(max_examples=400, deadline=None)
+@given(st.data())
+def test_span_fold_equals_sequential_loop(native_shim, data):
+    # the scan kernels' running fold over 64-position chunks, its 32 lanes
+    # emulated; runs of hits and misses of every length, invalid positions
+    # anywhere
+    n = data.draw(st.integers(0, 400))
+    k = data.draw(st.sampled_from([4, 15, 25, 31, 32]))
+    p_hit = data.draw(st.sampled_from([0.0, 0.1, 0.5, 0.9, 0.99, 1.0]))
+    p_valid = data.draw(st.sampled_from([1.0, 0.95, 0.5]))
+    seed = data.draw(st.integers(0, 2**32 - 1))
+    rng = np.random.default_rng(seed)
+    valid = rng.random(n) < p_valid
+    hit = valid & (rng.random(n) < p_hit)
+    assert span_fold(native_shim, valid, hit, k) == sequential(valid, hit, k)
