@@ -10,8 +10,11 @@
 // (so of two consecutive headers only the second names the sequence after
 // them). FASTQ text is refused here (its quality lines are read on the host).
 //
-// The host finds the header lines (a '>' at a line start, by memchr) and
-// cuts each record's body into tiles. The device counts the sequence bytes
+// The text is uploaded through the library's pinned staging slots: a few
+// host threads each copy every T-th 16 MiB chunk into one of their two slots
+// and issue its copy to the device on their own stream, and list the header
+// starts (a '>' at a line start) of that chunk on the way. The host cuts each
+// record's body into tiles. The device counts the sequence bytes
 // of every tile; the host turns the counts into contig lengths and each
 // tile's output base offset in the packed layout; the device then moves
 // every tile through shared memory, ranks its sequence bytes with a block
@@ -23,7 +26,9 @@
 #include <cstring>
 #include <functional>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace ibs {
@@ -127,6 +132,82 @@ __global__ void __launch_bounds__(kThreads) k_pack_tiles(const uint8_t *__restri
     }
 }
 
+// Pinned staging for text uploads, per device, kept for the process: each
+// of kWorkers threads owns two slots, a stream and one event per slot.
+constexpr uint32_t kWorkers = 8;
+constexpr uint64_t kChunk = 16ull << 20;
+
+struct Staging {
+    bool ready = false;
+    char *slot[kWorkers][2] = {};
+    cudaStream_t stream[kWorkers] = {};
+    cudaEvent_t free_[kWorkers][2] = {};
+};
+std::mutex g_stagingMu;
+Staging g_staging[16];
+
+// Uploads text[0, n) to dText and returns the header starts in file order:
+// 0 and every '>' that follows a '\n'. The caller holds g_stagingMu and has
+// made `device` current.
+ibs_status upload_text(const char *text, uint64_t n, uint8_t *dText, int device, std::vector<uint64_t> &heads)
+{
+    Staging &sg = g_staging[device];
+    if (!sg.ready) {
+        for (uint32_t t = 0; t < kWorkers; ++t) {
+            IBS_CUDA(cudaStreamCreateWithFlags(&sg.stream[t], cudaStreamNonBlocking), "stream create");
+            for (int i = 0; i < 2; ++i) {
+                IBS_CUDA(cudaMallocHost(&sg.slot[t][i], kChunk), "pinned text staging");
+                IBS_CUDA(cudaEventCreateWithFlags(&sg.free_[t][i], cudaEventDisableTiming), "event create");
+            }
+        }
+        sg.ready = true;
+    }
+    const uint64_t nChunks = (n + kChunk - 1) / kChunk;
+    const uint32_t nWorkers = (uint32_t)std::min<uint64_t>(kWorkers, nChunks);
+    std::vector<std::vector<uint64_t>> found(nChunks);
+    std::vector<cudaError_t> err(nWorkers, cudaSuccess);
+    auto work = [&](uint32_t t) {
+        cudaError_t e = cudaSetDevice(device);
+        for (uint64_t c = t, i = 0; c < nChunks && e == cudaSuccess; c += nWorkers, ++i) {
+            const uint64_t a = c * kChunk, len = std::min(kChunk, n - a);
+            char *slot = sg.slot[t][i & 1];
+            e = cudaEventSynchronize(sg.free_[t][i & 1]); // its previous copy has finished
+            if (e != cudaSuccess)
+                break;
+            std::memcpy(slot, text + a, len);
+            e = cudaMemcpyAsync(dText + a, slot, len, cudaMemcpyHostToDevice, sg.stream[t]);
+            if (e == cudaSuccess)
+                e = cudaEventRecord(sg.free_[t][i & 1], sg.stream[t]);
+            for (uint64_t q = a; q < a + len;) {
+                const char *gt = (const char *)std::memchr(text + q, '>', a + len - q);
+                if (!gt)
+                    break;
+                const uint64_t j = (uint64_t)(gt - text);
+                if (j == 0 || text[j - 1] == '\n')
+                    found[c].push_back(j);
+                q = j + 1;
+            }
+        }
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(sg.stream[t]);
+        err[t] = e;
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < nWorkers; ++t)
+        pool.emplace_back(work, t);
+    if (nWorkers)
+        work(0);
+    for (auto &th : pool)
+        th.join();
+    for (cudaError_t e : err)
+        if (e != cudaSuccess)
+            return cuda_fail(e, "fasta text upload");
+    heads.clear();
+    for (const auto &f : found)
+        heads.insert(heads.end(), f.begin(), f.end());
+    return IBS_OK;
+}
+
 int grid_for_tiles(uint64_t nTiles)
 {
     int dev = 0, sms = 148;
@@ -164,40 +245,6 @@ extern "C" ibs_status ibs_reference_from_fasta(const char *text, uint64_t n, int
         set_error("Unknown file type");
         return IBS_ERR_FORMAT;
     }
-    // header lines: a '>' that starts a line
-    std::vector<std::string> ids;
-    std::vector<uint64_t> bodyStart, bodyEnd;
-    uint64_t pos = 0;
-    while (pos < n) {
-        const char *nl = (const char *)memchr(text + pos, '\n', n - pos);
-        const uint64_t eol = nl ? (uint64_t)(nl - text) : n;
-        if (!bodyStart.empty())
-            bodyEnd.back() = pos; // the previous body runs up to this header
-        ids.emplace_back(text + pos + 1, eol - pos - 1);
-        bodyStart.push_back(eol < n ? eol + 1 : n);
-        bodyEnd.push_back(n);
-        // next header: the next '>' just after a '\n'
-        uint64_t q = bodyStart.back();
-        pos = n;
-        while (q < n) {
-            const char *gt = (const char *)memchr(text + q, '>', n - q);
-            if (!gt)
-                break;
-            const uint64_t i = (uint64_t)(gt - text);
-            if (text[i - 1] == '\n') {
-                pos = i;
-                break;
-            }
-            q = i + 1;
-        }
-    }
-    const uint32_t nBodies = (uint32_t)ids.size();
-    std::vector<Tile> tiles;
-    for (uint32_t b = 0; b < nBodies; ++b)
-        for (uint64_t s = bodyStart[b]; s < bodyEnd[b]; s += kTile)
-            tiles.push_back(Tile{s, (uint32_t)std::min<uint64_t>(kTile, bodyEnd[b] - s), b});
-    const uint64_t nTiles = tiles.size();
-
     DeviceGuard guard(device);
     uint8_t *dText = nullptr;
     Tile *dTiles = nullptr;
@@ -214,7 +261,32 @@ extern "C" ibs_status ibs_reference_from_fasta(const char *text, uint64_t n, int
         ~Guard() { f(); }
     } g{freeAll};
     IBS_CUDA(cudaMalloc(&dText, n), "fasta text alloc");
-    IBS_CUDA(cudaMemcpy(dText, text, n, cudaMemcpyHostToDevice), "fasta text upload");
+    std::vector<uint64_t> heads;
+    {
+        std::lock_guard<std::mutex> lock(g_stagingMu);
+        st = upload_text(text, n, dText, device, heads);
+    }
+    if (st != IBS_OK)
+        return st;
+    // records: the id is the rest of the header line, the body runs from the
+    // next line up to the next header
+    const uint32_t nBodies = (uint32_t)heads.size();
+    std::vector<std::string> ids(nBodies);
+    std::vector<uint64_t> bodyStart(nBodies), bodyEnd(nBodies);
+    for (uint32_t b = 0; b < nBodies; ++b) {
+        const uint64_t h = heads[b];
+        const uint64_t lim = b + 1 < nBodies ? heads[b + 1] : n;
+        const char *nl = (const char *)std::memchr(text + h, '\n', lim - h);
+        const uint64_t eol = nl ? (uint64_t)(nl - text) : lim;
+        ids[b].assign(text + h + 1, eol - h - 1);
+        bodyStart[b] = nl ? eol + 1 : lim;
+        bodyEnd[b] = lim;
+    }
+    std::vector<Tile> tiles;
+    for (uint32_t b = 0; b < nBodies; ++b)
+        for (uint64_t s = bodyStart[b]; s < bodyEnd[b]; s += kTile)
+            tiles.push_back(Tile{s, (uint32_t)std::min<uint64_t>(kTile, bodyEnd[b] - s), b});
+    const uint64_t nTiles = tiles.size();
     IBS_CUDA(cudaMalloc(&dTiles, std::max<uint64_t>(nTiles, 1) * sizeof(Tile)), "fasta tiles alloc");
     IBS_CUDA(cudaMalloc(&dCounts, std::max<uint64_t>(nTiles, 1) * 4), "fasta tiles alloc");
     IBS_CUDA(cudaMalloc(&dTileOut, std::max<uint64_t>(nTiles, 1) * 8), "fasta tiles alloc");
