@@ -98,7 +98,7 @@ static TableGeom choose_geometry(uint64_t nKeys, uint32_t k, const ibs_table_opt
         const uint64_t want = fmt == FMT_MZ8 ? n8 : n6; // sectors at the load
         const uint64_t nLines =
             std::min<uint64_t>(std::max((want + mz::kSectorsPerLine - 1) / mz::kSectorsPerLine, minLines),
-                               1ull << std::min<uint32_t>(2 * m, 40));
+                               1ull << 31); // line_of needs nLines < 2^32
         g.nBuckets = nLines * mz::kSectorsPerLine;
         g.fpBits = 2 * m - floor_log2(nLines);
         g.stashBuckets = 0;

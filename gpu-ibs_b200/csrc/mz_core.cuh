@@ -10,19 +10,19 @@
 // would pile two runs into one place.
 //
 // The table is an array of 128-byte lines of four 32-byte sectors; a sector
-// is a B8x32 bucket (format MZ8) or a B6x40 bucket (format MZ6). The minimizer picks the line and C itself picks one of
-// its four sectors, so a minimizer's k-mers spread over the line and a
-// warp's loads for a run of positions touch one DRAM line.
+// is a B8x32 bucket (format MZ8) or a B6x40 bucket (format MZ6). The
+// minimizer picks the line and C itself picks one of its four sectors, so a
+// minimizer's k-mers spread over the line and a warp's loads for a run of
+// positions touch one DRAM line.
 //
 // The slot value identifies C exactly inside its line: with g = line_hash(M)
-// (a second bijection of the 2m-bit canonical minimizer M, independent of the
-// rank key, whose minimum over w m-mers is biased towards 0), line =
-// floor(g * nLines / 2^2m), so the low hbits = 2m - log2(nLines) bits of g
-// single out g, hence M, among the line's interval; C is then M at offset
-// o (< w <= 8), in orientation s (M or its reverse complement), with the
-// other k - m bases around it:
+// (a bijection of the 2m-bit canonical minimizer M), line = the top 32 bits
+// of g scaled to [0, nLines), so the low hbits = 2m - floor(log2(nLines))
+// bits of g single out g, hence M, among the line's interval; C is then M at
+// offset o (< w <= 8), in orientation s (M or its reverse complement), with
+// the other k - m bases around it:
 //   slot = ((o << 1 | s) << 2(k-m) | C-without-the-m-mer) << hbits | (g mod 2^hbits)
-// which has 2k + 4 - log2(nLines) bits and must fit the sector's slots: 31
+// which has 2k + 4 - floor(log2(nLines)) bits and must fit the sector's slots: 31
 // bits in B8x32 sectors (format MZ8, the sentinels above), nLines >=
 // 2^(2k-27); 40 bits in B6x40 sectors (format MZ6, for k up to 31), nLines
 // >= 2^(2k-36).
@@ -98,15 +98,16 @@ IBS_HD uint64_t mmer_at(uint64_t C, uint32_t k, uint32_t o, uint32_t m)
 
 // (o, s, C without the m-mer) part of the slot value: the minimizer's
 // offset o in C and its orientation s there (1 when it reads as the reverse
-// complement of its canonical form).
-IBS_HD uint64_t slot_high(uint64_t C, uint32_t k, uint32_t o, uint32_t s)
+// complement of its canonical form), then the k - m other bases: C rotated
+// left by 2o bits inside its 2k puts the m-mer on top and below it the bases
+// right of the m-mer followed by the o bases left of it. 2(k - m) + 4 <= 16
+// bits; m >= 16 and o <= k - m keep both shifts below 32.
+IBS_HD uint32_t slot_high(uint64_t C, uint32_t k, uint32_t o, uint32_t s)
 {
     const uint32_t m = m_of(k);
-    const uint32_t rbits = 2 * (k - m - o);                    // bases right of the m-mer
-    const uint64_t right = rbits ? (C & ((1ull << rbits) - 1)) : 0;
-    const uint64_t left = C >> (2 * (k - o));                  // bases left of it (2o bits)
-    const uint64_t rest = (left << rbits) | right;             // 2(k-m) bits
-    return (((uint64_t)o << 1 | s) << (2 * (k - m))) | rest;
+    const uint32_t lo = (uint32_t)C, hi = (uint32_t)(C >> 32);
+    const uint32_t rest = ((lo << (2 * o)) | (hi >> (2 * k - 32 - 2 * o))) & (uint32_t)key_mask(2 * (k - m));
+    return (((o << 1) | s) << (2 * (k - m))) | rest;
 }
 
 // Minimizer offset of C by brute force (table build, single probes): the
@@ -125,19 +126,33 @@ IBS_HD uint32_t minimizer_offset(uint64_t C, uint32_t k)
     return o;
 }
 
-// Sector of C inside its line: two well-mixed bits of the code.
-IBS_HD uint32_t sector_of(uint64_t C) { return (uint32_t)((C * 0x9e3779b97f4a7c15ull) >> 62); }
+// Sector of C inside its line: the top two bits of a golden-ratio multiple
+// of the code's two halves folded together.
+IBS_HD uint32_t sector_of(uint64_t C) { return (((uint32_t)C ^ (uint32_t)(C >> 32)) * 0x9e3779b1u) >> 30; }
+
+// Line of a minimizer with line hash g (2m >= 32 bits) among nLines < 2^32:
+// the top 32 bits of g scaled to [0, nLines). Those of one line form an
+// interval of at most ceil(2^32 / nLines) values, so the g of a line form an
+// interval of at most 2^(2m - floor(log2 nLines)) = 2^hbits values and
+// g mod 2^hbits singles g out in its line.
+IBS_HD uint64_t line_of(uint64_t g, uint32_t m, uint64_t nLines)
+{
+    const uint32_t top = (uint32_t)(g >> (2 * m - 32));
+#if defined(__CUDA_ARCH__)
+    return __umulhi(top, (uint32_t)nLines);
+#else
+    return ((uint64_t)top * (uint32_t)nLines) >> 32;
+#endif
+}
 
 // Bucket (32-byte sector index) and slot value of canonical k-mer C whose
 // minimizer sits at offset o with orientation s and line hash g.
-// hbits = 2m - log2(nLines).
+// hbits = 2m - floor(log2(nLines)).
 IBS_HD void place(uint64_t C, uint32_t k, uint32_t o, uint32_t s, uint64_t g, uint64_t nBuckets,
                   uint32_t hbits, uint64_t &bucket, uint64_t &slot)
 {
-    const uint32_t m = m_of(k);
-    const uint64_t line = mulhi64(g << (64 - 2 * m), nBuckets / kSectorsPerLine);
-    bucket = line * kSectorsPerLine + sector_of(C);
-    slot = (slot_high(C, k, o, s) << hbits) | (g & key_mask(hbits));
+    bucket = line_of(g, m_of(k), nBuckets / kSectorsPerLine) * kSectorsPerLine + sector_of(C);
+    slot = ((uint64_t)slot_high(C, k, o, s) << hbits) | (g & key_mask(hbits));
 }
 
 // Slot value and bucket of a canonical k-mer (the build side, and single
