@@ -174,101 +174,108 @@ struct WindowRow {
     int32_t start, end, total_kmers, observed_kmers, variations, kmer_distance;
 };
 
-IBS_HD uint32_t popc64(uint64_t x)
+// Statistics of up to 32 consecutive positions in 32-bit fields (a block of
+// the scan, or a run of blocks whose counts stay below 2^32): the SegStats
+// monoid without the 64-bit distance.
+struct Seg32 {
+    uint32_t total, obs, lead, trail, gaps, dist;
+};
+
+IBS_HD uint32_t popc32(uint32_t x)
 {
 #if defined(__CUDA_ARCH__)
-    return __popcll(x);
+    return __popc(x);
 #else
-    return (uint32_t)__builtin_popcountll(x);
+    return (uint32_t)__builtin_popcount(x);
 #endif
 }
 
-// Index of the lowest / highest set bit of x != 0.
-IBS_HD uint32_t ctz64(uint64_t x)
+// Index of the lowest set bit of x != 0.
+IBS_HD uint32_t ctz32(uint32_t x)
 {
 #if defined(__CUDA_ARCH__)
-    return __ffsll(x) - 1;
+    return __ffs(x) - 1;
 #else
-    return (uint32_t)__builtin_ctzll(x);
+    return (uint32_t)__builtin_ctz(x);
 #endif
 }
 
-IBS_HD uint32_t clz64(uint64_t x)
+IBS_HD uint32_t clz32(uint32_t x)
 {
 #if defined(__CUDA_ARCH__)
-    return __clzll(x);
+    return __clz(x);
 #else
-    return (uint32_t)__builtin_clzll(x);
+    return (uint32_t)__builtin_clz(x);
 #endif
 }
 
-// Running statistics of one warp's span, fed 64 positions at a time as
-// valid (V) and hit (H) masks (bit i = the i-th position; H a subset of V).
-// The counts, the misses before the span's first hit (lead) and since its
-// last hit (pending) are warp-uniform. Gaps are closed where they end: a gap
-// that ends at a chunk's first hit by every lane alike (lane 0 counts it), a
-// gap inside a chunk by the lane of the hit that ends it. Each lane keeps its
-// own gap sums; the warp adds them up once at the end of the span. Chunks
-// with no valid miss between their first and last hit skip the per-lane
-// search.
-struct SpanFold {
-    uint32_t total = 0, obs = 0, lead = 0, pending = 0;
-    uint32_t gc = 0, d = 0; // this lane's closed gaps and their distance sum
+IBS_HD uint32_t gap_distance32(uint32_t g, int k)
+{
+    const int d = (int)g - (k - 1);
+    return (uint32_t)(d > 0 ? d : (d + 1 < 0 ? -(d + 1) : d + 1));
+}
 
-    IBS_HD void add(uint64_t V, uint64_t H, uint32_t lane, int k)
-    {
-        const uint32_t nV = popc64(V);
-        total += nV;
-        if (H == 0) {
-            if (obs == 0)
-                lead += nV;
-            else
-                pending += nV;
-            return;
-        }
-        const uint32_t first = ctz64(H);
-        const uint32_t last = 63 - clz64(H);
-        const uint32_t c0 = popc64(V & ((1ull << first) - 1ull));
-        if (obs == 0) {
-            lead += c0;
-        } else if (pending + c0 > 0 && lane == 0) {
-            gc += 1;
-            d += (uint32_t)gap_distance(pending + c0, k);
-        }
-        obs += popc64(H);
-        // valid misses strictly between the first and the last hit
-        const uint64_t inner = V & ~H & ~((2ull << first) - 1ull) & ((1ull << last) - 1ull);
-        if (inner) {
-            for (uint32_t half = 0; half < 2; ++half) {
-                const uint32_t pos = lane + 32 * half;
-                if (((H >> pos) & 1ull) && pos != first) {
-                    const uint64_t below = (1ull << pos) - 1ull;
-                    const uint32_t prev = 63 - clz64(H & below); // a hit before pos
-                    const uint32_t g = popc64(V & below & ~((2ull << prev) - 1ull));
-                    if (g) {
-                        gc += 1;
-                        d += (uint32_t)gap_distance(g, k);
-                    }
-                }
-            }
-        }
-        pending = last == 63 ? 0u : popc64(V >> (last + 1));
-    }
-
-    // The span's summary, given the sums of gc and d over the warp's lanes.
-    IBS_HD SegStats summary(uint32_t gaps, uint32_t dist) const
-    {
-        SegStats r;
-        r.pad = 0;
-        r.total = total;
-        r.obs = obs;
-        r.lead = obs ? lead : total;
-        r.trail = obs ? pending : total;
-        r.gaps = gaps;
-        r.dist = dist;
+// Summary of one 32-position block from its valid (V) and hit (H) masks
+// (bit i = position i; H a subset of V). The gaps closed inside the block
+// are walked one by one: from the first remaining valid miss after the first
+// hit to the next hit.
+IBS_HD Seg32 block_seg32(uint32_t V, uint32_t H, int k)
+{
+    Seg32 r;
+    r.total = popc32(V);
+    r.obs = popc32(H);
+    r.gaps = 0;
+    r.dist = 0;
+    if (H == 0) {
+        r.lead = r.trail = r.total;
         return r;
     }
-};
+    const uint32_t first = ctz32(H), last = 31 - clz32(H);
+    r.lead = popc32(V & ((1u << first) - 1u));
+    r.trail = popc32((V >> last) >> 1);
+    // valid misses strictly between the first and the last hit (last > first
+    // whenever there are any, so both shifts stay below 32)
+    uint32_t M = last > first ? V & ~H & ((1u << last) - 1u) & ~((2u << first) - 1u) : 0u;
+    while (M) {
+        const uint32_t a = ctz32(M);                         // a < last
+        const uint32_t nh = ctz32(H & ~((2u << a) - 1u));   // the hit that ends the gap
+        const uint32_t below = (1u << nh) - 1u;
+        const uint32_t g = popc32(M & below);
+        r.gaps += 1;
+        r.dist += gap_distance32(g, k);
+        M &= ~below;
+    }
+    return r;
+}
+
+// a followed by b, without branches: a side without hits has lead == trail
+// == total, and the gap across the boundary closes only between two hits.
+IBS_HD Seg32 seg32_combine(const Seg32 &a, const Seg32 &b, int k)
+{
+    Seg32 r;
+    r.total = a.total + b.total;
+    r.obs = a.obs + b.obs;
+    r.lead = a.obs ? a.lead : a.lead + b.lead;
+    r.trail = b.obs ? b.trail : a.trail + b.trail;
+    const uint32_t g = a.trail + b.lead;
+    const bool close = a.obs && b.obs && g;
+    r.gaps = a.gaps + b.gaps + (close ? 1u : 0u);
+    r.dist = a.dist + b.dist + (close ? gap_distance32(g, k) : 0u);
+    return r;
+}
+
+IBS_HD SegStats seg_of(const Seg32 &s)
+{
+    SegStats r;
+    r.total = s.total;
+    r.obs = s.obs;
+    r.lead = s.lead;
+    r.trail = s.trail;
+    r.gaps = s.gaps;
+    r.pad = 0;
+    r.dist = s.dist;
+    return r;
+}
 
 IBS_HD void seg_finish(const SegStats &s, int k, WindowRow &row)
 {

@@ -38,19 +38,14 @@ const ibs_tuning &tuning() { return g_tune; }
 
 using dev::canonical_at;
 
-// Feeds NB consecutive 32-position blocks' ballots to the span fold, two
-// blocks (64 positions) per step.
+// Feeds NB consecutive 32-position blocks' ballots to the span fold.
 template <int NB>
-__device__ __forceinline__ void fold_blocks(SpanFold &fold, const uint32_t (&V)[NB], const uint32_t (&H)[NB],
+__device__ __forceinline__ void fold_blocks(dev::LaneFold &fold, const uint32_t (&V)[NB], const uint32_t (&H)[NB],
                                             uint32_t lane, int k)
 {
 #pragma unroll
-    for (int b = 0; b < NB; b += 2) {
-        if (b + 1 < NB)
-            fold.add((uint64_t)V[b + 1] << 32 | V[b], (uint64_t)H[b + 1] << 32 | H[b], lane, k);
-        else
-            fold.add(V[b], H[b], lane, k);
-    }
+    for (int b = 0; b < NB; ++b)
+        fold.push(V[b], H[b], lane, k);
 }
 
 __device__ __forceinline__ uint32_t window_of_span(const uint32_t *__restrict__ span0,
@@ -87,7 +82,7 @@ __global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t 
         const uint32_t nPos = win[w].nPos;
         const uint32_t p0 = (uint32_t)(s - __ldg(span0 + w)) * spanLen;
         const uint32_t p1 = min(p0 + spanLen, nPos);
-        SpanFold fold;
+        dev::LaneFold fold;
         for (uint32_t p = p0; p < p1; p += 32 * NB) {
             uint4 v0[NB], v1[NB];
             uint64_t code[NB], fp[NB];
@@ -126,7 +121,7 @@ __global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t 
             }
             fold_blocks<NB>(fold, V, H, lane, (int)k);
         }
-        const SegStats acc = dev::span_finish(fold);
+        const SegStats acc = fold.finish((int)k);
         if (lane == 0)
             out[s] = acc;
     }
@@ -212,7 +207,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
         // Lanes past the span read positions up to it (inside the window's
         // bases) and are masked out.
         const uint32_t lastM = nPos - 1 + (w - 1);
-        SpanFold fold;
+        dev::LaneFold fold;
         MzPos next = mz_pos(seq, mask, base + min(p0 + lane, lastM), k, m);
         for (uint32_t p = p0; p < p1; p += 32 * NB) {
             MzPos ps[NB + 1];
@@ -243,7 +238,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                         // a source lane offers its next-block key exactly when it is
                         // below j -- one shuffle per offset
                         const uint32_t offer = lane < j ? ps[b + 1].key : ps[b].key;
-                        const uint32_t v = __shfl_sync(FULL, offer, (lane + j) & 31);
+                        const uint32_t v = __shfl_sync(FULL, offer, lane + j); // source lane mod 32
                         best = min(best, v ^ j ^ flip);
                     }
                 }
@@ -251,8 +246,8 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                 // the minimizer's line hash and orientation from the lane that
                 // keyed it: position q + jm
                 const uint32_t src = lane + jm;
-                const uint64_t ga = __shfl_sync(FULL, ps[b].gs, src & 31);
-                const uint64_t gc = __shfl_sync(FULL, ps[b + 1].gs, src & 31);
+                const uint64_t ga = __shfl_sync(FULL, ps[b].gs, src);
+                const uint64_t gc = __shfl_sync(FULL, ps[b + 1].gs, src);
                 const uint64_t gs = src < 32 ? ga : gc;
                 const uint32_t sm = isFwd ? (uint32_t)(gs >> 62) & 1u : (uint32_t)(gs >> 63);
                 const uint32_t o = isFwd ? jm : (w - 1 - jm);
@@ -279,7 +274,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
             }
             fold_blocks<NB>(fold, V, H, lane, (int)k);
         }
-        const SegStats acc = dev::span_finish(fold);
+        const SegStats acc = fold.finish((int)k);
         if (lane == 0)
             out[s] = acc;
     }

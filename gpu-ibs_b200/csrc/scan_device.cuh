@@ -44,11 +44,53 @@ __device__ __forceinline__ SegStats block_stats(uint32_t V, uint32_t H, uint32_t
     return b;
 }
 
-// The summary of a warp's span fold; every lane returns the same value.
-__device__ __forceinline__ SegStats span_finish(const SpanFold &f)
-{
-    return f.summary(__reduce_add_sync(FULL_MASK, f.gc), __reduce_add_sync(FULL_MASK, f.d));
-}
+// Window statistics of a warp's span, folded 32 blocks at a time: lane i
+// keeps the valid / hit ballots of the span's blocks i, i + 32, ...; after
+// every 32 blocks (and at the end of the span) each lane summarises its own
+// block with 32-bit operations and a shuffle tree combines the 32 summaries
+// in block order into the running summary. A block costs the keeping lane a
+// compare and two selects.
+struct LaneFold {
+    uint32_t v = 0, h = 0; // this lane's block since the last flush
+    uint32_t n = 0;        // blocks since the last flush (warp-uniform)
+    Seg32 acc{0, 0, 0, 0, 0, 0};
+
+    __device__ __forceinline__ void push(uint32_t V, uint32_t H, uint32_t lane, int k)
+    {
+        if (lane == n) {
+            v = V;
+            h = H;
+        }
+        if (++n == 32)
+            flush(k);
+    }
+
+    __device__ __forceinline__ void flush(int k)
+    {
+        Seg32 s = block_seg32(v, h, k); // lanes past n hold empty blocks
+#pragma unroll
+        for (uint32_t off = 1; off < 32; off <<= 1) {
+            Seg32 o;
+            o.total = __shfl_down_sync(FULL_MASK, s.total, off);
+            o.obs = __shfl_down_sync(FULL_MASK, s.obs, off);
+            o.lead = __shfl_down_sync(FULL_MASK, s.lead, off);
+            o.trail = __shfl_down_sync(FULL_MASK, s.trail, off);
+            o.gaps = __shfl_down_sync(FULL_MASK, s.gaps, off);
+            o.dist = __shfl_down_sync(FULL_MASK, s.dist, off);
+            s = seg32_combine(s, o, k); // right for lanes that are multiples of 2 off
+        }
+        acc = seg32_combine(acc, s, k); // lane 0's is the span so far
+        v = h = n = 0;
+    }
+
+    // The span's summary (lane 0).
+    __device__ __forceinline__ SegStats finish(int k)
+    {
+        if (n)
+            flush(k);
+        return seg_of(acc);
+    }
+};
 
 // Canonical code of the k-mer whose first base is packed base G, and whether
 // its k bases are all ACGT. Reads two sequence words and two mask words.

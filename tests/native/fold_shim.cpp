@@ -131,28 +131,46 @@ extern "C" void mz_query(const uint8_t *bases, uint64_t n, uint32_t k, uint64_t 
     delete[] rnc;
 }
 
-// The scan kernels' running span fold (SpanFold, gpu-ibs_b200/csrc/ibs_core.cuh)
-// with its 32 lanes emulated: positions [0, n) fed in 64-position chunks,
-// each lane's gap sums added up at the end, then the row values as above.
+// The scan kernels' span fold (LaneFold, gpu-ibs_b200/csrc/scan_device.cuh)
+// with its 32 lanes emulated: positions [0, n) in 32-position blocks, lane i
+// keeping block i of every 32; each flush summarises the lanes' blocks
+// (block_seg32) and combines them with the kernel's shuffle tree (lane l
+// takes lane l + off's value, or its own past lane 31); then the row values.
 extern "C" void span_fold(const uint8_t *valid, const uint8_t *hit, uint64_t n, int k, int32_t out[4])
 {
-    SpanFold lanes[32];
-    for (uint64_t a = 0; a < n; a += 64) {
-        uint64_t V = 0, H = 0;
-        for (uint64_t i = a; i < n && i < a + 64; ++i) {
-            V |= (uint64_t)(valid[i] != 0) << (i - a);
-            H |= (uint64_t)(valid[i] && hit[i]) << (i - a);
+    Seg32 acc{0, 0, 0, 0, 0, 0};
+    uint32_t v[32] = {}, h[32] = {}, kept = 0;
+    auto flush = [&]() {
+        Seg32 s[32];
+        for (int l = 0; l < 32; ++l)
+            s[l] = block_seg32(v[l], h[l], k);
+        for (int off = 1; off < 32; off <<= 1) {
+            Seg32 t[32];
+            for (int l = 0; l < 32; ++l)
+                t[l] = seg32_combine(s[l], l + off < 32 ? s[l + off] : s[l], k);
+            for (int l = 0; l < 32; ++l)
+                s[l] = t[l];
         }
-        for (uint32_t lane = 0; lane < 32; ++lane)
-            lanes[lane].add(V, H, lane, k);
+        acc = seg32_combine(acc, s[0], k);
+        for (int l = 0; l < 32; ++l)
+            v[l] = h[l] = 0;
+        kept = 0;
+    };
+    for (uint64_t a = 0; a < n; a += 32) {
+        uint32_t V = 0, H = 0;
+        for (uint64_t i = a; i < n && i < a + 32; ++i) {
+            V |= (uint32_t)(valid[i] != 0) << (i - a);
+            H |= (uint32_t)(valid[i] && hit[i]) << (i - a);
+        }
+        v[kept] = V;
+        h[kept] = H;
+        if (++kept == 32)
+            flush();
     }
-    uint32_t gaps = 0, dist = 0;
-    for (const SpanFold &f : lanes) {
-        gaps += f.gc;
-        dist += f.d;
-    }
+    if (kept)
+        flush();
     WindowRow row{};
-    seg_finish(lanes[0].summary(gaps, dist), k, row);
+    seg_finish(seg_of(acc), k, row);
     out[0] = row.total_kmers;
     out[1] = row.observed_kmers;
     out[2] = row.variations;

@@ -58,10 +58,11 @@ def span_fold(shim, valid, hit, k):
 @settings(max_examples=400, deadline=None)
 @given(st.data())
 def test_span_fold_equals_sequential_loop(native_shim, data):
-    # the scan kernels' running fold over 64-position chunks, its 32 lanes
-    # emulated; runs of hits and misses of every length, invalid positions
-    # anywhere
-    n = data.draw(st.integers(0, 400))
+    # the scan kernels' span fold (32-position blocks kept one per lane,
+    # summaries combined by the shuffle tree), its 32 lanes emulated; runs of
+    # hits and misses of every length, invalid positions anywhere, spans of
+    # several 32-block flushes
+    n = data.draw(st.integers(0, 2600))
     k = data.draw(st.sampled_from([4, 15, 25, 31, 32]))
     p_hit = data.draw(st.sampled_from([0.0, 0.1, 0.5, 0.9, 0.99, 1.0]))
     p_valid = data.draw(st.sampled_from([1.0, 0.95, 0.5]))
