@@ -84,6 +84,12 @@ enum : uint32_t { FMT_B8X32 = 1, FMT_B6X40 = 2, FMT_PANEL = 3, FMT_MZ8 = 4, FMT_
 IBS_HD bool is_mz(uint32_t fmt) { return fmt == FMT_MZ8 || fmt == FMT_MZ6; }
 constexpr uint32_t B8_EMPTY = 0xffffffffu;
 constexpr uint32_t B8_OVERFLOW = 0xfffffffeu;
+// Minimizer lines of B8x32 sectors (MZ8) keep a full sector's extra keys in
+// its partner sector of the same line (index ^ 1) while that has free slots:
+// slot 7 = B8_OVERFLOW says the extras are all there, B8_OVERFLOW_STASH that
+// some went on to the stash. (A slot value identifies its k-mer inside the
+// whole line, so the two sectors' keys never collide.)
+constexpr uint32_t B8_OVERFLOW_STASH = 0xfffffffdu;
 constexpr uint64_t STASH_EMPTY = ~0ull;
 
 struct TableGeom {

@@ -115,15 +115,42 @@ __device__ __forceinline__ uint32_t bucket_match(const uint4 &v0, const uint4 &v
     }
 }
 
+// An MZ8 sector compare: 1 on a hit, 0 on a sure miss, 2 when the sector's
+// extra keys are in its partner sector, 3 when also in the stash.
+__device__ __forceinline__ uint32_t mz8_match(const uint4 &v0, const uint4 &v1, uint32_t slot)
+{
+    const bool hit = (v0.x == slot) | (v0.y == slot) | (v0.z == slot) | (v0.w == slot) | (v1.x == slot) |
+                     (v1.y == slot) | (v1.z == slot) | (v1.w == slot);
+    return hit ? 1u : (v1.w == B8_OVERFLOW ? 2u : (v1.w == B8_OVERFLOW_STASH ? 3u : 0u));
+}
+
+// The rest of an MZ8 probe whose sector r reported m >= 2: the partner
+// sector r ^ 1 of the same line, then (m == 3) the stash.
+__device__ __forceinline__ bool mz8_overflow_lookup(const TableView &t, uint64_t r, uint32_t slot, uint32_t m,
+                                                    uint64_t code)
+{
+    const uint4 w0 = __ldg(t.buckets + 2 * (r ^ 1)), w1 = __ldg(t.buckets + 2 * (r ^ 1) + 1);
+    if ((w0.x == slot) | (w0.y == slot) | (w0.z == slot) | (w0.w == slot) | (w1.x == slot) | (w1.y == slot) |
+        (w1.z == slot) | (w1.w == slot))
+        return true;
+    return m == 3u && stash_lookup(t, code);
+}
+
 template <uint32_t FMT>
 __device__ __forceinline__ bool table_lookup(const TableView &t, uint64_t code)
 {
-    if (FMT == FMT_MZ8 || FMT == FMT_MZ6) {
+    if (FMT == FMT_MZ8) {
         uint64_t r, slot;
         mz::locate(code, t.g, r, slot);
         const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);
-        const uint32_t m = FMT == FMT_MZ8 ? bucket_match<FMT_B8X32>(v0, v1, slot)
-                                          : bucket_match<FMT_B6X40>(v0, v1, slot);
+        const uint32_t m = mz8_match(v0, v1, (uint32_t)slot);
+        return m == 1u || (m >= 2u && mz8_overflow_lookup(t, r, (uint32_t)slot, m, code));
+    }
+    if (FMT == FMT_MZ6) {
+        uint64_t r, slot;
+        mz::locate(code, t.g, r, slot);
+        const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);
+        const uint32_t m = bucket_match<FMT_B6X40>(v0, v1, slot);
         return m == 1u || (m == 2u && stash_lookup(t, code));
     }
     const uint64_t h = perm_hash(code, t.g.bits);

@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(256) k_na_spans(TableView t, const uint64_t *_
         const uint64_t base = cd[c].base + i * ((uint64_t)W - k);
         const uint32_t p0 = (uint32_t)sc * kSpanLen;
         const uint32_t p1 = (uint32_t)(p0 + kSpanLen < nPos ? p0 + kSpanLen : nPos);
-        SegStats acc = seg_empty();
+        dev::LaneFold fold;
         for (uint32_t p = p0; p < p1; p += 32 * NB) {
             uint4 v0[NB], v1[NB];
             uint64_t code[NB], fp[NB];
@@ -201,9 +201,10 @@ __global__ void __launch_bounds__(256) k_na_spans(TableView t, const uint64_t *_
                 }
                 const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
                 const uint32_t H = __ballot_sync(dev::FULL_MASK, hit);
-                acc = seg_combine(acc, dev::block_stats(V, H, lane, (int)k), (int)k);
+                fold.push(V, H, lane, (int)k);
             }
         }
+        const SegStats acc = fold.finish((int)k);
         if (lane == 0)
             out[s] = acc;
     }

@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                 ps[b] = mz_pos(seq, mask, base + min(p + 32 * b + lane, lastM), k, m);
             next = ps[NB];
             uint4 v0[NB], v1[NB];
-            uint64_t slot[NB];
+            uint64_t slot[NB], rb[NB];
             bool valid[NB];
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
                 const uint64_t gs = src < 32 ? ga : gc;
                 const uint32_t sm = isFwd ? (uint32_t)(gs >> 62) & 1u : (uint32_t)(gs >> 63);
                 const uint32_t o = isFwd ? jm : (w - 1 - jm);
-                uint64_t r;
+                uint64_t &r = rb[b];
                 mz::place(ps[b].code, k, o, sm, gs & ((1ull << 62) - 1), t.g.nBuckets, t.g.fpBits, r, slot[b]);
                 if (valid[b]) {
                     v0[b] = __ldg(t.buckets + 2 * r);
@@ -266,8 +266,14 @@ __global__ void __launch_bounds__(512) k_scan_spans_mz(TableView t, const uint64
             for (int b = 0; b < NB; ++b) {
                 bool hit = false;
                 if (valid[b]) {
-                    const uint32_t mt = bucket_match<SEC>(v0[b], v1[b], slot[b]);
-                    hit = mt == 1u || (mt == 2u && stash_lookup(t, ps[b].code));
+                    if constexpr (SEC == FMT_B8X32) {
+                        const uint32_t mt = mz8_match(v0[b], v1[b], (uint32_t)slot[b]);
+                        hit = mt == 1u ||
+                              (mt >= 2u && mz8_overflow_lookup(t, rb[b], (uint32_t)slot[b], mt, ps[b].code));
+                    } else {
+                        const uint32_t mt = bucket_match<SEC>(v0[b], v1[b], slot[b]);
+                        hit = mt == 1u || (mt == 2u && stash_lookup(t, ps[b].code));
+                    }
                 }
                 V[b] = __ballot_sync(FULL, valid[b]);
                 H[b] = __ballot_sync(FULL, hit);

@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) k_serve_single(const TableView *__restric
         const uint64_t kmask = key_mask(2 * k);
         const uint64_t kbits = (1ull << k) - 1;
         const bool b8 = t.g.format == FMT_B8X32;
-        SegStats acc = seg_empty();
+        dev::LaneFold fold;
         for (uint32_t p = it.p0; p < it.p1; p += 32 * NB) {
             uint4 v0[NB], v1[NB];
             uint64_t code[NB], fp[NB];
@@ -118,9 +118,10 @@ __global__ void __launch_bounds__(256) k_serve_single(const TableView *__restric
                 }
                 const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
                 const uint32_t H = __ballot_sync(dev::FULL_MASK, hit);
-                acc = seg_combine(acc, dev::block_stats(V, H, lane, (int)k), (int)k);
+                fold.push(V, H, lane, (int)k);
             }
         }
+        const SegStats acc = fold.finish((int)k);
         if (lane == 0)
             sums[it.out] = acc;
     }

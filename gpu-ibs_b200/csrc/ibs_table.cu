@@ -150,7 +150,7 @@ __global__ void k_mark(uint32_t *__restrict__ cnt, uint64_t nb, TableGeom g,
     for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < nb;
          r += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t c = cnt[r];
-        if (g.format == FMT_B8X32 || g.format == FMT_MZ8) {
+        if (g.format == FMT_B8X32) {
             if (c > 8) {
                 words[r * 8 + 7] = B8_OVERFLOW;
                 local += c - 7;
@@ -170,6 +170,42 @@ __global__ void k_mark(uint32_t *__restrict__ cnt, uint64_t nb, TableGeom g,
         atomicAdd(overflowKeys, local);
 }
 
+// MZ8: marks full sectors pair by pair (sectors 2i and 2i + 1 of a line are
+// partners). A sector with c > 8 keys keeps 7 and sends c - 7 to its
+// partner's free slots (8 - c' when the partner holds c' < 8) and the rest to
+// the stash. Sums the keys leaving their sector (spill) and those reaching
+// the stash, and resets the counters for the placement pass.
+__global__ void k_mark_mz8(uint32_t *__restrict__ cnt, uint64_t nb, uint32_t *__restrict__ words,
+                           unsigned long long *__restrict__ spillKeys, unsigned long long *__restrict__ stashKeys)
+{
+    unsigned long long spill = 0, stash = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; 2 * i < nb;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = 2 * i;
+        const uint32_t c[2] = {cnt[r], cnt[r + 1]};
+        for (int a = 0; a < 2; ++a) {
+            if (c[a] > 8) {
+                const uint32_t extra = c[a] - 7;
+                const uint32_t room = c[a ^ 1] < 8 ? 8 - c[a ^ 1] : 0;
+                words[(r + a) * 8 + 7] = extra > room ? B8_OVERFLOW_STASH : B8_OVERFLOW;
+                spill += extra;
+                stash += extra > room ? extra - room : 0;
+            }
+        }
+        cnt[r] = cnt[r + 1] = 0;
+    }
+    for (int o = 16; o; o >>= 1) {
+        spill += __shfl_xor_sync(0xffffffffu, spill, o);
+        stash += __shfl_xor_sync(0xffffffffu, stash, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (spill)
+            atomicAdd(spillKeys, spill);
+        if (stash)
+            atomicAdd(stashKeys, stash);
+    }
+}
+
 __device__ __forceinline__ bool stash_insert(uint64_t *stash, uint64_t stashBuckets, uint64_t code)
 {
     uint64_t b = stash_home(code, stashBuckets);
@@ -186,9 +222,13 @@ __device__ __forceinline__ bool stash_insert(uint64_t *stash, uint64_t stashBuck
     return false;
 }
 
+// Places every key in its bucket; the extra keys of a full bucket go to the
+// stash, or for MZ8 to the spill list (placed by k_spill_mz8 once every
+// sector holds its own keys).
 __global__ void k_place(const uint64_t *__restrict__ codes, uint64_t n, TableGeom g,
                         uint32_t *__restrict__ cnt, uint32_t *__restrict__ words,
-                        uint64_t *__restrict__ stash, int *__restrict__ err)
+                        uint64_t *__restrict__ stash, uint64_t *__restrict__ spillList,
+                        unsigned long long *__restrict__ spillN, uint64_t spillCap, int *__restrict__ err)
 {
     uint8_t *bytes = reinterpret_cast<uint8_t *>(words);
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
@@ -198,7 +238,19 @@ __global__ void k_place(const uint64_t *__restrict__ codes, uint64_t n, TableGeo
         locate_key(code, g, r, fp);
         const uint32_t s = atomicAdd(cnt + r, 1u);
         bool stashed = false;
-        if (g.format == FMT_B8X32 || g.format == FMT_MZ8) {
+        if (g.format == FMT_MZ8) {
+            const uint32_t w7 = words[r * 8 + 7];
+            const uint32_t limit = (w7 == B8_OVERFLOW || w7 == B8_OVERFLOW_STASH) ? 7u : 8u;
+            if (s < limit) {
+                words[r * 8 + s] = (uint32_t)fp;
+            } else {
+                const unsigned long long j = atomicAdd(spillN, 1ull);
+                if (j < spillCap)
+                    spillList[j] = code;
+                else
+                    atomicExch(err, 1);
+            }
+        } else if (g.format == FMT_B8X32) {
             const uint32_t limit = words[r * 8 + 7] == B8_OVERFLOW ? 7u : 8u;
             if (s < limit)
                 words[r * 8 + s] = (uint32_t)fp;
@@ -212,6 +264,27 @@ __global__ void k_place(const uint64_t *__restrict__ codes, uint64_t n, TableGeo
                 stashed = true;
         }
         if (stashed && !stash_insert(stash, g.stashBuckets, code))
+            atomicExch(err, 1);
+    }
+}
+
+// MZ8 spill pass: each extra key takes the next free slot of its partner
+// sector (after the partner's own keys, all placed by k_place), or the stash
+// once the partner is full. The numbers that land in each place follow from
+// the counts, as k_mark_mz8 recorded them in the sector markers.
+__global__ void k_spill_mz8(const uint64_t *__restrict__ spillList, uint64_t n, TableGeom g,
+                            uint32_t *__restrict__ cnt, uint32_t *__restrict__ words, uint64_t *__restrict__ stash,
+                            int *__restrict__ err)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t code = spillList[i];
+        uint64_t r, fp;
+        locate_key(code, g, r, fp);
+        const uint32_t s = atomicAdd(cnt + (r ^ 1), 1u);
+        if (s < 8)
+            words[(r ^ 1) * 8 + s] = (uint32_t)fp;
+        else if (!stash_insert(stash, g.stashBuckets, code))
             atomicExch(err, 1);
     }
 }
@@ -292,22 +365,24 @@ static ibs_status build_from_device_codes(ibs_table *t, const uint64_t *dCodes, 
     IBS_CUDA(cudaMemset(t->buckets, g.format == FMT_B6X40 || g.format == FMT_MZ6 ? 0x00 : 0xff, nb * 32),
              "table init");
     uint32_t *cnt = nullptr;
-    unsigned long long *dOverflow = nullptr;
+    unsigned long long *dOverflow = nullptr; // [0] keys to the stash, [1] MZ8 spill keys, [2] spill list fill
+    uint64_t *spillList = nullptr;
     int *dErr = nullptr;
     auto cleanup = [&]() {
         cudaFree(cnt);
         cudaFree(dOverflow);
+        cudaFree(spillList);
         cudaFree(dErr);
     };
     cudaError_t e = cudaMalloc(&cnt, nb * 4);
     if (e == cudaSuccess)
-        e = cudaMalloc(&dOverflow, 8);
+        e = cudaMalloc(&dOverflow, 3 * 8);
     if (e == cudaSuccess)
         e = cudaMalloc(&dErr, sizeof(int));
     if (e == cudaSuccess)
         e = cudaMemset(cnt, 0, nb * 4);
     if (e == cudaSuccess)
-        e = cudaMemset(dOverflow, 0, 8);
+        e = cudaMemset(dOverflow, 0, 3 * 8);
     if (e == cudaSuccess)
         e = cudaMemset(dErr, 0, sizeof(int));
     if (e != cudaSuccess) {
@@ -317,14 +392,20 @@ static ibs_status build_from_device_codes(ibs_table *t, const uint64_t *dCodes, 
     uint32_t *words = reinterpret_cast<uint32_t *>(t->buckets);
     k_count<<<grid_for(n, 256), 256>>>(dCodes, n, g, cnt);
     IBS_LAUNCHED();
-    k_mark<<<grid_for(nb, 256), 256>>>(cnt, nb, g, words, dOverflow);
+    if (g.format == FMT_MZ8)
+        k_mark_mz8<<<grid_for(nb / 2, 256), 256>>>(cnt, nb, words, dOverflow + 1, dOverflow);
+    else
+        k_mark<<<grid_for(nb, 256), 256>>>(cnt, nb, g, words, dOverflow);
     IBS_LAUNCHED();
-    unsigned long long overflow = 0;
-    e = cudaMemcpy(&overflow, dOverflow, 8, cudaMemcpyDeviceToHost);
+    unsigned long long counts[2] = {0, 0}; // keys to the stash, MZ8 keys leaving their sector
+    e = cudaMemcpy(counts, dOverflow, 2 * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && counts[1])
+        e = cudaMalloc(&spillList, counts[1] * 8);
     if (e != cudaSuccess) {
         cleanup();
         return cuda_fail(e, "table build count");
     }
+    const unsigned long long overflow = counts[0];
     t->stashKeys = overflow;
     if (overflow) {
         g.stashBuckets = next_pow2((overflow * 2 + 3) / 4);
@@ -337,8 +418,13 @@ static ibs_status build_from_device_codes(ibs_table *t, const uint64_t *dCodes, 
         }
         t->deviceBytes += g.stashBuckets * 32;
     }
-    k_place<<<grid_for(n, 256), 256>>>(dCodes, n, g, cnt, words, t->stash, dErr);
+    k_place<<<grid_for(n, 256), 256>>>(dCodes, n, g, cnt, words, t->stash, spillList, dOverflow + 2, counts[1],
+                                       dErr);
     IBS_LAUNCHED();
+    if (counts[1]) {
+        k_spill_mz8<<<grid_for(counts[1], 256), 256>>>(spillList, counts[1], g, cnt, words, t->stash, dErr);
+        IBS_LAUNCHED();
+    }
     int herr = 0;
     e = cudaMemcpy(&herr, dErr, sizeof(int), cudaMemcpyDeviceToHost);
     cleanup();

@@ -1,6 +1,6 @@
-// Device helpers of the window scan: the 32-position block statistics from
+// Device helpers of the window scans: the span statistics fold over
 // hit/valid ballots and the canonical code of a k-mer read from the 2-bit
-// packed reference. See ibs_scan.cu for the kernel they serve.
+// packed reference. See ibs_scan.cu for the kernels they serve.
 #pragma once
 
 #include "ibs_core.cuh"
@@ -9,40 +9,6 @@ namespace ibs {
 namespace dev {
 
 constexpr uint32_t FULL_MASK = 0xffffffffu;
-
-// Statistics of one 32-position block from its valid (V) and hit (H)
-// ballots (bit i = position p+i; H is a subset of V); every lane returns the
-// same value. The lane of each hit except the first counts the valid misses
-// since the previous hit, so the gaps closed inside the block are found
-// lane-parallel.
-__device__ __forceinline__ SegStats block_stats(uint32_t V, uint32_t H, uint32_t lane, int k)
-{
-    SegStats b;
-    b.pad = 0;
-    b.total = __popc(V);
-    b.obs = __popc(H);
-    if (H == 0) {
-        b.lead = b.trail = b.total;
-        b.gaps = 0;
-        b.dist = 0;
-        return b;
-    }
-    const uint32_t first = __ffs(H) - 1;
-    const uint32_t last = 31 - __clz(H);
-    b.lead = __popc(V & ((1u << first) - 1u));
-    b.trail = last == 31 ? 0u : __popc(V >> (last + 1));
-    uint32_t g = 0;
-    if (((H >> lane) & 1u) && lane != first) {
-        const uint32_t below = (1u << lane) - 1u;
-        const uint32_t prev = 31 - __clz(H & below);
-        g = __popc(V & below & ~((2u << prev) - 1u));
-    }
-    const uint32_t gc = g > 0 ? 1u : 0u;
-    const uint32_t d = g > 0 ? (uint32_t)gap_distance(g, k) : 0u;
-    b.gaps = __reduce_add_sync(FULL_MASK, gc);
-    b.dist = __reduce_add_sync(FULL_MASK, d);
-    return b;
-}
 
 // Window statistics of a warp's span, folded 32 blocks at a time: lane i
 // keeps the valid / hit ballots of the span's blocks i, i + 32, ...; after
