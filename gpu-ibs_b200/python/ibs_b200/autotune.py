@@ -6,6 +6,10 @@ writes the sweep and its best point to gpu-ibs_b200/tuning/<gpu>.json.
 
     python -m ibs_b200.autotune [--scale 0.25] [--out PATH]
 
+The launch shapes cover the region where earlier full sweeps (up to spans
+of 16384, 8 blocks in flight, 128 threads, 4 CTAs per SM) found every
+fastest point.
+
 The workload is plain_2gbp scaled down (default 500 Mbp and ~5.5e8 k-mers:
 tables of several GB, far beyond L2, so a point's timing is DRAM-bound as at
 full size). `apply()` loads a committed result into the library.
@@ -60,11 +64,11 @@ def sweep(scale: float = 0.25, reps: int = 3, quick: bool = False) -> dict:
     stream = torch.cuda.Stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     base = get_tuning()
-    layouts = [(1, 3.0), (4, 3.0)] if quick else [(1, 3.0), (1, 4.0), (4, 2.0), (4, 3.0), (4, 4.0)]
-    shapes = list(itertools.product([2048, 4096, 16384] if not quick else [4096],
-                                    [2, 4] if quick else [1, 2, 4, 8],
-                                    [256, 512] if quick else [128, 256, 512],
-                                    [8, 16] if quick else [4, 8, 16]))
+    layouts = [(1, 3.0), (4, 2.0)] if quick else [(1, 3.0), (1, 4.0), (4, 1.5), (4, 2.0), (4, 3.0)]
+    shapes = list(itertools.product([4096] if quick else [1024, 2048, 4096],
+                                    [2, 4] if quick else [1, 2, 4],
+                                    [256, 512],
+                                    [8, 16]))
     points, reference_rows = [], None
     for fmt, kpb in layouts:
         table = Table.from_codes(codes.data_ptr(), n, k, on_device=True, force_format=fmt, keys_per_bucket=kpb)
