@@ -150,8 +150,10 @@ void ibs_reference_free(ibs_reference *r);
  * and packs as a non-ACGT base; the id is the header line after '>'; a
  * record without sequence is dropped -- with the line-break removal and
  * the packing (packWindow, src/gpu/EncodeProbeCore.hpp:157-186) done on the
- * device. FASTQ text returns IBS_ERR_UNSUPPORTED (pack it with
- * ibs_pack_ascii); text not starting with '>' or '@' IBS_ERR_FORMAT. */
+ * device. The text goes up through the library's pinned staging (8 x 2
+ * slots of 16 MiB per device, allocated by the first call and kept; calls
+ * on one device take turns). FASTQ text returns IBS_ERR_UNSUPPORTED (pack it
+ * with ibs_pack_ascii); text not starting with '>' or '@' IBS_ERR_FORMAT. */
 ibs_status ibs_reference_from_fasta(const char *text, uint64_t n_bytes, int device, ibs_reference **out);
 /* Contigs of a reference: count, and each one's length and id (the id
  * string lives as long as the reference; "" when it was built from arrays). */
