@@ -233,6 +233,10 @@ extern "C" ibs_status ibs_reference_from_fasta(const char *text, uint64_t n, int
     ibs_status st = check_device_ordinal(device);
     if (st != IBS_OK)
         return st;
+    if (device >= 16) {
+        set_error("ibs_reference_from_fasta: device ordinal beyond 15");
+        return IBS_ERR_ARG;
+    }
     if (n == 0) {
         set_error("Empty file");
         return IBS_ERR_FORMAT;
