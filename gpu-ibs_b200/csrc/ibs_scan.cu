@@ -29,10 +29,10 @@ constexpr uint32_t FULL = 0xffffffffu;
 
 static std::mutex g_tuneMu;
 // Defaults: the autotuner's best point on the B200 (gpu-ibs_b200/tuning/b200.json,
-// plain 2 Gbp x 2.19e9 k-mers): minimizer table at 2 keys per 32-byte
+// plain 2 Gbp x 2.19e9 k-mers): minimizer table at 1.5 keys per 32-byte
 // sector, spans of 2048 positions, 2 blocks in flight, 512 threads, 16 CTAs
 // per SM.
-static ibs_tuning g_tune = {2048, 2, 512, 16, 2.0, FMT_MZ8, 0, {0, 0}};
+static ibs_tuning g_tune = {2048, 2, 512, 16, 1.5, FMT_MZ8, 0, {0, 0}};
 
 const ibs_tuning &tuning() { return g_tune; }
 

@@ -58,7 +58,8 @@ typedef struct ibs_reference ibs_reference; /* a device-resident 2-bit packed re
 /* Table build options; zero-initialise for the defaults. */
 typedef struct ibs_table_opts {
     int device;             /* CUDA device ordinal (default 0) */
-    double keys_per_bucket; /* target mean keys per 32 B bucket (0 = default 4.0) */
+    double keys_per_bucket; /* target mean keys per 32 B bucket (0 = ibs_tuning.keys_per_bucket,
+                               or 4.0 for a hash table while the tuned format is minimizer lines) */
     uint32_t force_format;  /* 0 = the tuned default (ibs_tuning.table_format), 1 = B8x32,
                                2 = B6x40, 4 = minimizer lines of B8x32 sectors (16 <= k <= 27),
                                5 = hash buckets, B8x32 or B6x40 by size,
