@@ -897,6 +897,7 @@ struct Workspace {
     ibs_window *dRows = nullptr;
     uint64_t rowsCap = 0;
     uint64_t spansCap = 0;
+    uint64_t winCap = 0; // windows the plan's device arrays hold
     ScanPlan plan;
     cudaStream_t copy = nullptr, comp = nullptr;
     std::vector<cudaEvent_t> ev;
@@ -997,10 +998,6 @@ extern "C" ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit,
     packed_offsets(lens, n, off, seqWords, maskWords);
     std::vector<uint64_t> lv(lens, lens + n);
     ScanPlan &p = ws.plan;
-    cudaFree(p.dWin);
-    cudaFree(p.dSpan0);
-    p.dWin = nullptr;
-    p.dSpan0 = nullptr;
     plan_windows(p, lv, off, W, k, tuning().span_len);
     if (p.nSpans > ws.spansCap || !p.dSpans) {
         cudaFree(p.dSpans);
@@ -1010,8 +1007,16 @@ extern "C" ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit,
                  "span scratch alloc");
         ws.spansCap = std::max<uint64_t>(p.nSpans, 1);
     }
-    IBS_CUDA(cudaMalloc(&p.dWin, std::max<uint64_t>(p.nWin, 1) * sizeof(WinDesc)), "plan alloc");
-    IBS_CUDA(cudaMalloc(&p.dSpan0, (p.nWin + 1) * sizeof(uint32_t)), "plan alloc");
+    if (p.nWin + 1 > ws.winCap || !p.dWin) { // kept across calls; the previous call has finished
+        cudaFree(p.dWin);
+        cudaFree(p.dSpan0);
+        p.dWin = nullptr;
+        p.dSpan0 = nullptr;
+        ws.winCap = 0;
+        IBS_CUDA(cudaMalloc(&p.dWin, (p.nWin + 1) * sizeof(WinDesc)), "plan alloc");
+        IBS_CUDA(cudaMalloc(&p.dSpan0, (p.nWin + 1) * sizeof(uint32_t)), "plan alloc");
+        ws.winCap = p.nWin + 1;
+    }
     ibs_status s = grow(ws.dSeq, ws.seqCap, seqWords, "reference alloc");
     if (s != IBS_OK)
         return s;
@@ -1027,14 +1032,20 @@ extern "C" ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit,
         ws.rowsCap = nWin;
     }
     const bool pinnedIn = is_pinned(seq2bit) && is_pinned(nmask);
-    // window groups of ~16 Mbase (0.5 MB of packed words) .. at most 64 groups
+    // window groups: the first 1/128 of the reference (at least 4 Mbase), so
+    // that the scan starts after a short copy, then each group 1.3x the one
+    // before (a copy of the next group takes no longer than the scan of the
+    // current one: host-to-device bandwidth carries about 1.35x the scan's
+    // bases per second) up to 1/8 of the reference
     const uint64_t totalBases = (seqWords - 1) * 32;
-    const uint64_t groupBases = std::max<uint64_t>(totalBases / 16 + 1, 16ull << 20);
+    const uint64_t maxGroup = std::max<uint64_t>(totalBases / 8 + 1, 16ull << 20);
     std::vector<uint64_t> gWin; // first window of each group
     {
-        uint64_t lastBase = 0;
+        uint64_t lastBase = 0, size = std::max<uint64_t>(totalBases / 128 + 1, 4ull << 20);
         for (uint64_t w = 0; w < p.nWin; ++w)
-            if (gWin.empty() || p.win[w].base >= lastBase + groupBases) {
+            if (gWin.empty() || p.win[w].base >= lastBase + size) {
+                if (!gWin.empty())
+                    size = std::min<uint64_t>(maxGroup, size + size * 3 / 10);
                 gWin.push_back(w);
                 lastBase = p.win[w].base;
             }
