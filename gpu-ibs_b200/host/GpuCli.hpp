@@ -1,6 +1,6 @@
 // The engine options the reference's GPU tools accept (src/GpuCli.hpp:17-71),
 // shared by fastibs and fastibsmapper. Those that steer a part of the
-// reference's engine this build does not have are accepted and ignored;
+// reference's engine this library does not have are accepted and ignored;
 // --cpu / --probe=batched (the reference's CPU paths) warn and run on the
 // GPU, whose results are identical.
 #pragma once
@@ -45,7 +45,7 @@ inline int parse_gpu_flag(const std::string &arg)
         o.enable = 1;
     else if (arg == "--cpu" || arg == "--probe=batched") {
         o.enable = 0;
-        std::cerr << "Warning: " << arg << " selects the reference's CPU path, which this build does "
+        std::cerr << "Warning: " << arg << " selects the reference's CPU path, which this program does "
                   << "not have; running on the GPU (identical results)" << std::endl;
     } else if (arg == "--sync")
         o.sync = true;

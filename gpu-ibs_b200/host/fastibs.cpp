@@ -8,7 +8,7 @@
 // log (log.txt, exit status 1) and panel options (--db, --db-list,
 // --resident). The reference's engine knobs are accepted; those with no
 // meaning for this engine are ignored, and --cpu / --probe=batched (the
-// reference's CPU paths, which this build does not have) say so and scan on
+// reference's CPU paths, which this program does not have) say so and scan on
 // the GPU, whose rows are identical.
 #include <algorithm>
 #include <cerrno>
@@ -80,10 +80,10 @@ void usage(const char *argv0)
          << "  <windowSize>     Length of the sequence window for IBS calculation\n"
          << "                   (integer larger than k, e.g., 50000)\n\n"
          << "Options:\n"
-         << "  --gpu            Scan on the GPU (the only path of this build)\n"
+         << "  --gpu            Scan on the GPU (the only path of this program)\n"
          << "  --device=N       CUDA device ordinal (default 0)\n"
          << "  --cpu, --probe=batched\n"
-         << "                   The reference's CPU paths: not in this build; the scan runs\n"
+         << "                   The reference's CPU paths: not in this program; the scan runs\n"
          << "                   on the GPU with identical rows\n"
          << "  --batch-mb=N --streams=N --sync --sort-queries --probe=bs|hash --hash-lf=F\n"
          << "  --pin-lut --gpus=N|all --no-peer\n"

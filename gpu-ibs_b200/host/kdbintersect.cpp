@@ -90,7 +90,7 @@ int run(int argc, char **argv)
         return 1;
     }
     if (h1.kmerLength > 32) {
-        cerr << "Error: k = " << h1.kmerLength << " is above 32, which this build does not handle" << endl;
+        cerr << "Error: k = " << h1.kmerLength << " is above 32, which this program does not handle" << endl;
         return 1;
     }
     // small (enumerated) = db1, big (probed) = db2 after the reference's rule
