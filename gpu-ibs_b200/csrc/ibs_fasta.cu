@@ -316,6 +316,9 @@ extern "C" ibs_status ibs_reference_from_fasta(const char *text, uint64_t n, int
             lens.push_back(bodyLen[b]);
             keptIds.push_back(std::move(ids[b]));
         }
+    st = check_contig_lengths(lens.data(), (uint32_t)lens.size(), "ibs_reference_from_fasta");
+    if (st != IBS_OK)
+        return st;
     std::vector<uint64_t> off;
     uint64_t sw = 0, mw = 0;
     packed_offsets(lens.data(), (uint32_t)lens.size(), off, sw, mw);

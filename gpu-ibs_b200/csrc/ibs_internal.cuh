@@ -33,6 +33,12 @@ ibs_status cuda_fail(cudaError_t e, const char *what);
 
 // Device count check shared by the entry points.
 ibs_status check_device_ordinal(int dev);
+// Rows carry 32-bit window coordinates (ibs_window.start / end, the
+// reference's int Window::start / end, src/Window.hpp:11-12), so a contig
+// longer than INT32_MAX bases would print wrapped, negative coordinates:
+// IBS_ERR_ARG with a message naming the contig instead.
+ibs_status check_contig_lengths(const uint64_t *lens, uint32_t n, const char *what);
+constexpr uint64_t kMaxContigLen = 2147483647ull;
 // Decodes a KMC 3 database into canonical codes in device memory (caller frees).
 ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodes, uint64_t *n, uint32_t *k);
 // Packed base offset of each contig (roundup64 of the lengths before it) and

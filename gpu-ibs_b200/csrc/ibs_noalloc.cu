@@ -300,16 +300,16 @@ extern "C" ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev
         set_error("ibs_scan_noalloc: device ordinal out of range");
         return IBS_ERR_ARG;
     }
+    ibs_status cs = check_contig_lengths(lens, n_contigs, "ibs_scan_noalloc");
+    if (cs != IBS_OK)
+        return cs;
     uint64_t nWin = 0, nSpans = 0;
     for (uint32_t c = 0; c < n_contigs; ++c) {
         nWin += contig_windows(lens[c], W, k).nWin;
         nSpans += contig_spans(lens[c], W, k);
     }
-    if (nWin > cap || (nWin && !rows_dev)) {
-        set_error("ibs_scan_noalloc: row capacity " + std::to_string(cap) + " < " +
-                  std::to_string(nWin) + " windows");
-        return IBS_ERR_ARG;
-    }
+    // the scratch limit first: a scan beyond it is refused whatever the
+    // caller's buffers hold
     const uint64_t offDesc = align256((uint64_t)n_contigs * 8);
     const uint64_t offSpans = offDesc + align256((uint64_t)n_contigs * sizeof(ContigDesc));
     const uint64_t need = offSpans + nSpans * sizeof(SegStats);
@@ -320,6 +320,11 @@ extern "C" ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev
                   " Mbp of reference in windows of " + std::to_string(W) +
                   "); use ibs_scan_async for larger references");
         return IBS_ERR_CAPACITY;
+    }
+    if (nWin > cap || (nWin && !rows_dev)) {
+        set_error("ibs_scan_noalloc: row capacity " + std::to_string(cap) + " < " +
+                  std::to_string(nWin) + " windows");
+        return IBS_ERR_ARG;
     }
     if (nWin == 0)
         return IBS_OK;

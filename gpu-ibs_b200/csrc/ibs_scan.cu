@@ -600,10 +600,29 @@ extern "C" uint64_t ibs_window_count(const uint64_t *lens, uint32_t n, uint32_t 
     return tot;
 }
 
+ibs_status ibs::check_contig_lengths(const uint64_t *lens, uint32_t n, const char *what)
+{
+    for (uint32_t c = 0; c < n; ++c)
+        if (lens[c] > kMaxContigLen) {
+            set_error(std::string(what) + ": contig " + std::to_string(c) + " has " + std::to_string(lens[c]) +
+                      " bases; window coordinates are 32-bit, so contigs longer than " +
+                      std::to_string(kMaxContigLen) + " bases are not supported");
+            return IBS_ERR_ARG;
+        }
+    return IBS_OK;
+}
+
 extern "C" ibs_status ibs_window_bounds(const uint64_t *lens, uint32_t n, uint32_t W, uint32_t k,
                                         ibs_window *rows, uint64_t cap)
 {
     clear_error();
+    if (n && !lens) {
+        set_error("ibs_window_bounds: bad argument");
+        return IBS_ERR_ARG;
+    }
+    ibs_status cs = check_contig_lengths(lens, n, "ibs_window_bounds");
+    if (cs != IBS_OK)
+        return cs;
     if (W <= k) {
         set_error("window size " + std::to_string(W) + " must be larger than k (" +
                   std::to_string(k) + ")");
@@ -633,6 +652,9 @@ static ibs_status reference_new(const uint64_t *lens, uint32_t n, int device, ib
         return IBS_ERR_ARG;
     }
     *out = nullptr;
+    ibs_status cs = check_contig_lengths(lens, n, "ibs_reference_create");
+    if (cs != IBS_OK)
+        return cs;
     int nd = 0;
     if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0) {
         cudaGetLastError();
@@ -964,6 +986,9 @@ extern "C" ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit,
         set_error("ibs_scan_packed: bad argument");
         return IBS_ERR_ARG;
     }
+    const ibs_status lenStatus = check_contig_lengths(lens, n, "ibs_scan_packed");
+    if (lenStatus != IBS_OK)
+        return lenStatus;
     const uint32_t k = t->geom.k;
     if (W <= k) {
         set_error("window size " + std::to_string(W) + " must be larger than k (" +
@@ -993,6 +1018,11 @@ extern "C" ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit,
         }
         ws.device = t->device;
     }
+    // the workspace's device arrays are rewritten below: wait for any work a
+    // previous call left queued on its streams (a call that failed after
+    // enqueueing returns without waiting)
+    IBS_CUDA(cudaStreamSynchronize(ws.comp), "scan workspace");
+    IBS_CUDA(cudaStreamSynchronize(ws.copy), "scan workspace");
     std::vector<uint64_t> off;
     uint64_t seqWords, maskWords;
     packed_offsets(lens, n, off, seqWords, maskWords);
@@ -1007,7 +1037,7 @@ extern "C" ibs_status ibs_scan_packed(ibs_table *t, const uint64_t *seq2bit,
                  "span scratch alloc");
         ws.spansCap = std::max<uint64_t>(p.nSpans, 1);
     }
-    if (p.nWin + 1 > ws.winCap || !p.dWin) { // kept across calls; the previous call has finished
+    if (p.nWin + 1 > ws.winCap || !p.dWin) { // kept across calls (both streams are idle here)
         cudaFree(p.dWin);
         cudaFree(p.dSpan0);
         p.dWin = nullptr;

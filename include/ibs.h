@@ -183,7 +183,12 @@ void ibs_map_text_free(char *text);
  * ceil(len / (W - k)). 0 when W <= k. */
 uint64_t ibs_window_count(const uint64_t *lens, uint32_t n_contigs, uint32_t W, uint32_t k);
 
-/* Window starts/ends in output order (host arrays of ibs_window_count). */
+/* Window starts/ends in output order (host arrays of ibs_window_count).
+ * Row coordinates are 32-bit, as the reference's Window::start / end are int
+ * (src/Window.hpp:11-12): every call that takes contig lengths (this one,
+ * the reference constructors, ibs_reference_from_fasta, ibs_scan_packed,
+ * ibs_scan_noalloc) returns IBS_ERR_ARG for a contig longer than 2147483647
+ * bases instead of writing wrapped coordinates. */
 ibs_status ibs_window_bounds(const uint64_t *lens, uint32_t n_contigs, uint32_t W, uint32_t k,
                              ibs_window *rows, uint64_t cap);
 
@@ -343,7 +348,13 @@ void ibs_server_close(ibs_server *s);
  * All calls on a device share that array: calls whose work overlaps on the
  * GPU (different streams, or different host threads without ordering) race;
  * order them on one stream. The first call on a device looks up the array's
- * device address; make that first call before any stream capture. */
+ * device address; make that first call before any stream capture.
+ * `lens` is read by an asynchronous host-to-device copy on `stream`: keep it
+ * valid and unchanged until the stream has passed the call (when `lens` is
+ * pinned the copy may run after the call returns), and, if the call was
+ * captured into a CUDA graph, for as long as the graph is replayed (each
+ * replay reads it again). Contigs longer than 2147483647 bases return
+ * IBS_ERR_ARG (window coordinates are 32-bit). */
 #define IBS_NOALLOC_SCRATCH_BYTES (32ull << 20)
 ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev, const uint64_t *nmask_dev,
                             const uint64_t *lens, uint32_t n_contigs, uint32_t W,

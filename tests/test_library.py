@@ -42,6 +42,19 @@ def test_window_count_and_bounds_match_reference_rule():
     assert ib.window_count(lens, 25, 25) == 0
 
 
+def test_contigs_beyond_32_bit_coordinates_are_refused():
+    # rows carry int32 coordinates (the reference's Window::start / end are
+    # int): a contig of 2^31 bases would wrap them, so it is refused; one of
+    # 2^31 - 1 bases still fits
+    edge = np.array([1000, 2**31 - 1], dtype=np.uint64)
+    rows = ib.window_bounds(edge, 50_000, 25)
+    assert rows[-1]["end"] == 2**31 - 1 and rows[-1]["start"] > 0
+    with pytest.raises(ib.IbsError) as e:
+        ib.window_bounds(np.array([1000, 2**31], dtype=np.uint64), 50_000, 25)
+    assert e.value.status == 1  # IBS_ERR_ARG
+    assert "contig 1" in str(e.value) and "32-bit" in str(e.value)
+
+
 def _pack_np(seqs):
     """Independent restatement of the packed layout of include/ibs.h."""
     lens = [len(s) for s in seqs]

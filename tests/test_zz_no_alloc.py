@@ -56,11 +56,11 @@ def test_noalloc_rejects_scans_beyond_its_scratch(build_case):
     tiny = torch.zeros(4, dtype=torch.int64, device="cuda")
     rows = torch.zeros(6, dtype=torch.int32, device="cuda")
     # 20 Gbp of contigs at W=100: far more span summaries than the fixed
-    # scratch holds; refused before any device access
+    # scratch holds; refused on the host before any device access, ahead of
+    # the row-capacity check (the honest capacity of `rows` is one row)
     lens = np.full(10, 2_000_000_000, dtype=np.uint64)
-    n = ib.window_count(lens, 100, 25)
     with pytest.raises(ib.IbsError) as e:
-        ib.scan_noalloc(table, tiny, tiny, lens, 100, rows, n)
+        ib.scan_noalloc(table, tiny, tiny, lens, 100, rows, 1)
     assert e.value.status == 7  # IBS_ERR_CAPACITY
     assert "fixed maximum" in str(e.value)
     table.close()
