@@ -14,9 +14,18 @@ host-buffer C-ABI call ibs_scan_packed (pinned host reference in, rows out,
 copies inside the timed region). With N GPUs every rank scans its own sample
 (weak scaling, no collective on the data path).
 
---impl reference times the reference's own CPU implementation (CPU-BATCHED:
-`fastibs --cpu --probe=batched` built from its sources into oracle/_ref/) on
-bounded slices of the same workload, on all host cores.
+At N=1 the workload is also written as files (the sample's KMC 3 database,
+the whole reference as FASTA; cached in /dev/shm): the table is built from
+the database by ibs_open, the reference's own CPU-BATCHED fastibs (built from
+its sources into oracle/_ref/) scans the whole reference as the CPU baseline,
+the timed rows are compared with its TSV, and this repository's fastibs CLI
+(the drop-in) runs on the same files and its TSV is compared byte for byte
+(`parity`, `e2e_cli`).
+
+--impl reference times the reference's CPU-BATCHED fastibs on all host
+cores, one contig of the same workload per step; --prepare only writes the
+input files (the reference arm runs it as a separate process when they are
+missing).
 """
 from __future__ import annotations
 
@@ -48,24 +57,22 @@ def log(*a):
 # ---------------------------------------------------------------------------
 # workload helpers
 # ---------------------------------------------------------------------------
-def valid_positions(lens, k, runs, lo=None, hi=None) -> int:
-    """k-mer start positions whose k bases are ACGT, per contig from its N
-    runs; optionally only positions in [lo, hi) of contig 0 (a slice)."""
+def valid_positions_by_contig(lens, k, runs) -> list[int]:
+    """Per contig, the k-mer start positions whose k bases are ACGT (from
+    the contig's N runs)."""
     rc, rs, rl = runs
-    total = 0
+    out = []
     for c, L in enumerate(lens):
         L = int(L)
-        a, b = (0, L) if lo is None or c != 0 else (lo, min(hi, L))
-        if lo is not None and c != 0:
-            continue
-        npos = max(0, (b - a) - k + 1)
+        npos = max(0, L - k + 1)
         if npos == 0:
+            out.append(0)
             continue
-        last = a + npos - 1  # last valid start in the slice
+        last = npos - 1  # last valid start
         iv = []
         sel = rc == c
         for s, ln in zip(rs[sel].tolist(), rl[sel].tolist()):
-            x, y = max(a, s - k + 1), min(last, s + ln - 1)
+            x, y = max(0, s - k + 1), min(last, s + ln - 1)
             if x <= y:
                 iv.append((x, y))
         iv.sort()
@@ -79,8 +86,12 @@ def valid_positions(lens, k, runs, lo=None, hi=None) -> int:
                 cur[1] = max(cur[1], y)
         if cur:
             bad += cur[1] - cur[0] + 1
-        total += npos - bad
-    return total
+        out.append(npos - bad)
+    return out
+
+
+def valid_positions(lens, k, runs) -> int:
+    return sum(valid_positions_by_contig(lens, k, runs))
 
 
 def sample_for_rank(w, rank: int):
@@ -168,98 +179,187 @@ def profiled_traffic(workload: str, table_format: int):
 
 
 # ---------------------------------------------------------------------------
-# CPU side: the reference's own binary on bounded slices
+# inputs on disk and the reference's own binary
 # ---------------------------------------------------------------------------
+REF_FASTIBS = REPO / "oracle" / "_ref" / "fastibs"
+OUR_FASTIBS = REPO / "gpu-ibs_b200" / "bin" / "fastibs"
+TSV_DTYPE = [("start", "<i8"), ("end", "<i8"), ("total_kmers", "<i8"), ("observed_kmers", "<i8"),
+             ("variations", "<i8"), ("kmer_distance", "<i8")]
+
+
 def cache_dir(w) -> Path:
     root = Path("/dev/shm") if Path("/dev/shm").is_dir() else Path(tempfile.gettempdir())
     return root / f"ibs_bench_{w.name}"
 
 
-def write_kmc_db(w, dcodes_ptr: int, n: int, d: Path) -> Path:
+def input_paths(w) -> dict:
+    """Where the workload's files live: the sample's KMC 3 database
+    (db/sample.kmc_pre/.kmc_suf), the whole reference as one FASTA
+    (genome/<workload>_genome.fasta) and each contig as its own FASTA
+    (contigs/<contig>_genome.fasta)."""
+    d = cache_dir(w)
+    return {"root": d, "dbdir": d / "db", "prefix": d / "db" / "sample", "db_stamp": d / "db" / "complete",
+            "genome_dir": d / "genome", "genome": d / "genome" / f"{w.name}_genome.fasta",
+            "contig_dir": d / "contigs", "contig_stamp": d / "contigs" / "complete"}
+
+
+def prepare_inputs(w, dcodes_ptr: int, n_codes: int) -> dict:
+    """Writes the workload's input files once (kept across runs in the cache
+    folder): the KMC 3 database of sample 0 from its codes in device memory,
+    the whole-genome FASTA and the per-contig FASTAs. Returns input_paths(w)
+    plus the number of distinct k-mers in the database."""
     import ibs_b200 as ib
-    prefix = d / "db" / "sample"
-    stamp = d / "db" / "complete"
-    if stamp.exists():
-        return prefix
-    (d / "db").mkdir(parents=True, exist_ok=True)
-    t = time.time()
-    written = ib.kmc_write(str(prefix), dcodes_ptr, n, on_device=True, **w.kmc)
-    stamp.write_text(str(written))
-    log(f"[bench] KMC database of {written} k-mers written in {time.time() - t:.1f} s")
-    return prefix
+    p = input_paths(w)
+    if not p["db_stamp"].exists():
+        p["dbdir"].mkdir(parents=True, exist_ok=True)
+        t = time.time()
+        written = ib.kmc_write(str(p["prefix"]), dcodes_ptr, n_codes, on_device=True, **w.kmc)
+        p["db_stamp"].write_text(str(written))
+        log(f"[bench] KMC database of {written} k-mers written in {time.time() - t:.1f} s")
+    if not p["genome"].exists():
+        p["genome_dir"].mkdir(parents=True, exist_ok=True)
+        t = time.time()
+        w.ref.write_fasta(str(p["genome"]) + ".partial")
+        os.replace(str(p["genome"]) + ".partial", p["genome"])
+        log(f"[bench] whole-genome FASTA written in {time.time() - t:.1f} s")
+    if not p["contig_stamp"].exists():
+        p["contig_dir"].mkdir(parents=True, exist_ok=True)
+        text = p["genome"].read_bytes()
+        heads = [0] + [m.start() + 1 for m in re.finditer(rb"\n>", text)]
+        for i, h in enumerate(heads):
+            rec = text[h: heads[i + 1] if i + 1 < len(heads) else len(text)]
+            name = rec[1: rec.index(b"\n")].decode()
+            (p["contig_dir"] / f"{name}_genome.fasta").write_bytes(rec)
+        p["contig_stamp"].write_text(str(len(heads)))
+        del text
+    p["distinct_kmers"] = int(p["db_stamp"].read_text())
+    return p
 
 
-def write_slices(w, d: Path, starts, length: int) -> list[Path]:
-    """FASTA files of slices [s, s+length) of contig 0."""
-    ascii0 = w.ref.contig_ascii(0)
-    out = []
-    for i, s in enumerate(starts):
-        p = d / f"refs_{i}"
-        p.mkdir(parents=True, exist_ok=True)
-        f = p / f"slice{i}_genome.fasta"
-        if not f.exists():
-            seq = ascii0[s:s + length]
-            with open(f, "wb") as fh:
-                fh.write(b">" + w.ref.names[0].encode() + b"\n")
-                for j in range(0, len(seq), 80):
-                    fh.write(seq[j:j + 80] + b"\n")
-        out.append(p)
-    return out
+def prepare_main(args, w) -> int:
+    """bench.py --prepare: generate the workload on the device and write its
+    input files (a separate process, so that the process timing the
+    reference's binary maps none of this repository's libraries)."""
+    import torch
+    import ibs_b200 as ib
+    torch.cuda.set_device(0)
+    sw, mw = w.ref.packed_words()
+    dseq = torch.empty(sw, dtype=torch.int64, device="cuda")
+    dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
+    w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
+    smp = w.samples[0]
+    bound = smp.codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
+    dcodes = torch.empty(bound, dtype=torch.int64, device="cuda")
+    n = smp.codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), dcodes.data_ptr(), bound)
+    torch.cuda.synchronize()
+    p = prepare_inputs(w, dcodes.data_ptr(), n)
+    log(f"[prepare] {w.name}: {p['distinct_kmers']} distinct k-mers; files under {p['root']}")
+    return 0
 
 
-def run_reference_scans(dbdir: Path, refdirs: list[Path], W: int, workdir: Path):
-    """Runs the reference CLI once over a folder holding every slice; returns
-    per-slice 'stats' seconds in slice order."""
-    binp = REPO / "oracle" / "_ref" / "fastibs"
-    allrefs = workdir / "allrefs"
-    shutil.rmtree(allrefs, ignore_errors=True)
-    allrefs.mkdir(parents=True)
-    for rd in refdirs:
-        for f in rd.iterdir():
-            os.symlink(f, allrefs / f.name)
-    out = workdir / "out"
-    shutil.rmtree(out, ignore_errors=True)
-    env = dict(os.environ, FASTIBS_THREADS=str(os.cpu_count()), FASTIBS_CPU_BATCH="16")
-    r = subprocess.run([str(binp), str(dbdir), str(allrefs), str(out), str(W), "--cpu", "--probe=batched"],
+PHASES_RE = re.compile(r"Scan phases: setup ([\d.e+-]+) s, read ([\d.e+-]+) s, window ([\d.e+-]+) s, "
+                       r"stats ([\d.e+-]+) s, write ([\d.e+-]+) s")
+
+
+def run_fastibs(binary: Path, dbdir: Path, refdir: Path, outdir: Path, W: int, extra=(), env=None):
+    """One run of a fastibs CLI (the reference's, or this repository's
+    drop-in) over every reference file in refdir; returns the wall seconds,
+    the per-reference 'Scan phases' (keyed by the reference name the CLI
+    prints) and stdout."""
+    shutil.rmtree(outdir, ignore_errors=True)
+    t0 = time.perf_counter()
+    r = subprocess.run([str(binary), str(dbdir), str(refdir), str(outdir), str(W), *extra],
                        env=env, capture_output=True, text=True)
+    wall = time.perf_counter() - t0
     if r.returncode != 0:
-        raise RuntimeError(f"reference fastibs failed: {r.stderr[-1500:]}")
-    stats = {}
-    cur = None
+        raise RuntimeError(f"{binary.name} failed ({r.returncode}): {r.stdout[-800:]} {r.stderr[-800:]}")
+    phases, cur = {}, None
     for line in r.stdout.splitlines():
-        m = re.match(r"Processing reference: (slice\d+)", line)
+        m = re.match(r"Processing reference: (\S+)", line)
         if m:
             cur = m.group(1)
-        m = re.search(r"Scan phases: setup ([\d.e-]+) s, read ([\d.e-]+) s, window ([\d.e-]+) s, "
-                      r"stats ([\d.e-]+) s", line)
+        m = PHASES_RE.search(line)
         if m and cur:
-            stats[cur] = float(m.group(4))
-    return [stats[f"slice{i}"] for i in range(len(refdirs))], r.stdout
+            phases[cur] = dict(zip(("setup", "read", "window", "stats", "write"), map(float, m.groups())))
+    return wall, phases, r.stdout
 
 
-def cpu_arm(w, runs, steps: int, warmup: int, slice_len: int, dcodes_ptr=None, n_codes=0):
-    """Times the reference CPU-BATCHED scan on steps+warmup slices."""
-    d = cache_dir(w)
-    d.mkdir(parents=True, exist_ok=True)
-    prefix = d / "db" / "sample"
-    if not (d / "db" / "complete").exists():
-        if dcodes_ptr is None:
-            raise RuntimeError("no sample codes to write the KMC database from")
-        write_kmc_db(w, dcodes_ptr, n_codes, d)
-    n = steps + warmup
-    L0 = int(w.ref.lens[0])
-    starts = [(i * slice_len) % max(1, L0 - slice_len) for i in range(n)]
-    refdirs = write_slices(w, d, starts, slice_len)
-    secs, _ = run_reference_scans(prefix.parent, refdirs, w.window, d / "run")
-    probes = [valid_positions(w.ref.lens, w.k, runs, s, s + slice_len) for s in starts]
-    timed = list(range(warmup, n))
-    value = sum(probes[i] for i in timed) / sum(secs[i] for i in timed)
-    return value, secs, probes
+def reference_env(threads: int) -> dict:
+    return dict(os.environ, FASTIBS_THREADS=str(threads), FASTIBS_CPU_BATCH="16")
+
+
+def tsv_rows(path: Path):
+    """(seqname column, numeric rows) of a fastibs TSV."""
+    lines = path.read_bytes().split(b"\n")
+    assert lines[0] == b"seqname\tstart\tend\ttotal_kmers\tobserved_kmers\tvariations\tkmer_distance"
+    body = [ln.split(b"\t") for ln in lines[1:] if ln]
+    names = [f[0] for f in body]
+    nums = np.array([tuple(int(x) for x in f[1:]) for f in body], dtype=TSV_DTYPE)
+    return names, nums
+
+
+def rows_equal_tsv(rows, nums) -> bool:
+    if len(rows) != len(nums):
+        return False
+    return all(np.array_equal(rows[f].astype(np.int64), nums[f]) for f in rows.dtype.names)
+
+
+def sha256_file(path: Path) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for b in iter(lambda: f.read(1 << 24), b""):
+            h.update(b)
+    return h.hexdigest()
 
 
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def reference_cpu_run(w, p: dict, threads: int) -> dict:
+    """The reference's CPU-BATCHED fastibs over the whole reference (one
+    FASTA of every contig) against the sample's KMC database: its TSV and its
+    own phase timings."""
+    out = p["root"] / "ref_out"
+    wall, phases, _ = run_fastibs(REF_FASTIBS, p["dbdir"], p["genome_dir"], out, w.window,
+                                  ("--cpu", "--probe=batched"), env=reference_env(threads))
+    tsv = out / f"db_v_{w.name}_{w.window}.tsv"
+    return {"wall_s": wall, "phases": phases[w.name], "tsv": tsv}
+
+
+def reference_check(w, tag: str, sample: int, contig: int, dcodes_ptr: int, n_codes: int, rows) -> dict:
+    """Rows of one sample over one contig against the reference's own
+    CPU-BATCHED fastibs on the same inputs: the sample's KMC database and the
+    contig's FASTA are written (cached), the reference scans the contig, and
+    its TSV is compared with `rows` (that contig's rows of the sample)."""
+    import ibs_b200 as ib
+    d = cache_dir(w) / f"check_{tag}_s{sample}_c{contig}"
+    (d / "db").mkdir(parents=True, exist_ok=True)
+    (d / "refs").mkdir(parents=True, exist_ok=True)
+    stamp = d / "db" / "complete"
+    if not stamp.exists():
+        stamp.write_text(str(ib.kmc_write(str(d / "db" / "sample"), dcodes_ptr, n_codes, on_device=True,
+                                          **w.kmc)))
+    name = w.ref.names[contig]
+    fa = d / "refs" / f"{name}_genome.fasta"
+    if not fa.exists():
+        seq = w.ref.contig_ascii(contig)
+        with open(str(fa) + ".partial", "wb") as fh:
+            fh.write(b">" + name.encode() + b"\n")
+            for j in range(0, len(seq), 80):
+                fh.write(seq[j:j + 80] + b"\n")
+        os.replace(str(fa) + ".partial", fa)
+    threads = os.cpu_count() or 1
+    wall, phases, _ = run_fastibs(REF_FASTIBS, d / "db", d / "refs", d / "out", w.window,
+                                  ("--cpu", "--probe=batched"), env=reference_env(threads))
+    _, nums = tsv_rows(d / "out" / f"db_v_{name}_{w.window}.tsv")
+    equal = rows_equal_tsv(rows, nums)
+    return {"status": "bit-exact" if equal else "MISMATCH", "sample": sample, "contig": name,
+            "sample_kmers": int(stamp.read_text()), "windows": int(len(nums)),
+            "against": "oracle/_ref/fastibs --cpu --probe=batched on this sample's KMC database and this "
+                       "contig's FASTA", "reference_wall_s": wall}
+
+
 def gpu_arm(args, w, rank: int, world: int, local: int):
     import torch
     import ibs_b200 as ib
@@ -272,6 +372,7 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
     probes_per_scan = valid_positions(lens, k, runs)
     sw, mw = w.ref.packed_words()
     n_win = ib.window_count(lens, W, k)
+    files = rank == 0 and world == 1  # the KMC database, FASTA files, CPU baseline and parity
 
     # random-sector ceiling of this GPU (before the big allocations)
     sector_rate = ib.random_sector_rate(16 << 30) if args.scale >= 0.5 else ib.random_sector_rate(4 << 30)
@@ -287,31 +388,52 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
     n_codes = smp.codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), dcodes.data_ptr(), bound)
     torch.cuda.synchronize()
     t_gen = time.time() - t0
+
+    # the sample's table: rank 0 of a 1-GPU run decodes the KMC database the
+    # reference reads (ibs_open: the .kmc_suf records decoded on the device);
+    # the other ranks of a multi-GPU run build theirs from their own codes
+    paths = None
+    if files:
+        paths = prepare_inputs(w, dcodes.data_ptr(), n_codes)
+    del dcodes
+    torch.cuda.empty_cache()
     t0 = time.time()
-    table = ib.Table.from_codes(dcodes.data_ptr(), n_codes, k, on_device=True, device=dev,
-                                force_format=args.table_format, keys_per_bucket=args.keys_per_bucket)
+    if files:
+        table = ib.Table.open(str(paths["prefix"]), device=dev, force_format=args.table_format,
+                              keys_per_bucket=args.keys_per_bucket)
+    else:
+        dcodes = torch.empty(bound, dtype=torch.int64, device="cuda")
+        n_codes = smp.codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), dcodes.data_ptr(), bound)
+        table = ib.Table.from_codes(dcodes.data_ptr(), n_codes, k, on_device=True, device=dev,
+                                    force_format=args.table_format, keys_per_bucket=args.keys_per_bucket)
+        del dcodes
+        torch.cuda.empty_cache()
     info = table.info()
     t_build = time.time() - t0
-    log(f"[bench r{rank}] generated {sum(map(int, lens)) / 1e9:.3f} Gbp + {n_codes / 1e9:.3f}e9 k-mers "
-        f"in {t_gen:.1f} s; table {info.n_buckets * 32 / 1e9:.2f} GB (format {info.format}, "
-        f"{info.stash_keys} stashed) in {t_build:.1f} s")
+    build_call = "ibs_open (KMC 3 files decoded on the device)" if files else "ibs_table_from_codes"
+    log(f"[bench r{rank}] generated {sum(map(int, lens)) / 1e9:.3f} Gbp + {n_codes / 1e9:.3f}e9 codes "
+        f"in {t_gen:.1f} s; table of {info.n_keys} k-mers, {info.n_buckets * 32 / 1e9:.2f} GB (format "
+        f"{info.format}, {info.stash_keys} stashed) by {build_call} in {t_build:.1f} s")
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    # the reference's own CPU-BATCHED scan of the whole reference (its TSV is
+    # the parity target of the rows timed below)
+    cpu, ref_run = None, None
+    if files and not args.no_cpu_baseline:
         try:
-            value, secs, probes = cpu_arm(w, runs, steps=args.cpu_steps, warmup=1,
-                                          slice_len=args.cpu_slice, dcodes_ptr=dcodes.data_ptr(),
-                                          n_codes=n_codes)
-            cpu = {"value": value, "unit": "probes/s", "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"{args.cpu_steps} slices of {args.cpu_slice / 1e6:g} Mbp of {w.ref.names[0]} "
-                             f"(+1 warm-up) against the full {n_codes / 1e9:.2f}e9-k-mer sample database; "
-                             f"fastibs --cpu --probe=batched, FASTIBS_THREADS={os.cpu_count()}, "
-                             f"'stats' phase seconds {', '.join(f'{s:.2f}' for s in secs[1:])}"}
+            threads = os.cpu_count() or 1
+            ref_run = reference_cpu_run(w, paths, threads)
+            ph = ref_run["phases"]
+            cpu = {"value": probes_per_scan / ph["stats"], "unit": "probes/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": f"the whole {w.name} workload ({sum(map(int, lens)) / 1e9:g} Gbp in {len(lens)} "
+                             f"contigs) against the {paths['distinct_kmers'] / 1e9:.3f}e9-k-mer KMC database: "
+                             f"oracle/_ref/fastibs --cpu --probe=batched (CPU-BATCHED), FASTIBS_THREADS={threads}; "
+                             f"probes/s = valid positions / the 'stats' phase of its Scan phases line",
+                   "phases_s": ph, "wall_s": ref_run["wall_s"]}
+            log(f"[bench] reference CPU-BATCHED scan: {ph} (wall {ref_run['wall_s']:.1f} s)")
         except Exception as e:  # the baseline is reported, not required
             cpu = {"value": None, "unit": "probes/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {e}"}
-    del dcodes
-    torch.cuda.empty_cache()
 
     ref = ib.Reference(dseq.data_ptr(), dmask.data_ptr(), lens, device=dev, on_device=True)
     rows_dev = torch.empty(max(n_win, 1) * 6, dtype=torch.int32, device="cuda")
@@ -369,13 +491,8 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
     # from FASTA text in host memory: parse + pack on the device, scan, rows
     # back (the fastibs CLI's path for a plain .fasta reference)
     fasta = None
-    if world == 1 and not args.no_fasta_e2e:
-        fpath = cache_dir(w) / "reference.fasta"
-        fpath.parent.mkdir(parents=True, exist_ok=True)
-        if not fpath.exists():
-            w.ref.write_fasta(str(fpath) + ".partial")
-            os.replace(str(fpath) + ".partial", fpath)
-        text = fpath.read_bytes()
+    if files and not args.no_fasta_e2e:
+        text = paths["genome"].read_bytes()
         secs, parse = [], []
         for it in range(3):
             torch.cuda.synchronize()
@@ -393,6 +510,40 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
                  "fasta_bytes": len(text), "h2d_bytes_per_step": len(text), "d2h_bytes_per_step": int(d2h),
                  "call": "ibs_reference_from_fasta (FASTA bytes in host memory) + ibs_scan (rows to host)"}
         del text
+    table_info = {"format": int(info.format), "buckets": int(info.n_buckets), "keys": int(info.n_keys),
+                  "fp_bits": int(info.fp_bits), "stash_keys": int(info.stash_keys),
+                  "device_gb": info.device_bytes / 1e9, "build_s": t_build, "build_call": build_call}
+    table.close()
+    ref.free()
+    del rows_dev, hseq, hmask, hrows
+    torch.cuda.empty_cache()
+
+    # parity at full size: the timed scan's rows against the reference's own
+    # TSV, and this repository's fastibs CLI (the drop-in: KMC files and FASTA
+    # in, TSV out) byte for byte against it
+    parity, cli = None, None
+    if ref_run is not None:
+        names, nums = tsv_rows(ref_run["tsv"])
+        timed_equal = rows_equal_tsv(rows, nums)
+        try:
+            wall, phases, _ = run_fastibs(OUR_FASTIBS, paths["dbdir"], paths["genome_dir"],
+                                          paths["root"] / "our_out", W)
+            our_tsv = paths["root"] / "our_out" / ref_run["tsv"].name
+            cli_identical = our_tsv.read_bytes() == ref_run["tsv"].read_bytes()
+            cli = {"value": total_probes / wall, "unit": "probes/s", "seconds": wall,
+                   "phases_s": phases.get(w.name),
+                   "call": "gpu-ibs_b200/bin/fastibs <db> <refs> <out> 50000: KMC 3 files and the FASTA file "
+                           "in, TSV out (process start to exit)",
+                   "reference_seconds": ref_run["wall_s"]}
+        except Exception as e:
+            cli_identical = False
+            cli = {"value": None, "unavailable": str(e)[-400:]}
+        parity = {"status": "bit-exact" if timed_equal and cli_identical else "MISMATCH",
+                  "against": "the reference's fastibs --cpu --probe=batched TSV of the whole workload",
+                  "windows": int(len(nums)), "timed_rows_equal_reference_tsv": bool(timed_equal),
+                  "cli_tsv_identical_to_reference_tsv": bool(cli_identical),
+                  "tsv_sha256": sha256_file(ref_run["tsv"])}
+        log(f"[bench] parity {parity}")
 
     peak, peak_kind = measured_peaks()
     achieved = probes_per_scan / (ms_step * 1e-3) * BYTES_PER_PROBE / 1e9
@@ -403,10 +554,11 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
         "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic (seeded generator; stands in for plant-genome inputs not available here)",
         "config": {"workload": w.name, "reference_bp": int(sum(map(int, lens))), "contigs": len(lens),
-                   "sample_kmers": int(n_codes), "k": k, "window": W, "windows": int(n_win),
+                   "sample_kmers": int(info.n_keys), "k": k, "window": W, "windows": int(n_win),
                    "probes_per_scan": int(probes_per_scan), "parallelism": f"{world} sample(s), one per GPU",
                    "l2": f"inputs larger than L2: {info.n_buckets * 32 / 1e9:.1f} GB table, "
                          f"{(sw + mw) * 8 / 1e9:.2f} GB packed reference"},
+        "parity": parity,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": profiled_traffic(w.name, int(info.format)),
@@ -422,19 +574,16 @@ def gpu_arm(args, w, rank: int, world: int, local: int):
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3,
                 "call": "ibs_scan_packed (pinned host 2-bit reference -> host rows)"},
         "e2e_from_fasta": fasta,
+        "e2e_cli": cli,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "extra": {"gbp_x_samples_per_s": sum(map(int, lens)) * world / (ms_step * 1e-3) / 1e9,
-                  "table": {"format": int(info.format), "buckets": int(info.n_buckets),
-                            "fp_bits": int(info.fp_bits), "stash_keys": int(info.stash_keys),
-                            "device_gb": info.device_bytes / 1e9, "build_s": t_build},
+                  "table": table_info, "generator_codes": int(n_codes),
                   "rows_checksum_observed": checksum, "gen_s": t_gen,
                   "tuning": getattr(args, "tuning_used", None)},
     }
     if cpu is not None:
         out["cpu_baseline"] = cpu
-    table.close()
-    ref.free()
     return out
 
 
@@ -567,6 +716,18 @@ def panel_arm(args, rank: int):
     ns = len(w.samples)
     mismatched = [i for i in range(ns) if not np.array_equal(got[i], singles[i])]
     assert not mismatched, f"panel rows differ from single-sample rows for samples {mismatched}"
+    # the smallest sample's rows over the shortest contig against the
+    # reference's own CPU scan of the same inputs
+    win_start = np.concatenate([[0], np.cumsum([ib.window_count(lens[c:c + 1], W, k) for c in range(len(lens))])])
+    si = int(np.argmin(sizes))
+    ci = int(np.argmin([int(x) for x in lens]))
+    ref_check = None
+    if REF_FASTIBS.exists() and not args.no_cpu_baseline:
+        buf, n = sample_codes(si)
+        ref_check = reference_check(w, "panel", si, ci, buf.data_ptr(), n,
+                                    got[si][int(win_start[ci]):int(win_start[ci + 1])])
+        del buf
+        torch.cuda.empty_cache()
     probes = positions * ns
     out = {"workload": w.name, "samples": ns, "sample_kmers": sizes, "k": k, "window": W,
            "reference_bp": int(sum(map(int, lens))), "positions": int(positions),
@@ -576,6 +737,10 @@ def panel_arm(args, rank: int):
            "plain_probes_per_s": probes / (plain_ms * 1e-3), "plain_ms_all_samples": plain_ms,
            "speedup_vs_plain": plain_ms / panel_ms, "graph_launches_per_scan": launches / args.steps,
            "rows_equal_single_sample": True,
+           "parity": {"status": "bit-exact" if ref_check is None or ref_check["status"] == "bit-exact"
+                      else "MISMATCH",
+                      "single_sample": "every sample's panel rows equal its single-sample scan's rows",
+                      "reference": ref_check},
            "note": "batched = joint tables (one per group; one group when all samples fit), each scan a "
                    "replayed CUDA graph; plain = one table and one scan launch per sample; scan time only"}
     ref.free()
@@ -635,6 +800,17 @@ def served_arm(args, rank: int):
         t.close()
     del rows_dev
     torch.cuda.empty_cache()
+    # the full-scan rows every served row is checked against: one sample's
+    # over one contig against the reference's own CPU scan
+    si = int(np.argmin(n_keys))
+    ci = int(np.argmin([int(x) for x in lens]))
+    ref_check = None
+    if REF_FASTIBS.exists() and not args.no_cpu_baseline:
+        buf, n = codes(si)
+        ref_check = reference_check(w, "served", si, ci, buf.data_ptr(), n,
+                                    full[si][int(win_start[ci]):int(win_start[ci + 1])])
+        del buf
+        torch.cuda.empty_cache()
     setup_s = time.time() - t0
 
     # the request stream
@@ -651,27 +827,33 @@ def served_arm(args, rank: int):
         first = min(first, nw_c - 1)
         cnt = max(1, min(nw_c - first, ln // step))
         reqs.append((s_, c, first, cnt))
-    gaps = rng.exponential(1.0 / args.serve_rate, len(reqs))
+    unit_gaps = rng.exponential(1.0, len(reqs))  # arrival gaps at 1 req/s, scaled per rate
+    rates = [float(x) for x in str(args.serve_rates).split(",") if x]
 
-    def run(srv, paced: bool):
+    def run(srv, rate):
+        """rate = None: every request submitted at once (saturated); else
+        Poisson arrivals at `rate` per second of the first requests (all of
+        them at the highest rate, about args.serve_seconds worth below it)."""
         done = []
         stats0 = srv.stats()
         t_start = srv.now()
-        if paced:
+        if rate:
+            n = len(reqs) if rate == max(rates) else min(len(reqs), max(50, int(rate * args.serve_seconds)))
             t_next = time.perf_counter()
-            for req, g in zip(reqs, gaps):
+            for req, g in zip(reqs[:n], unit_gaps[:n] / rate):
                 t_next += g
                 while time.perf_counter() < t_next:
                     done += srv.poll(256, timeout_ms=0)
                     time.sleep(0.0002)
                 srv.submit(*req)
         else:
+            n = len(reqs)
             for req in reqs:
                 srv.submit(*req)
         deadline = time.time() + 1800
-        while len(done) < len(reqs) and time.time() < deadline:
+        while len(done) < n and time.time() < deadline:
             done += srv.poll(256, timeout_ms=1000)
-        assert len(done) == len(reqs), f"served requests unfinished: {srv.stats()}"
+        assert len(done) == n, f"served requests unfinished: {srv.stats()}"
         makespan = srv.now() - t_start
         st = srv.stats()
         lat = np.array([r["done_time"] - r["submit_time"] for r in done])
@@ -681,21 +863,26 @@ def served_arm(args, rank: int):
             assert np.array_equal(r["rows"], full[r["sample"]][a:a + int(r["n_windows"])]), "served rows differ"
         probes = st["probes"] - stats0["probes"]
         busy = st["busy_seconds"] - stats0["busy_seconds"]
-        return {"requests": len(done), "probes": int(probes), "scanned": int(st["scanned"] - stats0["scanned"]),
+        sp = st["sample_probes"] - stats0["sample_probes"]
+        return {"requests": n, "arrival_rate_per_s": rate, "probes": int(probes),
+                "scanned": int(st["scanned"] - stats0["scanned"]), "sample_probes_computed": int(sp),
                 "makespan_s": makespan, "probes_per_s": probes / makespan,
                 "device_busy_s": busy, "probes_per_device_s": probes / max(busy, 1e-9),
+                "sample_probes_per_device_s": sp / max(busy, 1e-9),
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
                 "latency_max_s": float(lat.max()), "launches": int(st["launches"] - stats0["launches"]),
                 "reloads": int(st["reloads"] - stats0["reloads"]),
-                "reload_bytes": int(st["reload_bytes"] - stats0["reload_bytes"])}
+                "reload_bytes": int(st["reload_bytes"] - stats0["reload_bytes"]),
+                "rows_equal_full_scan": True}
 
     out = {"workload": f"{w.name} reference x {n_samples} resident samples", "k": k, "window": W,
            "reference_bp": int(sum(map(int, lens))), "sample_kmers": n_keys, "requests": len(reqs),
-           "arrival_rate_per_s": args.serve_rate, "region": "log-uniform 1 Mbp .. whole contig",
+           "arrival_rates_per_s": rates, "region": "log-uniform 1 Mbp .. whole contig",
            "setup_s": setup_s}
 
-    # plain path: per-sample tables, one request per launch. The budget
-    # leaves room for registering a sample (its codes and a transient table)
+    # plain path: per-sample tables in the plain scan's layout (minimizer
+    # lines at the tuned load), one request per launch. The budget leaves
+    # room for registering a sample (its codes and a transient table)
     free, _ = torch.cuda.mem_get_info()
     transient = max_bound * 8 + ib.table_bytes_for(max(n_keys), k) * 2 + (4 << 30)
     srv = ib.Server(ref, W, k, memory_budget=int(free - transient), one_request_per_launch=True)
@@ -705,8 +892,9 @@ def served_arm(args, rank: int):
         del buf
         torch.cuda.empty_cache()
     out["plain_tables_gb"] = srv.stats()["resident_bytes"] / 1e9
-    out["plain_poisson"] = run(srv, True)
-    out["plain_saturated"] = run(srv, False)
+    for r in rates:
+        out[f"plain_poisson_{r:g}"] = run(srv, r)
+    out["plain_saturated"] = run(srv, None)
     srv.close()
     torch.cuda.empty_cache()
 
@@ -745,14 +933,22 @@ def served_arm(args, rank: int):
     assert all(id_of[i] == i for i in range(n_samples))
     out["batched_groups"] = groups
     out["batched_tables_gb"] = srv.stats()["resident_bytes"] / 1e9
-    out["batched_poisson"] = run(srv, True)
-    out["batched_saturated"] = run(srv, False)
+    for r in rates:
+        out[f"batched_poisson_{r:g}"] = run(srv, r)
+    out["batched_saturated"] = run(srv, None)
     srv.close()
     out["saturated_speedup_vs_plain"] = (out["batched_saturated"]["probes_per_s"] /
                                          out["plain_saturated"]["probes_per_s"])
-    out["rows_equal_full_scan"] = True
+    out["p99_ratio_batched_over_plain"] = {f"{r:g}": out[f"batched_poisson_{r:g}"]["latency_p99_s"] /
+                                           out[f"plain_poisson_{r:g}"]["latency_p99_s"] for r in rates}
+    out["parity"] = {"status": "bit-exact" if ref_check is None or ref_check["status"] == "bit-exact"
+                     else "MISMATCH",
+                     "single_sample": "every served row equals the same window of its sample's full "
+                                      "single-sample scan",
+                     "reference": ref_check}
     out["note"] = ("probes = positions of the completed requests (a window shared by k requests counts k "
-                   "times); scanned = positions the device scanned")
+                   "times); scanned = positions the device scanned; sample_probes_computed = positions x "
+                   "samples the scans answered")
     ref.free()
     return out
 
@@ -803,6 +999,16 @@ def admitted_arm(args, rank: int):
         t.close()
     del rows_dev
     torch.cuda.empty_cache()
+    # one sample over one contig against the reference's own CPU scan
+    si = int(np.argmin(n_keys))
+    ci = int(np.argmin([int(x) for x in lens]))
+    ref_check = None
+    if REF_FASTIBS.exists() and not args.no_cpu_baseline:
+        buf, n = codes(si)
+        ref_check = reference_check(w, "admitted", si, ci, buf.data_ptr(), n,
+                                    full[si][int(win_start[ci]):int(win_start[ci + 1])])
+        del buf
+        torch.cuda.empty_cache()
     setup_s = time.time() - t0
     budget = int(sum(table_bytes) / args.admit_overcommit)
     log(f"[admitted] {n_samples} samples, {sum(n_keys) / 1e9:.2f}e9 k-mers, tables {sum(table_bytes) / 1e9:.1f} GB "
@@ -902,6 +1108,11 @@ def admitted_arm(args, rank: int):
     out["saturated_speedup_vs_plain"] = (out["batched_saturated"]["probes_per_s"] /
                                          out["plain_saturated"]["probes_per_s"])
     out["rows_equal_full_scan"] = True
+    out["parity"] = {"status": "bit-exact" if ref_check is None or ref_check["status"] == "bit-exact"
+                     else "MISMATCH",
+                     "single_sample": "every admitted row equals the same window of its sample's full "
+                                      "single-sample scan",
+                     "reference": ref_check}
     out["note"] = ("latency of a whole-genome request = its last contig's completion - its submission; "
                    "both modes use per-sample tables under the same budget")
     ref.free()
@@ -909,46 +1120,58 @@ def admitted_arm(args, rank: int):
 
 
 def reference_arm(args, w):
-    """--impl reference: the reference's CPU-BATCHED scan on bounded slices."""
-    import torch
-    import ibs_b200 as ib
-    binp = REPO / "oracle" / "_ref" / "fastibs"
-    if not binp.exists():
+    """--impl reference: the reference's own CPU-BATCHED fastibs (built from
+    its sources into oracle/_ref/; FASTIBS_THREADS = all host threads) on the
+    workload's files, one contig of the reference per step, in contig order
+    and cycling: the warm-up steps and then `steps` timed ones (with at least
+    as many steps as contigs, the timed ones cover the whole reference). The
+    input files come from a separate `bench.py --prepare` process when they
+    are not there yet, so this process runs nothing of this repository's
+    libraries."""
+    if not REF_FASTIBS.exists():
         return {"impl": "reference", "unavailable": "oracle/_ref/fastibs was not built (the reference "
                 "sources are needed at build time)"}
-    runs = w.ref.n_runs()
-    d = cache_dir(w)
-    codes_ptr, n_codes, keep = None, 0, []
-    if not (d / "db" / "complete").exists():
-        if not torch.cuda.is_available():
-            return {"impl": "reference", "unavailable": "no GPU to generate the sample database"}
-        sw, mw = w.ref.packed_words()
-        dseq = torch.empty(sw, dtype=torch.int64, device="cuda")
-        dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
-        w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
-        bound = w.samples[0].codes_device_bound(w.ref, dseq.data_ptr(), dmask.data_ptr())
-        dcodes = torch.empty(bound, dtype=torch.int64, device="cuda")
-        n_codes = w.samples[0].codes_device(w.ref, dseq.data_ptr(), dmask.data_ptr(), dcodes.data_ptr(), bound)
-        codes_ptr = dcodes.data_ptr()
-        keep = [dseq, dmask, dcodes]
-    value, secs, probes = cpu_arm(w, runs, steps=args.steps, warmup=args.warmup,
-                                  slice_len=args.cpu_slice, dcodes_ptr=codes_ptr, n_codes=n_codes)
-    del keep
-    timed = secs[args.warmup:]
-    ms_step = 1e3 * sum(timed) / len(timed)
+    p = input_paths(w)
+    if not (p["db_stamp"].exists() and p["genome"].exists() and p["contig_stamp"].exists()):
+        cmd = [sys.executable, str(REPO / "bench.py"), "--prepare", "--workload", args.workload]
+        if args.scale != 1.0:
+            cmd += ["--scale", str(args.scale)]
+        r = subprocess.run(cmd)
+        if r.returncode != 0:
+            return {"impl": "reference", "unavailable": f"input preparation failed ({r.returncode})"}
+    k, W = w.k, w.window
+    names = list(w.ref.names)
+    per_contig = valid_positions_by_contig(w.ref.lens, k, w.ref.n_runs())
+    n = args.warmup + args.steps
+    steps = [i % len(names) for i in range(n)]
+    refdir = p["root"] / "ref_steps"
+    shutil.rmtree(refdir, ignore_errors=True)
+    refdir.mkdir(parents=True)
+    for i, c in enumerate(steps):
+        os.symlink(p["contig_dir"] / f"{names[c]}_genome.fasta", refdir / f"s{i:03d}_{names[c]}_genome.fasta")
+    threads = os.cpu_count() or 1
+    wall, phases, _ = run_fastibs(REF_FASTIBS, p["dbdir"], refdir, p["root"] / "ref_steps_out", W,
+                                  ("--cpu", "--probe=batched"), env=reference_env(threads))
+    stats = [phases[f"s{i:03d}_{names[c]}"]["stats"] for i, c in enumerate(steps)]
+    timed = range(args.warmup, n)
+    probes = sum(per_contig[steps[i]] for i in timed)
+    secs = sum(stats[i] for i in timed)
+    value = probes / secs
+    covered = sorted({steps[i] for i in timed})
     return {
         "metric": METRIC, "value": value, "unit": "probes/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u64", "impl": "reference",
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "impl": "reference",
         "data": "synthetic (seeded generator; stands in for plant-genome inputs not available here)",
-        "config": {"workload": w.name, "k": w.k, "window": w.window,
-                   "step": f"one {args.cpu_slice / 1e6:g} Mbp slice of {w.ref.names[0]} against the full "
-                           f"sample database"},
-        "cpu_baseline": {"value": value, "unit": "probes/s", "cores": os.cpu_count(), "kind": "reference",
-                         "sample": f"{args.steps} timed + {args.warmup} warm-up slices of "
-                                   f"{args.cpu_slice / 1e6:g} Mbp; fastibs --cpu --probe=batched "
-                                   f"(CPU-BATCHED, FASTIBS_THREADS={os.cpu_count()}); probes/s = valid "
-                                   f"positions / 'stats' phase seconds"},
+        "config": {"workload": w.name, "reference_bp": int(sum(map(int, w.ref.lens))), "contigs": len(names),
+                   "sample_kmers": int(p["db_stamp"].read_text()), "k": k, "window": W,
+                   "step": "one contig of the reference (in order, cycling) against the whole sample database",
+                   "timed_contigs_covered": f"{len(covered)} of {len(names)}"},
+        "cpu_baseline": {"value": value, "unit": "probes/s", "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} timed + {args.warmup} warm-up contig scans of {w.name}; "
+                                   f"oracle/_ref/fastibs --cpu --probe=batched (CPU-BATCHED, FASTIBS_THREADS="
+                                   f"{threads}); probes/s = valid positions / 'stats' phase seconds",
+                         "setup_s": phases[f"s000_{names[steps[0]]}"]["setup"], "wall_s": wall},
         "e2e": {"value": value, "unit": "probes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -980,8 +1203,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="plain_2gbp")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (testing)")
-    ap.add_argument("--cpu-slice", type=int, default=50_000_000, help="bases per CPU-baseline slice")
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--prepare", action="store_true",
+                    help="only write the workload's input files (KMC database, FASTA) and exit")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fasta-e2e", action="store_true", help="skip the from-FASTA end-to-end measurement")
     ap.add_argument("--table-format", type=int, default=0,
@@ -994,18 +1217,25 @@ def main():
     ap.add_argument("--blocks-in-flight", type=int, default=0)
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
-    ap.add_argument("--panel", action="store_true", help="also measure the 16-sample batched panel")
+    ap.add_argument("--no-panel", action="store_true",
+                    help="skip the 16-sample batched panel (measured by default at N=1)")
     ap.add_argument("--panel-only", action="store_true")
     ap.add_argument("--panel-samples", type=int, default=16)
     ap.add_argument("--panel-scale", type=float, default=1.0)
     ap.add_argument("--panel-keys-per-bucket", type=float, default=3.0)
     ap.add_argument("--panel-workload", choices=["panel_4gbp", "served_2gbp"], default="panel_4gbp",
                     help="panel_4gbp (k=31); served_2gbp's 16 k=25 samples make small profiling cases")
-    ap.add_argument("--serve", action="store_true", help="also measure the served request stream")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="skip the served request stream (measured by default at N=1)")
+    ap.add_argument("--no-admitted", action="store_true",
+                    help="skip memory-admitted serving (measured by default at N=1)")
     ap.add_argument("--serve-only", action="store_true")
     ap.add_argument("--serve-samples", type=int, default=16)
     ap.add_argument("--serve-requests", type=int, default=2000)
-    ap.add_argument("--serve-rate", type=float, default=50.0)
+    ap.add_argument("--serve-rates", default="5,20,50",
+                    help="Poisson arrival rates (req/s); the highest runs every request")
+    ap.add_argument("--serve-seconds", type=float, default=30.0,
+                    help="arrival time of the request prefix run at the lower rates")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="reference length scale")
     ap.add_argument("--admitted-only", action="store_true",
                     help="memory-admitted serving: 48 samples, tables ~3x the server's budget")
@@ -1029,12 +1259,13 @@ def main():
     from ibs_b200 import configs
     fn = getattr(configs, args.workload)
     w = fn(scale=args.scale) if args.scale != 1.0 else fn()
-    args.cpu_slice = min(args.cpu_slice, int(w.ref.lens[0]) // 2)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.prepare:
+        return prepare_main(args, w)
     if args.impl == "reference":
         if rank != 0:
             return 0
@@ -1065,14 +1296,26 @@ def main():
         print(json.dumps({"admitted": admitted_arm(args, rank)}), flush=True)
         return 0
     out = gpu_arm(args, w, rank, world, local)
-    if args.panel and world == 1:
+    # the batched and served forms, each on its own workload with its own
+    # parity check against single-sample scans; one failing is reported in
+    # the line, not fatal to it
+    if world == 1:
         import torch
-        torch.cuda.empty_cache()
-        out["extra"]["panel"] = panel_arm(args, rank)
-    if args.serve and world == 1:
-        import torch
-        torch.cuda.empty_cache()
-        out["extra"]["served"] = served_arm(args, rank)
+        for key, skip, fn in (("panel", args.no_panel, panel_arm), ("served", args.no_serve, served_arm),
+                              ("admitted", args.no_admitted, admitted_arm)):
+            if skip:
+                continue
+            torch.cuda.empty_cache()
+            t0 = time.time()
+            try:
+                out[key] = fn(args, rank)
+            except Exception as e:  # reported in the line
+                import traceback
+                traceback.print_exc()
+                out[key] = {"error": f"{type(e).__name__}: {e}"[-600:]}
+            out[key]["arm_wall_s"] = time.time() - t0
+            log(f"[bench] {key} arm done in {time.time() - t0:.0f} s")
+            torch.cuda.empty_cache()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

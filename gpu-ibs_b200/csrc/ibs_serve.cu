@@ -1,9 +1,10 @@
 // The serving loop: continuous batching of window-scan requests.
 //
 // A request names a sample and a range of windows of one contig. Samples
-// live in device tables, here called groups: a single-sample table (hash
-// formats B8x32 / B6x40) or a joint panel table (P5x48, one sample-mask per
-// key, up to 16 samples). Windows are numbered across contigs, so a request
+// live in device tables, here called groups: a single-sample table (the
+// minimizer-line formats MZ8 / MZ6 or the hash formats B8x32 / B6x40; the
+// server builds them in its table_format option's layout) or a joint panel
+// table (P5x48, one sample-mask per key, up to 16 samples). Windows are numbered across contigs, so a request
 // is an interval of that numbering.
 //
 // A background thread runs iterations. Each one admits new requests, makes
@@ -25,6 +26,7 @@
 //
 // No device code waits on the host: each launch is a finite kernel over a
 // finite work list.
+#include "mz_scan.cuh"
 #include "panel_core.cuh"
 #include "scan_device.cuh"
 
@@ -67,7 +69,11 @@ struct FinItem {
     uint64_t row;    // row slot
 };
 
-template <int NB>
+// Single-sample tables: one warp per work item. Minimizer-line tables (MZ8,
+// MZ6) take the window scan's minimizer path (dev::mz_span_stats), the
+// hash-bucket tables one bucket load per position. K > 0 is the server's k
+// fixed at compile time (0: read from the table).
+template <int NB, uint32_t K>
 __global__ void __launch_bounds__(256) k_serve_single(const TableView *__restrict__ views,
                                                       const WorkItem *__restrict__ items, uint32_t nItems,
                                                       const uint64_t *__restrict__ seq,
@@ -80,6 +86,18 @@ __global__ void __launch_bounds__(256) k_serve_single(const TableView *__restric
     for (uint64_t i = warp; i < nItems; i += nWarps) {
         const WorkItem it = items[i];
         const TableView t = views[it.view];
+        if (is_mz(t.g.format)) {
+            // the span's m-mer reads stop at its last position's last m-mer,
+            // inside the window's bases
+            const uint32_t lastM = it.p1 - 1 + (mz::w_of(K ? K : t.g.k) - 1);
+            const SegStats acc =
+                t.g.format == FMT_MZ8
+                    ? dev::mz_span_stats<NB, K, FMT_B8X32>(t, seq, mask, it.base, it.p0, it.p1, lastM, lane)
+                    : dev::mz_span_stats<NB, K, FMT_B6X40>(t, seq, mask, it.base, it.p0, it.p1, lastM, lane);
+            if (lane == 0)
+                sums[it.out] = acc;
+            continue;
+        }
         const uint32_t k = t.g.k;
         const uint64_t kmask = key_mask(2 * k);
         const uint64_t kbits = (1ull << k) - 1;
@@ -316,7 +334,8 @@ struct Launch {
     TableView *hSV = nullptr, *dSV = nullptr;
     panel::View *hJV = nullptr, *dJV = nullptr;
     SegStats *dSums = nullptr;
-    uint64_t positions = 0;
+    uint64_t positions = 0;        // reference positions scanned
+    uint64_t samplePositions = 0;  // positions x samples answered by those scans
     bool active = false;
 };
 
@@ -333,6 +352,8 @@ struct ibs_server {
     uint64_t budget = 0, resident = 0;
     uint64_t itemCap = kSumCap;
     bool serial = false; // one request per launch
+    uint32_t tableFormat = 0;   // single-sample tables built by the server (0: tuned default)
+    double keysPerBucket = 0;
     std::vector<std::unique_ptr<Group>> groups;
     std::vector<SampleRef> samples;
     std::vector<uint64_t> contigWin0; // global index of each contig's first window; back() = total
@@ -480,6 +501,7 @@ void retire(ibs_server *s, Launch &L)
     for (uint32_t g : L.groups)
         s->groups[g]->inflight--;
     s->st.scanned += L.positions;
+    s->st.sample_probes += L.samplePositions;
     for (Request *r : L.finishing) {
         ibs_request_result res = result_of(*r, IBS_OK, t);
         res.rows = static_cast<ibs_window *>(malloc(std::max<uint64_t>(r->nw, 1) * sizeof(ibs_window)));
@@ -612,6 +634,7 @@ void plan_group(ibs_server *s, Launch &L, Group &g, uint32_t view, const std::ve
             used.items += items;
             used.fins += requesters;
             L.positions += pos;
+            L.samplePositions += pos * (uint64_t)__builtin_popcount(m);
         }
         x1 = x + 1;
     }
@@ -662,6 +685,7 @@ bool iterate(ibs_server *s)
     retire(s, L); // its staging buffers are reused below
     uint32_t nSingle = 0, nJoint = 0, nFin = 0, nSV = 0, nJV = 0;
     L.positions = 0;
+    L.samplePositions = 0;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         // admit queued requests while the row pool has room
@@ -758,8 +782,15 @@ bool iterate(ibs_server *s)
     cudaEventRecord(L.start, st);
     if (nSingle) {
         const int grid = (int)std::min<uint64_t>((nSingle + 7) / 8, (uint64_t)s->sms * 8);
-        k_serve_single<kNB><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq, s->ref->dMask,
-                                                  L.dSums);
+        if (s->k == 25)
+            k_serve_single<kNB, 25><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq,
+                                                          s->ref->dMask, L.dSums);
+        else if (s->k == 31)
+            k_serve_single<kNB, 31><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq,
+                                                          s->ref->dMask, L.dSums);
+        else
+            k_serve_single<kNB, 0><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq,
+                                                         s->ref->dMask, L.dSums);
         IBS_LAUNCHED();
     }
     if (nJoint) {
@@ -894,6 +925,10 @@ extern "C" ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t
     if (opts && opts->max_spans_per_launch)
         s->itemCap = std::min<uint64_t>(opts->max_spans_per_launch, kSumCap);
     s->serial = opts && opts->one_request_per_launch;
+    if (opts) {
+        s->tableFormat = opts->table_format;
+        s->keysPerBucket = opts->keys_per_bucket;
+    }
     cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
     size_t fr = 0, tot = 0;
     IBS_CUDA(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
@@ -940,7 +975,8 @@ extern "C" ibs_status ibs_server_add_sample_codes(ibs_server *s, const uint64_t 
     }
     ibs_table_opts o{};
     o.device = s->device;
-    o.force_format = FMT_AUTO_HASH; // the serving kernel probes the hash-bucket formats
+    o.force_format = s->tableFormat;
+    o.keys_per_bucket = s->keysPerBucket;
     ibs_table *t = nullptr;
     ibs_status st = ibs_table_from_codes(codes, n, s->k, on_device, &o, &t);
     if (st != IBS_OK)
@@ -960,7 +996,8 @@ extern "C" ibs_status ibs_server_add_sample_kmc(ibs_server *s, const char *prefi
     }
     ibs_table_opts o{};
     o.device = s->device;
-    o.force_format = FMT_AUTO_HASH;
+    o.force_format = s->tableFormat;
+    o.keys_per_bucket = s->keysPerBucket;
     ibs_table *t = nullptr;
     ibs_status st = ibs_open(prefix, &o, &t);
     if (st != IBS_OK)

@@ -275,7 +275,11 @@ typedef struct ibs_server_opts {
     uint32_t max_spans_per_launch; /* 0 = 1<<15 */
     uint32_t min_spans_per_request; /* per launch, 0 = 16 */
     uint32_t one_request_per_launch; /* 1: no batching (every launch carries one whole request) */
-    uint32_t reserved[5];
+    uint32_t table_format;      /* layout of the single-sample tables the server builds (add_sample_*):
+                                   0 = the tuned default (ibs_tuning.table_format: minimizer lines for
+                                   large tables), else as ibs_table_opts.force_format */
+    double keys_per_bucket;     /* load of those tables (0 = the library default) */
+    uint32_t reserved[2];
 } ibs_server_opts;
 
 typedef struct ibs_request_result {
@@ -297,6 +301,9 @@ typedef struct ibs_server_stats {
     uint64_t queued, running;         /* waiting for admission / admitted and not yet complete */
     uint64_t scanned;                 /* reference positions the device scanned: a window that several
                                          requests share counts once (probes counts it per request) */
+    uint64_t sample_probes;           /* positions x samples the scans answered: a joint-table scan of a
+                                         window for three requesting samples counts its positions three
+                                         times (two requests of one sample count once) */
 } ibs_server_stats;
 
 ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t k, const ibs_server_opts *opts,
