@@ -655,7 +655,7 @@ def panel_arm(args, rank: int):
 
     # batched: joint tables of as many samples as fit next to the build's
     # scratch (one sample's codes); all 16 in one table when memory allows
-    kpb = args.panel_keys_per_bucket
+    kpb = args.panel_keys_per_bucket or ib.get_tuning().panel_keys_per_bucket
     free, _ = torch.cuda.mem_get_info()
     max_codes = max(sample_codes_bound(i) for i in range(len(w.samples))) * 8
     rows_bytes = n_win * len(w.samples) * 24 + 64 * n_win * len(w.samples)
@@ -899,7 +899,7 @@ def served_arm(args, rank: int):
     torch.cuda.empty_cache()
 
     # batched: joint panel tables (as many samples per table as memory allows)
-    kpb = args.panel_keys_per_bucket
+    kpb = args.panel_keys_per_bucket or ib.get_tuning().panel_keys_per_bucket
     free, _ = torch.cuda.mem_get_info()
     budget = free - max_bound * 8 - (4 << 30) - (8 << 30)
     union_of = {}
@@ -1222,7 +1222,8 @@ def main():
     ap.add_argument("--panel-only", action="store_true")
     ap.add_argument("--panel-samples", type=int, default=16)
     ap.add_argument("--panel-scale", type=float, default=1.0)
-    ap.add_argument("--panel-keys-per-bucket", type=float, default=3.0)
+    ap.add_argument("--panel-keys-per-bucket", type=float, default=0.0,
+                    help="joint-table load (0: the tuned default)")
     ap.add_argument("--panel-workload", choices=["panel_4gbp", "served_2gbp"], default="panel_4gbp",
                     help="panel_4gbp (k=31); served_2gbp's 16 k=25 samples make small profiling cases")
     ap.add_argument("--no-serve", action="store_true",

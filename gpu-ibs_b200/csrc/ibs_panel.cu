@@ -12,8 +12,6 @@
 namespace ibs {
 namespace panel {
 
-constexpr uint32_t kSpanLen = 8192;
-constexpr int kNB = 4;
 constexpr uint64_t kBuildChunk = 1ull << 27; // keys per build step (1 GiB of scratch each way)
 
 // ---- build: phase A finds keys already present and ORs in the sample bit;
@@ -355,7 +353,7 @@ extern "C" ibs_status ibs_panel_table_create(uint32_t k, uint64_t expected_keys,
     g.k = k;
     g.bits = 2 * k;
     g.format = 3;
-    const double lam = (opts && opts->keys_per_bucket > 0) ? opts->keys_per_bucket : 3.0;
+    const double lam = (opts && opts->keys_per_bucket > 0) ? opts->keys_per_bucket : tuning().panel_keys_per_bucket;
     uint64_t nb = (uint64_t)((double)expected_keys / lam) + 1;
     const uint64_t minN = g.bits > 32 ? (1ull << (g.bits - 32)) : 1;
     nb = std::max(nb, minN);
@@ -582,11 +580,12 @@ static uint32_t pass_count(const ibs_panel_table *p)
 // Plan and scratch of (reference, W) for the panel scan.
 static ibs_status panel_plan(ibs_panel_table *p, const ibs_reference *ref, uint32_t W)
 {
+    const uint32_t spanLen = tuning().panel_span_len;
     if (p->planRef == ref && p->plan.W == W && p->plan.dWin && p->planLens == ref->lens &&
-        (pass_count(p) <= 1 || p->dMasks))
+        p->plan.spanLen == spanLen && (pass_count(p) <= 1 || p->dMasks))
         return IBS_OK;
     p->plan.release();
-    plan_windows(p->plan, ref->lens, ref->baseOff, W, p->geom.k, kSpanLen);
+    plan_windows(p->plan, ref->lens, ref->baseOff, W, p->geom.k, spanLen);
     IBS_CUDA(cudaMalloc(&p->plan.dWin, std::max<uint64_t>(p->plan.nWin, 1) * sizeof(WinDesc)), "plan alloc");
     IBS_CUDA(cudaMalloc(&p->plan.dSpan0, (p->plan.nWin + 1) * sizeof(uint32_t)), "plan alloc");
     if (p->plan.nWin)
@@ -619,37 +618,49 @@ static ibs_status panel_plan(ibs_panel_table *p, const ibs_reference *ref, uint3
     return IBS_OK;
 }
 
+// The span kernel's launches of one scan: one launch, or one per
+// bucket-range pass and a statistics launch.
+template <int NB>
+static ibs_status enqueue_spans(ibs_panel_table *p, const ibs_reference *ref, uint32_t passes, int grid,
+                                cudaStream_t st)
+{
+    const ScanPlan &pl = p->plan;
+    if (passes <= 1) {
+        IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
+        k_panel_spans<NB, kScan><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
+                                                       (uint32_t)pl.nWin, pl.nSpans, pl.spanLen, p->nSamples,
+                                                       p->dCounters + 1, p->dSpans, nullptr, 0, 0, false);
+        IBS_LAUNCHED();
+        return IBS_OK;
+    }
+    const uint64_t nb = p->geom.nBuckets;
+    for (uint32_t i = 0; i < passes; ++i) {
+        IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
+        k_panel_spans<NB, kMaskPass><<<grid, 256, 0, st>>>(
+            p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0, (uint32_t)pl.nWin, pl.nSpans, pl.spanLen,
+            p->nSamples, p->dCounters + 1, p->dSpans, p->dMasks, nb * i / passes, nb * (i + 1) / passes, i == 0);
+        IBS_LAUNCHED();
+    }
+    IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
+    k_panel_spans<NB, kStats><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
+                                                    (uint32_t)pl.nWin, pl.nSpans, pl.spanLen, p->nSamples,
+                                                    p->dCounters + 1, p->dSpans, p->dMasks, 0, 0, false);
+    IBS_LAUNCHED();
+    return IBS_OK;
+}
+
 static ibs_status panel_enqueue(ibs_panel_table *p, const ibs_reference *ref, ibs_window *rowsDev,
                                 cudaStream_t st)
 {
     const ScanPlan &pl = p->plan;
     const uint32_t passes = pass_count(p);
     if (pl.nSpans) {
-        const int grid = sm_count() * 6;
-        if (passes <= 1) {
-            IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
-            k_panel_spans<kNB, kScan><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
-                                                            (uint32_t)pl.nWin, pl.nSpans, pl.spanLen,
-                                                            p->nSamples, p->dCounters + 1, p->dSpans, nullptr,
-                                                            0, 0, false);
-            IBS_LAUNCHED();
-        } else {
-            const uint64_t nb = p->geom.nBuckets;
-            for (uint32_t i = 0; i < passes; ++i) {
-                IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
-                k_panel_spans<kNB, kMaskPass><<<grid, 256, 0, st>>>(
-                    p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0, (uint32_t)pl.nWin, pl.nSpans,
-                    pl.spanLen, p->nSamples, p->dCounters + 1, p->dSpans, p->dMasks, nb * i / passes,
-                    nb * (i + 1) / passes, i == 0);
-                IBS_LAUNCHED();
-            }
-            IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
-            k_panel_spans<kNB, kStats><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
-                                                             (uint32_t)pl.nWin, pl.nSpans, pl.spanLen,
-                                                             p->nSamples, p->dCounters + 1, p->dSpans, p->dMasks,
-                                                             0, 0, false);
-            IBS_LAUNCHED();
-        }
+        const ibs_tuning tu = tuning();
+        const int grid = sm_count() * (int)tu.panel_ctas_per_sm;
+        const ibs_status s = tu.panel_blocks_in_flight == 2 ? enqueue_spans<2>(p, ref, passes, grid, st)
+                                                            : enqueue_spans<4>(p, ref, passes, grid, st);
+        if (s != IBS_OK)
+            return s;
     }
     if (pl.nWin && p->nSamples) {
         k_panel_finalize<<<grid_for(pl.nWin * p->nSamples), 256, 0, st>>>(
@@ -688,7 +699,10 @@ extern "C" ibs_status ibs_panel_table_scan_async(ibs_panel_table *p, ibs_referen
     // Replay the captured scan when (reference, W, rows, stream) repeat:
     // the work reset, the span kernel and the finalizer as one graph.
     const void *key[3] = {ref, rows_dev, stream};
-    if (p->graph && p->graphW == W && !memcmp(key, p->graphKey, sizeof key)) {
+    const ibs_tuning tu = tuning();
+    const uint32_t shape[2] = {tu.panel_ctas_per_sm, tu.panel_blocks_in_flight};
+    if (p->graph && p->graphW == W && !memcmp(key, p->graphKey, sizeof key) &&
+        !memcmp(shape, p->graphShape, sizeof shape)) {
         IBS_CUDA(cudaGraphLaunch(p->graph, st), "panel graph launch");
         IBS_LAUNCHED();
         return IBS_OK;
@@ -714,6 +728,7 @@ extern "C" ibs_status ibs_panel_table_scan_async(ibs_panel_table *p, ibs_referen
         return s;
     IBS_CUDA(e, "panel graph capture");
     memcpy(p->graphKey, key, sizeof key);
+    memcpy(p->graphShape, shape, sizeof shape);
     p->graphW = W;
     IBS_CUDA(cudaGraphLaunch(p->graph, st), "panel graph launch");
     return IBS_OK;

@@ -33,7 +33,9 @@ static std::mutex g_tuneMu;
 // plain 2 Gbp x 2.19e9 k-mers): minimizer table at 1.5 keys per 32-byte
 // sector, spans of 2048 positions, 2 blocks in flight, 512 threads, 16 CTAs
 // per SM.
-static ibs_tuning g_tune = {2048, 2, 512, 16, 1.5, FMT_MZ8, 0, {0, 0}};
+// Joint-table scans: spans of 8192 positions, 6 CTAs of 256 threads per SM,
+// 4 blocks in flight, 3 keys per 5-slot bucket.
+static ibs_tuning g_tune = {2048, 2, 512, 16, 1.5, FMT_MZ8, 0, 8192, 6, 3.0, 4, {0, 0, 0}};
 
 const ibs_tuning &tuning() { return g_tune; }
 
@@ -1052,6 +1054,29 @@ extern "C" ibs_status ibs_set_tuning(const ibs_tuning *t)
         n.table_format = t->table_format == 0xffffffffu ? 0 : t->table_format;
     if (t->panel_pass_mb)
         n.panel_pass_mb = t->panel_pass_mb == 0xffffffffu ? 0 : t->panel_pass_mb;
+    if (t->panel_span_len) {
+        if (t->panel_span_len % 128 || t->panel_span_len > (1u << 24)) {
+            set_error("ibs_set_tuning: panel_span_len must be a multiple of 128");
+            return IBS_ERR_ARG;
+        }
+        n.panel_span_len = t->panel_span_len;
+    }
+    if (t->panel_ctas_per_sm)
+        n.panel_ctas_per_sm = std::min<uint32_t>(t->panel_ctas_per_sm, 8);
+    if (t->panel_keys_per_bucket > 0) {
+        if (t->panel_keys_per_bucket > 5.0) {
+            set_error("ibs_set_tuning: panel_keys_per_bucket must be at most 5 (slots per bucket)");
+            return IBS_ERR_ARG;
+        }
+        n.panel_keys_per_bucket = t->panel_keys_per_bucket;
+    }
+    if (t->panel_blocks_in_flight) {
+        if (t->panel_blocks_in_flight != 2 && t->panel_blocks_in_flight != 4) {
+            set_error("ibs_set_tuning: panel_blocks_in_flight must be 2 or 4");
+            return IBS_ERR_ARG;
+        }
+        n.panel_blocks_in_flight = t->panel_blocks_in_flight;
+    }
     g_tune = n;
     return IBS_OK;
 }

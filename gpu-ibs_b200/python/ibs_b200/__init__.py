@@ -71,7 +71,9 @@ class ServerStats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("span_len", C.c_uint32), ("blocks_in_flight", C.c_uint32), ("block_threads", C.c_uint32),
                 ("ctas_per_sm", C.c_uint32), ("keys_per_bucket", C.c_double), ("table_format", C.c_uint32),
-                ("panel_pass_mb", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+                ("panel_pass_mb", C.c_uint32), ("panel_span_len", C.c_uint32), ("panel_ctas_per_sm", C.c_uint32),
+                ("panel_keys_per_bucket", C.c_double), ("panel_blocks_in_flight", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
@@ -364,8 +366,11 @@ class PanelTable:
             pass
 
 
-def table_bytes_for(n_keys: int, k: int) -> int:
-    return _ibs_table_bytes_for(n_keys, k, None)
+def table_bytes_for(n_keys: int, k: int, force_format: int = 0, keys_per_bucket: float = 0.0) -> int:
+    if not force_format and not keys_per_bucket:
+        return _ibs_table_bytes_for(n_keys, k, None)
+    opts = TableOpts(0, keys_per_bucket, force_format)
+    return _ibs_table_bytes_for(n_keys, k, C.byref(opts))
 
 
 def device_memory(device: int = 0) -> tuple[int, int]:

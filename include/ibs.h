@@ -381,10 +381,16 @@ typedef struct ibs_tuning {
     uint32_t table_format;     /* default format of new tables (0 = automatic, 4 = minimizer buckets) */
     uint32_t panel_pass_mb;    /* joint-table scans probe bucket ranges of at most this many MiB per
                                   pass (random loads over a larger range translate slowly); 0 = 48 GiB */
-    uint32_t reserved[2];
+    uint32_t panel_span_len;   /* positions per work item of the joint-table scan (multiple of 128) */
+    uint32_t panel_ctas_per_sm; /* resident CTAs per SM of the persistent joint-table scan (256 threads) */
+    double panel_keys_per_bucket; /* default load of new joint tables (keys per 5-slot bucket) */
+    uint32_t panel_blocks_in_flight; /* 32-position blocks in flight per lane in that scan: 2 or 4 */
+    uint32_t reserved[3];
 } ibs_tuning;
 /* Fields left 0 keep their value; table_format and panel_pass_mb take
- * 0xffffffff to go back to 0 (automatic / the default). */
+ * 0xffffffff to go back to 0 (automatic / the default). The joint-table
+ * fields apply to joint tables created (load) and scans enqueued (launch
+ * shape) after the call. */
 ibs_status ibs_set_tuning(const ibs_tuning *t);
 void ibs_get_tuning(ibs_tuning *t);
 

@@ -45,10 +45,11 @@ def expected(world, r):
     return rows[a:a + r["n_windows"]]
 
 
-def make_server(world, budget_tables=2.5):
-    sizes = [ib.table_bytes_for(len(c), K) for c in world["samples"]]
+def make_server(world, budget_tables=2.5, table_format=0, serial=False):
+    sizes = [ib.table_bytes_for(len(c), K, force_format=table_format) for c in world["samples"]]
     budget = int(max(sizes) * budget_tables)
-    srv = ib.Server(world["ref"], W, K, memory_budget=budget, max_spans_per_launch=512, min_spans_per_request=8)
+    srv = ib.Server(world["ref"], W, K, memory_budget=budget, max_spans_per_launch=512, min_spans_per_request=8,
+                    table_format=table_format, one_request_per_launch=serial)
     ids = [srv.add_codes(c, len(c), on_device=False) for c in world["samples"]]
     assert ids == list(range(len(world["samples"])))
     return srv
@@ -107,6 +108,34 @@ def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world):
     srv.close()
 
 
+@pytest.mark.parametrize("table_format,serial", [(4, False), (4, True), (6, False)])
+def test_minimizer_tables_alone_and_in_a_mix(world, table_format, serial):
+    """The server's single-sample tables in the minimizer-line layouts (MZ8,
+    MZ6), one request per launch or batched, under a budget that forces
+    evictions: every row equals the full scan's."""
+    srv = make_server(world, budget_tables=2.2, table_format=table_format, serial=serial)
+    for req in random_requests(world, 8, 11):
+        srv.submit(*req)
+        got = srv.poll(1, timeout_ms=60_000)
+        assert len(got) == 1, ("no result within 60 s", req, srv.stats())
+        assert got[0]["status"] == 0
+        assert np.array_equal(got[0]["rows"], expected(world, got[0])), req
+    reqs = random_requests(world, 120, 12) + [(s, 0, 0, 0) for s in range(6)]
+    for req in reqs:
+        srv.submit(*req)
+    done, deadline = [], time.time() + 300
+    while len(done) < len(reqs) and time.time() < deadline:
+        done += srv.poll(64, timeout_ms=2000)
+    assert len(done) == len(reqs), ("requests left unfinished", srv.stats())
+    for r in done:
+        assert r["status"] == 0
+        assert np.array_equal(r["rows"], expected(world, r)), (r["sample"], r["contig"], r["first_window"])
+    st = srv.stats()
+    assert st["evictions"] > 0 and st["reloads"] > 0, st
+    assert st["sample_probes"] == st["scanned"]  # single-sample tables: one sample per scanned position
+    srv.close()
+
+
 def make_panel_server(world, serial=False):
     """The six samples as one joint panel table, plus sample 0 once more as a
     single-sample table (id 6), in one server."""
@@ -156,6 +185,7 @@ def test_panel_server_alone_and_in_a_mix(world, serial):
         assert r["status"] == 0
         assert np.array_equal(r["rows"], expected_any(world, r)), (r["sample"], r["contig"], r["first_window"])
     st = srv.stats()
+    assert st["sample_probes"] >= st["scanned"]
     if serial:
         assert st["scanned"] == st["probes"]  # one request per launch: nothing shared
     else:

@@ -162,3 +162,28 @@ def test_library_defaults_are_the_committed_tuning():
                 "table_format"):
         assert t[key] == best[key], key
     assert best["rows_equal"]
+
+
+def test_python_structs_match_the_c_header(tmp_path):
+    """ctypes mirrors of the header's structs: same size and field offsets
+    as the C compiler lays them out."""
+    import subprocess
+    structs = {"ibs_tuning": ib.Tuning, "ibs_server_opts": ib.ServerOpts, "ibs_server_stats": ib.ServerStats,
+               "ibs_table_opts": ib.TableOpts, "ibs_table_info": ib.TableInfo,
+               "ibs_request_result": ib.RequestResult}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "ibs.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "sizes.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-I", str(REPO / "include"), "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(ln.split()[:2]): int(ln.split()[2]) for ln in out if ln}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
