@@ -52,7 +52,9 @@ constexpr uint64_t kPosCap = 512ull << 20; // reference positions scanned per la
 constexpr uint64_t kFinCap = 1ull << 20;   // (request, window) rows finalized per launch
 constexpr uint64_t kRowPool = 4ull << 20;  // rows of admitted requests (24 B each): 96 MiB
 constexpr uint32_t kMaxGroups = 4096;
-constexpr int kDepth = 2;                  // launches in flight
+constexpr int kDepth = 4;                  // iterations (batches) in flight
+constexpr int kServeNB = 2;                // blocks in flight per lane of the single-table and persistent
+                                           // kernels (64 registers, four CTAs of 256 per SM)
 
 struct WorkItem {
     uint64_t base;   // packed base offset of the window's first base
@@ -69,84 +71,176 @@ struct FinItem {
     uint64_t row;    // row slot
 };
 
-// Single-sample tables: one warp per work item. Minimizer-line tables (MZ8,
-// MZ6) take the window scan's minimizer path (dev::mz_span_stats), the
-// hash-bucket tables one bucket load per position. K > 0 is the server's k
-// fixed at compile time (0: read from the table).
+// One work item over a single-sample table, by one warp: the summary of
+// positions [p0, p1) of its window goes to sums[it.out]. Minimizer-line
+// tables (MZ8, MZ6) take the window scan's minimizer path
+// (dev::mz_span_stats), the hash-bucket tables one bucket load per
+// position. K > 0 is the server's k fixed at compile time (0: read from the
+// table).
 template <int NB, uint32_t K>
-__global__ void __launch_bounds__(256) k_serve_single(const TableView *__restrict__ views,
-                                                      const WorkItem *__restrict__ items, uint32_t nItems,
-                                                      const uint64_t *__restrict__ seq,
-                                                      const uint64_t *__restrict__ mask,
-                                                      SegStats *__restrict__ sums)
+__device__ __forceinline__ void serve_single_item(const WorkItem &it, const TableView &t,
+                                                  const uint64_t *__restrict__ seq,
+                                                  const uint64_t *__restrict__ mask, SegStats *__restrict__ sums,
+                                                  uint32_t lane)
+{
+    if (is_mz(t.g.format)) {
+        // the span's m-mer reads stop at its last position's last m-mer,
+        // inside the window's bases
+        const uint32_t lastM = it.p1 - 1 + (mz::w_of(K ? K : t.g.k) - 1);
+        const SegStats acc =
+            t.g.format == FMT_MZ8
+                ? dev::mz_span_stats<NB, K, FMT_B8X32>(t, seq, mask, it.base, it.p0, it.p1, lastM, lane)
+                : dev::mz_span_stats<NB, K, FMT_B6X40>(t, seq, mask, it.base, it.p0, it.p1, lastM, lane);
+        if (lane == 0)
+            sums[it.out] = acc;
+        return;
+    }
+    const uint32_t k = t.g.k;
+    const uint64_t kmask = key_mask(2 * k);
+    const uint64_t kbits = (1ull << k) - 1;
+    const bool b8 = t.g.format == FMT_B8X32;
+    dev::LaneFold fold;
+    for (uint32_t p = it.p0; p < it.p1; p += 32 * NB) {
+        uint4 v0[NB], v1[NB];
+        uint64_t code[NB], fp[NB];
+        bool valid[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const uint32_t q = p + 32 * b + lane;
+            const bool in = q < it.p1;
+            const uint64_t G = it.base + (in ? q : it.p0);
+            bool acgt;
+            code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
+            valid[b] = in && acgt;
+            const uint64_t h = perm_hash(code[b], t.g.bits);
+            const uint64_t r = bucket_of(h, t.g);
+            fp[b] = fp_of(h, t.g);
+            if (valid[b]) {
+                v0[b] = __ldg(t.buckets + 2 * r);
+                v1[b] = __ldg(t.buckets + 2 * r + 1);
+            } else {
+                v0[b] = make_uint4(0, 0, 0, 0);
+                v1[b] = make_uint4(0, 0, 0, 0);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            bool hit = false;
+            if (valid[b]) {
+                const uint32_t m = b8 ? bucket_match<FMT_B8X32>(v0[b], v1[b], fp[b])
+                                      : bucket_match<FMT_B6X40>(v0[b], v1[b], fp[b]);
+                hit = m == 1u || (m == 2u && stash_lookup(t, code[b]));
+            }
+            const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
+            const uint32_t H = __ballot_sync(dev::FULL_MASK, hit);
+            fold.push(V, H, lane, (int)k);
+        }
+    }
+    const SegStats acc = fold.finish((int)k);
+    if (lane == 0)
+        sums[it.out] = acc;
+}
+
+// One work item over a joint table: one bucket load per position; lane j
+// keeps the statistics of sample j when j is in the item's mask, and the
+// requesting samples' summaries go to sums[it.out + rank].
+template <int NB>
+__device__ __forceinline__ void serve_joint_item(const WorkItem &it, const panel::View &t,
+                                                 const uint64_t *__restrict__ seq,
+                                                 const uint64_t *__restrict__ mask, SegStats *__restrict__ sums,
+                                                 uint32_t lane)
+{
+    const uint32_t k = t.g.k;
+    const uint64_t kmask = key_mask(2 * k);
+    const uint64_t kbits = (1ull << k) - 1;
+    const uint32_t want = it.mask & 0xffffu;
+    SegStats acc = seg_empty();
+    for (uint32_t p = it.p0; p < it.p1; p += 32 * NB) {
+        uint4 v0[NB], v1[NB];
+        uint64_t code[NB];
+        uint32_t fp[NB];
+        bool valid[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const uint32_t q = p + 32 * b + lane;
+            const bool in = q < it.p1;
+            const uint64_t G = it.base + (in ? q : it.p0);
+            bool acgt;
+            code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
+            valid[b] = in && acgt;
+            const uint64_t h = perm_hash(code[b], t.g.bits);
+            const uint64_t r = bucket_of(h, t.g);
+            fp[b] = (uint32_t)fp_of(h, t.g);
+            if (valid[b]) {
+                v0[b] = __ldg(t.buckets + 2 * r);
+                v1[b] = __ldg(t.buckets + 2 * r + 1);
+            } else {
+                v0[b] = make_uint4(0, 0, 0, 0);
+                v1[b] = make_uint4(0, 0, 0, 0);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            uint32_t m = 0;
+            if (valid[b]) {
+                m = panel::bucket_mask(v0[b], v1[b], fp[b]);
+                if (m & 0x80000000u)
+                    m = panel::stash_mask(t, code[b]);
+            }
+            const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
+            uint32_t myH = 0;
+            for (uint32_t rest = want; rest; rest &= rest - 1) { // warp-uniform
+                const uint32_t j = __ffs(rest) - 1;
+                const uint32_t Hj = __ballot_sync(dev::FULL_MASK, (m >> j) & 1u);
+                if (lane == j)
+                    myH = Hj;
+            }
+            if ((want >> lane) & 1u)
+                acc = seg_combine(acc, panel::block_stats_serial(V, myH, (int)k), (int)k);
+        }
+    }
+    if ((want >> lane) & 1u)
+        sums[it.out + __popc(want & ((1u << lane) - 1u))] = acc;
+}
+
+// One (request, window) row from the window's span summaries.
+__device__ __forceinline__ void serve_fin_item(const FinItem &f, const SegStats *__restrict__ sums, int k,
+                                               ibs_window *__restrict__ rows)
+{
+    SegStats acc = seg_empty();
+    for (uint32_t s = 0; s < f.nSpans; ++s)
+        acc = seg_combine(acc, sums[f.sum + (uint64_t)s * f.stride], k);
+    WindowRow row;
+    row.start = f.start;
+    row.end = f.end;
+    seg_finish(acc, k, row);
+    ibs_window o;
+    o.start = row.start;
+    o.end = row.end;
+    o.total_kmers = row.total_kmers;
+    o.observed_kmers = row.observed_kmers;
+    o.variations = row.variations;
+    o.kmer_distance = row.kmer_distance;
+    rows[f.row] = o;
+}
+
+// ---- one launch per iteration (one_request_per_launch: the plain path) ----
+template <int NB, uint32_t K>
+__global__ void __launch_bounds__(256, 4) k_serve_single(const TableView *__restrict__ views,
+                                                         const WorkItem *__restrict__ items, uint32_t nItems,
+                                                         const uint64_t *__restrict__ seq,
+                                                         const uint64_t *__restrict__ mask,
+                                                         SegStats *__restrict__ sums)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = warp; i < nItems; i += nWarps) {
         const WorkItem it = items[i];
-        const TableView t = views[it.view];
-        if (is_mz(t.g.format)) {
-            // the span's m-mer reads stop at its last position's last m-mer,
-            // inside the window's bases
-            const uint32_t lastM = it.p1 - 1 + (mz::w_of(K ? K : t.g.k) - 1);
-            const SegStats acc =
-                t.g.format == FMT_MZ8
-                    ? dev::mz_span_stats<NB, K, FMT_B8X32>(t, seq, mask, it.base, it.p0, it.p1, lastM, lane)
-                    : dev::mz_span_stats<NB, K, FMT_B6X40>(t, seq, mask, it.base, it.p0, it.p1, lastM, lane);
-            if (lane == 0)
-                sums[it.out] = acc;
-            continue;
-        }
-        const uint32_t k = t.g.k;
-        const uint64_t kmask = key_mask(2 * k);
-        const uint64_t kbits = (1ull << k) - 1;
-        const bool b8 = t.g.format == FMT_B8X32;
-        dev::LaneFold fold;
-        for (uint32_t p = it.p0; p < it.p1; p += 32 * NB) {
-            uint4 v0[NB], v1[NB];
-            uint64_t code[NB], fp[NB];
-            bool valid[NB];
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const uint32_t q = p + 32 * b + lane;
-                const bool in = q < it.p1;
-                const uint64_t G = it.base + (in ? q : it.p0);
-                bool acgt;
-                code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
-                valid[b] = in && acgt;
-                const uint64_t h = perm_hash(code[b], t.g.bits);
-                const uint64_t r = bucket_of(h, t.g);
-                fp[b] = fp_of(h, t.g);
-                if (valid[b]) {
-                    v0[b] = __ldg(t.buckets + 2 * r);
-                    v1[b] = __ldg(t.buckets + 2 * r + 1);
-                } else {
-                    v0[b] = make_uint4(0, 0, 0, 0);
-                    v1[b] = make_uint4(0, 0, 0, 0);
-                }
-            }
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                bool hit = false;
-                if (valid[b]) {
-                    const uint32_t m = b8 ? bucket_match<FMT_B8X32>(v0[b], v1[b], fp[b])
-                                          : bucket_match<FMT_B6X40>(v0[b], v1[b], fp[b]);
-                    hit = m == 1u || (m == 2u && stash_lookup(t, code[b]));
-                }
-                const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
-                const uint32_t H = __ballot_sync(dev::FULL_MASK, hit);
-                fold.push(V, H, lane, (int)k);
-            }
-        }
-        const SegStats acc = fold.finish((int)k);
-        if (lane == 0)
-            sums[it.out] = acc;
+        serve_single_item<NB, K>(it, views[it.view], seq, mask, sums, lane);
     }
 }
 
-// Joint tables: one bucket load per position; lane j keeps the statistics
-// of sample j when j is in the item's mask.
 template <int NB>
 __global__ void __launch_bounds__(256) k_serve_joint(const panel::View *__restrict__ views,
                                                      const WorkItem *__restrict__ items, uint32_t nItems,
@@ -159,58 +253,7 @@ __global__ void __launch_bounds__(256) k_serve_joint(const panel::View *__restri
     const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = warp; i < nItems; i += nWarps) {
         const WorkItem it = items[i];
-        const panel::View t = views[it.view];
-        const uint32_t k = t.g.k;
-        const uint64_t kmask = key_mask(2 * k);
-        const uint64_t kbits = (1ull << k) - 1;
-        const uint32_t want = it.mask & 0xffffu;
-        SegStats acc = seg_empty();
-        for (uint32_t p = it.p0; p < it.p1; p += 32 * NB) {
-            uint4 v0[NB], v1[NB];
-            uint64_t code[NB];
-            uint32_t fp[NB];
-            bool valid[NB];
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const uint32_t q = p + 32 * b + lane;
-                const bool in = q < it.p1;
-                const uint64_t G = it.base + (in ? q : it.p0);
-                bool acgt;
-                code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
-                valid[b] = in && acgt;
-                const uint64_t h = perm_hash(code[b], t.g.bits);
-                const uint64_t r = bucket_of(h, t.g);
-                fp[b] = (uint32_t)fp_of(h, t.g);
-                if (valid[b]) {
-                    v0[b] = __ldg(t.buckets + 2 * r);
-                    v1[b] = __ldg(t.buckets + 2 * r + 1);
-                } else {
-                    v0[b] = make_uint4(0, 0, 0, 0);
-                    v1[b] = make_uint4(0, 0, 0, 0);
-                }
-            }
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                uint32_t m = 0;
-                if (valid[b]) {
-                    m = panel::bucket_mask(v0[b], v1[b], fp[b]);
-                    if (m & 0x80000000u)
-                        m = panel::stash_mask(t, code[b]);
-                }
-                const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
-                uint32_t myH = 0;
-                for (uint32_t rest = want; rest; rest &= rest - 1) { // warp-uniform
-                    const uint32_t j = __ffs(rest) - 1;
-                    const uint32_t Hj = __ballot_sync(dev::FULL_MASK, (m >> j) & 1u);
-                    if (lane == j)
-                        myH = Hj;
-                }
-                if ((want >> lane) & 1u)
-                    acc = seg_combine(acc, panel::block_stats_serial(V, myH, (int)k), (int)k);
-            }
-        }
-        if ((want >> lane) & 1u)
-            sums[it.out + __popc(want & ((1u << lane) - 1u))] = acc;
+        serve_joint_item<NB>(it, views[it.view], seq, mask, sums, lane);
     }
 }
 
@@ -218,23 +261,217 @@ __global__ void k_serve_finalize(const FinItem *__restrict__ fin, uint32_t n, co
                                  int k, ibs_window *__restrict__ rows)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const FinItem f = fin[i];
-        SegStats acc = seg_empty();
-        for (uint32_t s = 0; s < f.nSpans; ++s)
-            acc = seg_combine(acc, sums[f.sum + (uint64_t)s * f.stride], k);
-        WindowRow row;
-        row.start = f.start;
-        row.end = f.end;
-        seg_finish(acc, k, row);
-        ibs_window o;
-        o.start = row.start;
-        o.end = row.end;
-        o.total_kmers = row.total_kmers;
-        o.observed_kmers = row.observed_kmers;
-        o.variations = row.variations;
-        o.kmer_distance = row.kmer_distance;
-        rows[f.row] = o;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        serve_fin_item(fin[i], sums, k, rows);
+}
+
+// ---- the persistent launch (batched serving) --------------------------------
+// One kernel stays resident while requests keep arriving. The host publishes
+// batches (the work of one loop iteration: span items over single and joint
+// tables, then the rows to fold) into a ring of kRing descriptors in pinned
+// host memory and raises `published`, a count of tickets. Warps claim
+// tickets from a device counter in order: the scan tickets of a batch come
+// first, one span item each, then its fold tickets, kFinPerTicket rows each.
+// A fold ticket waits until the batch's scan items are done; the warp that
+// completes a batch's last fold ticket stamps it done in pinned host memory,
+// where the host loop sees it. Rows are written straight into the pinned
+// row pool.
+//
+// Every wait is bounded. A warp whose ticket is not published within the
+// idle limit stops the kernel (the host launches it again when work comes);
+// a fold ticket whose batch's scans do not finish within the wait limit
+// stops it with a timeout status. Batches that were published but not done
+// when the kernel stopped are published again to the next launch: a
+// batch's scans and folds rewrite the same sums and rows, so a repeat gives
+// the same result.
+constexpr int kRing = kDepth;
+constexpr uint32_t kFinPerTicket = 256;
+enum : uint32_t { kExitNone = 0, kExitIdle = 1, kExitStop = 2, kExitTimeout = 3 };
+
+struct BatchDesc {                 // host-written
+    uint64_t seq;                  // batch number, from 1 (0: slot unused)
+    uint64_t ticket0;              // first ticket
+    uint32_t nSingle, nJoint, nFin, nFinTickets;
+    const WorkItem *single, *joint;
+    const FinItem *fin;
+    const TableView *sv;
+    const panel::View *jv;
+    SegStats *sums;
+};
+constexpr int kDescWords = sizeof(BatchDesc) / 8;
+static_assert(sizeof(BatchDesc) % 8 == 0 && kDescWords <= 32, "descriptor read by one warp, a word per lane");
+
+struct Ctrl {                      // pinned host memory, written by the host
+    uint64_t published;            // tickets published so far (release-stored)
+    uint32_t stop, pad;
+    BatchDesc slot[kRing];
+};
+
+struct Status {                    // pinned host memory, written by the kernel
+    uint64_t doneSeq[kRing];       // last batch completed in each slot
+    uint64_t tFirst[kRing], tDone[kRing]; // global timer (ns) of a batch's first claim and its completion
+    uint32_t exitReason, pad;
+};
+
+struct DevState {                  // device memory, zeroed before each launch
+    unsigned long long ticket;
+    unsigned long long scanDone[kRing], finDone[kRing];
+    unsigned int draining;
+};
+
+__device__ __forceinline__ uint64_t ld_acquire_sys(const uint64_t *p)
+{
+    uint64_t v;
+    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_sys(uint64_t *p, uint64_t v)
+{
+    asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <int NB, uint32_t K>
+__global__ void __launch_bounds__(256, 4) k_serve_persistent(const Ctrl *ctrl, Status *status, DevState *ds,
+                                                             const uint64_t *__restrict__ seq,
+                                                             const uint64_t *__restrict__ mask, int k,
+                                                             ibs_window *rows, uint64_t idleNs, uint64_t waitNs)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    // this warp's copy of the batch it worked on last
+    uint64_t dT0 = 0, dEnd = 0;
+    uint32_t slot = 0;
+    uint64_t word = 0; // lane i < kDescWords: word i of that batch's descriptor
+    for (;;) {
+        // claim the next ticket, unless the kernel is stopping
+        unsigned long long t = 0;
+        uint32_t go = 0;
+        if (lane == 0) {
+            if (!*(volatile unsigned int *)&ds->draining && !*(volatile const uint32_t *)&ctrl->stop) {
+                t = atomicAdd(&ds->ticket, 1ull);
+                // wait (bounded) until it is published
+                const uint64_t t0 = global_ns();
+                for (uint64_t spin = 0;; ++spin) {
+                    if (ld_acquire_sys(&ctrl->published) > t) {
+                        go = 1;
+                        break;
+                    }
+                    if (*(volatile unsigned int *)&ds->draining || *(volatile const uint32_t *)&ctrl->stop)
+                        break;
+                    if (global_ns() - t0 > idleNs || spin > (idleNs >> 9) + 1024) {
+                        if (atomicExch(&ds->draining, 1u) == 0u)
+                            *(volatile uint32_t *)&status->exitReason = kExitIdle;
+                        break;
+                    }
+                    __nanosleep(1024);
+                }
+            }
+        }
+        go = __shfl_sync(dev::FULL_MASK, go, 0);
+        if (!go)
+            return;
+        t = __shfl_sync(dev::FULL_MASK, t, 0);
+        if (t < dT0 || t >= dEnd) {
+            // find the ticket's batch among the ring's descriptors: lane i
+            // looks at slot i
+            uint64_t t0 = 0, n = 0;
+            if (lane < kRing) {
+                // a slot the host is rewriting shows seq 0 or a different seq
+                // on the second read (the host clears seq, writes the fields,
+                // then stores the new seq): only a slot read whole counts
+                const uint64_t *sp = &ctrl->slot[lane].seq;
+                const uint64_t sq = ld_acquire_sys(sp);
+                const volatile uint64_t *w = reinterpret_cast<const volatile uint64_t *>(&ctrl->slot[lane]);
+                t0 = w[1];
+                const uint64_t c0 = w[2], c1 = w[3];
+                asm volatile("fence.acq_rel.sys;" ::: "memory");
+                const uint64_t sq2 = *(const volatile uint64_t *)sp;
+                n = (sq && sq == sq2) ? (c0 & 0xffffffffu) + (c0 >> 32) + (c1 >> 32) : 0; // scan + fold tickets
+            }
+            const uint32_t hit = __ballot_sync(dev::FULL_MASK, lane < kRing && n && t >= t0 && t < t0 + n);
+            if (!hit) { // published tickets always have a descriptor: stop rather than guess
+                if (lane == 0) {
+                    atomicExch(&ds->draining, 1u);
+                    *(volatile uint32_t *)&status->exitReason = kExitTimeout;
+                }
+                return;
+            }
+            slot = __ffs(hit) - 1;
+            dT0 = __shfl_sync(dev::FULL_MASK, t0, slot);
+            dEnd = dT0 + __shfl_sync(dev::FULL_MASK, n, slot);
+            word = 0;
+            if (lane < kDescWords) {
+                (void)ld_acquire_sys(&ctrl->published);
+                word = reinterpret_cast<const volatile uint64_t *>(&ctrl->slot[slot])[lane];
+            }
+        }
+        // the descriptor's fields, from the lanes holding them
+        BatchDesc d;
+        {
+            uint64_t *dp = reinterpret_cast<uint64_t *>(&d);
+#pragma unroll
+            for (int i = 0; i < kDescWords; ++i)
+                dp[i] = __shfl_sync(dev::FULL_MASK, word, i);
+        }
+        const uint64_t local = t - d.ticket0;
+        const uint64_t nScan = (uint64_t)d.nSingle + d.nJoint;
+        if (local == 0 && lane == 0)
+            *(volatile uint64_t *)&status->tFirst[slot] = global_ns();
+        if (local < nScan) {
+            if (local < d.nSingle) {
+                const WorkItem it = d.single[local];
+                serve_single_item<NB, K>(it, d.sv[it.view], seq, mask, d.sums, lane);
+            } else {
+                const WorkItem it = d.joint[local - d.nSingle];
+                serve_joint_item<NB>(it, d.jv[it.view], seq, mask, d.sums, lane);
+            }
+            __threadfence(); // every lane's summaries are visible before the count
+            __syncwarp();
+            if (lane == 0)
+                atomicAdd(&ds->scanDone[slot], 1ull);
+            continue;
+        }
+        // a fold ticket: wait (bounded) for the batch's scans
+        uint32_t ready = 1;
+        if (lane == 0) {
+            const uint64_t t0 = global_ns();
+            for (uint64_t spin = 0; *(volatile unsigned long long *)&ds->scanDone[slot] < nScan; ++spin) {
+                if (global_ns() - t0 > waitNs || spin > (waitNs >> 8) + 1024) {
+                    ready = 0;
+                    atomicExch(&ds->draining, 1u);
+                    *(volatile uint32_t *)&status->exitReason = kExitTimeout;
+                    break;
+                }
+                __nanosleep(256);
+            }
+        }
+        ready = __shfl_sync(dev::FULL_MASK, ready, 0);
+        if (!ready)
+            return;
+        __threadfence(); // the summaries counted above are read after the count
+        const uint64_t f0 = (local - nScan) * kFinPerTicket;
+        const uint64_t f1 = f0 + kFinPerTicket < d.nFin ? f0 + kFinPerTicket : (uint64_t)d.nFin;
+        for (uint64_t f = f0 + lane; f < f1; f += 32)
+            serve_fin_item(d.fin[f], d.sums, k, rows);
+        __threadfence_system(); // every lane's rows reach host memory before the batch is stamped done
+        __syncwarp();
+        if (lane == 0) {
+            if (atomicAdd(&ds->finDone[slot], 1ull) + 1 == d.nFinTickets) {
+                // the batch's last fold: its counters are free for the slot's next batch
+                ds->scanDone[slot] = 0;
+                ds->finDone[slot] = 0;
+                __threadfence_system();
+                *(volatile uint64_t *)&status->tDone[slot] = global_ns();
+                st_release_sys(&status->doneSeq[slot], d.seq);
+            }
+        }
     }
 }
 
@@ -325,10 +562,20 @@ struct Request {
     uint64_t planned = 0, rowOff = 0;
 };
 
+// An iteration's batch. In the persistent mode its states run Copying
+// (items on their way to the device) -> Published -> done (Idle); a batch
+// that was published when the kernel stopped goes back to Copying and is
+// published to the next launch.
+enum class BatchState { Idle, Copying, Published };
+
 struct Launch {
     std::vector<uint32_t> groups;       // groups used (claimed: inflight)
     std::vector<Request *> finishing;   // requests whose last windows ran here
     cudaEvent_t start = nullptr, stop = nullptr;
+    cudaEvent_t copied = nullptr;       // persistent mode: the items reached the device
+    BatchState state = BatchState::Idle;
+    uint64_t seq = 0;                   // persistent mode: batch number
+    uint32_t nSingle = 0, nJoint = 0, nFin = 0, replays = 0;
     WorkItem *hSingle = nullptr, *hJoint = nullptr, *dSingle = nullptr, *dJoint = nullptr;
     FinItem *hFin = nullptr, *dFin = nullptr;
     TableView *hSV = nullptr, *dSV = nullptr;
@@ -364,6 +611,21 @@ struct ibs_server {
     Launch launches[kDepth];
     int nextLaunch = 0;
     int sms = 148;
+    // the persistent launch (batched mode unless iteration_launches)
+    bool persistent = false;
+    cudaStream_t copy = nullptr;          // item uploads while the kernel runs
+    Ctrl *ctrl = nullptr;                 // pinned, mapped
+    Status *status = nullptr;             // pinned, mapped
+    Ctrl *dCtrl = nullptr;
+    Status *dStatus = nullptr;
+    DevState *ds = nullptr;
+    ibs_window *dRowsMapped = nullptr;    // device address of hRows
+    cudaEvent_t kernelEnd = nullptr;
+    bool kernelRunning = false;
+    int persistentGrid = 0;
+    uint64_t nextSeq = 1, published = 0;
+    uint64_t idleNs = 100000000ull, waitNs = 10000000000ull;
+    uint64_t busyLastEnd = 0;
     // request state
     std::mutex mu;
     std::condition_variable cv, doneCv;
@@ -488,14 +750,10 @@ ibs_request_result result_of(const Request &r, ibs_status status, double t)
 }
 
 // Completes launch L: its finishing requests' rows move to their results.
-void retire(ibs_server *s, Launch &L)
+// Bookkeeping of a finished launch or batch: its tables are released and
+// its finishing requests' rows move to their results.
+void complete(ibs_server *s, Launch &L)
 {
-    if (!L.active)
-        return;
-    cudaEventSynchronize(L.stop);
-    float ms = 0;
-    if (cudaEventElapsedTime(&ms, L.start, L.stop) == cudaSuccess)
-        s->st.busy_seconds += ms * 1e-3;
     const double t = s->now();
     std::lock_guard<std::mutex> lock(s->mu);
     for (uint32_t g : L.groups)
@@ -516,7 +774,188 @@ void retire(ibs_server *s, Launch &L)
     L.finishing.clear();
     L.groups.clear();
     L.active = false;
+    L.state = BatchState::Idle;
     s->doneCv.notify_all();
+}
+
+void set_fatal(ibs_server *s, const std::string &msg)
+{
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (s->fatal.empty())
+        s->fatal = msg;
+    s->doneCv.notify_all();
+}
+
+// Launches the persistent kernel over fresh device state; tickets count
+// from 0 again.
+bool start_kernel(ibs_server *s)
+{
+    s->ctrl->stop = 0;
+    s->status->exitReason = kExitNone;
+    memset(s->ctrl->slot, 0, sizeof(s->ctrl->slot)); // no descriptor of the last launch's ticket space survives
+    __atomic_store_n(&s->ctrl->published, 0ull, __ATOMIC_RELEASE);
+    s->published = 0;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    cudaError_t e = cudaMemsetAsync(s->ds, 0, sizeof(DevState), s->comp);
+    if (e == cudaSuccess) {
+        if (s->k == 25)
+            k_serve_persistent<kServeNB, 25><<<s->persistentGrid, 256, 0, s->comp>>>(
+                s->dCtrl, s->dStatus, s->ds, s->ref->dSeq, s->ref->dMask, (int)s->k, s->dRowsMapped, s->idleNs,
+                s->waitNs);
+        else if (s->k == 31)
+            k_serve_persistent<kServeNB, 31><<<s->persistentGrid, 256, 0, s->comp>>>(
+                s->dCtrl, s->dStatus, s->ds, s->ref->dSeq, s->ref->dMask, (int)s->k, s->dRowsMapped, s->idleNs,
+                s->waitNs);
+        else
+            k_serve_persistent<kServeNB, 0><<<s->persistentGrid, 256, 0, s->comp>>>(
+                s->dCtrl, s->dStatus, s->ds, s->ref->dSeq, s->ref->dMask, (int)s->k, s->dRowsMapped, s->idleNs,
+                s->waitNs);
+        IBS_LAUNCHED();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaEventRecord(s->kernelEnd, s->comp);
+    if (e != cudaSuccess) {
+        set_fatal(s, std::string("CUDA error in the persistent serving launch: ") + cudaGetErrorString(e));
+        return false;
+    }
+    s->kernelRunning = true;
+    s->st.persistent_launches++;
+    return true;
+}
+
+// Publishes batch L to the running kernel: its descriptor into its ring
+// slot, then the ticket count (release).
+void publish(ibs_server *s, Launch &L, int slot)
+{
+    BatchDesc d{};
+    d.seq = L.seq;
+    d.ticket0 = s->published;
+    d.nSingle = L.nSingle;
+    d.nJoint = L.nJoint;
+    d.nFin = L.nFin;
+    d.nFinTickets = std::max<uint32_t>(1, (L.nFin + kFinPerTicket - 1) / kFinPerTicket);
+    d.single = L.dSingle;
+    d.joint = L.dJoint;
+    d.fin = L.dFin;
+    d.sv = L.dSV;
+    d.jv = L.dJV;
+    d.sums = L.dSums;
+    // seq last: a warp reading the slot while it changes sees seq 0 or a
+    // changed seq and ignores it (the slot's previous batch is done, so no
+    // live ticket belongs to it)
+    BatchDesc *dst = &s->ctrl->slot[slot];
+    __atomic_store_n(&dst->seq, 0ull, __ATOMIC_SEQ_CST);
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    const uint64_t seqNo = d.seq;
+    d.seq = 0;
+    *dst = d;
+    __atomic_store_n(&dst->seq, seqNo, __ATOMIC_RELEASE);
+    s->published += (uint64_t)d.nSingle + d.nJoint + d.nFinTickets;
+    __atomic_store_n(&s->ctrl->published, s->published, __ATOMIC_RELEASE);
+    L.state = BatchState::Published;
+}
+
+// The persistent mode's housekeeping, called by the loop between
+// iterations: notices a stopped kernel (its unfinished batches go back to
+// be published again), completes batches the kernel stamped done, and
+// publishes copied batches in order, launching the kernel when needed.
+void pump(ibs_server *s)
+{
+    if (s->kernelRunning && cudaEventQuery(s->kernelEnd) == cudaSuccess) {
+        s->kernelRunning = false;
+        const uint32_t why = *(volatile uint32_t *)&s->status->exitReason;
+        if (why == kExitIdle)
+            s->st.idle_exits++;
+        else if (why == kExitTimeout)
+            s->st.wait_timeouts++;
+    }
+    // batches the kernel stamped done, completed in batch order: a request's
+    // rows can come from several batches, and it completes with the last
+    // one, so an earlier batch must be done before a later one completes
+    for (;;) {
+        Launch *first = nullptr;
+        int slot = -1;
+        for (int i = 0; i < kDepth; ++i) {
+            Launch &L = s->launches[i];
+            if (L.state == BatchState::Published && (!first || L.seq < first->seq)) {
+                first = &L;
+                slot = i;
+            }
+        }
+        if (!first || __atomic_load_n(&s->status->doneSeq[slot], __ATOMIC_ACQUIRE) != first->seq)
+            break;
+        const uint64_t a = *(volatile uint64_t *)&s->status->tFirst[slot];
+        const uint64_t b = *(volatile uint64_t *)&s->status->tDone[slot];
+        const uint64_t from = std::max(a, s->busyLastEnd);
+        if (b > from)
+            s->st.busy_seconds += (b - from) * 1e-9;
+        s->busyLastEnd = std::max(s->busyLastEnd, b);
+        complete(s, *first);
+    }
+    // published to a kernel that stopped before finishing them: publish again
+    if (!s->kernelRunning)
+        for (int i = 0; i < kDepth; ++i) {
+            Launch &L = s->launches[i];
+            if (L.state != BatchState::Published ||
+                __atomic_load_n(&s->status->doneSeq[i], __ATOMIC_ACQUIRE) == L.seq)
+                continue;
+            if (++L.replays > 3) {
+                set_fatal(s, "serving: a batch did not finish in four persistent launches (device wait timeout)");
+                return;
+            }
+            s->st.replays++;
+            L.state = BatchState::Copying; // its items are on the device already
+        }
+    // publication in batch order
+    for (;;) {
+        Launch *next = nullptr;
+        int slot = -1;
+        for (int i = 0; i < kDepth; ++i) {
+            Launch &L = s->launches[i];
+            if (L.state == BatchState::Copying && (!next || L.seq < next->seq)) {
+                next = &L;
+                slot = i;
+            }
+        }
+        if (!next || cudaEventQuery(next->copied) != cudaSuccess)
+            break;
+        if (!s->kernelRunning && !start_kernel(s))
+            break;
+        publish(s, *next, slot);
+    }
+}
+
+// Waits until launch or batch L has finished and completes it.
+void retire(ibs_server *s, Launch &L)
+{
+    if (!s->persistent) {
+        if (!L.active)
+            return;
+        cudaEventSynchronize(L.stop);
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, L.start, L.stop) == cudaSuccess)
+            s->st.busy_seconds += ms * 1e-3;
+        complete(s, L);
+        return;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    while (L.state != BatchState::Idle) {
+        pump(s);
+        if (L.state == BatchState::Idle)
+            break;
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            if (!s->fatal.empty())
+                break;
+        }
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(120)) {
+            set_fatal(s, "serving: a batch did not finish within 120 s");
+            break;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    L.active = false;
 }
 
 // Removes [lo, hi) (inside one of its intervals) from r's remaining windows.
@@ -768,6 +1207,37 @@ bool iterate(ibs_server *s)
             plan_group(s, L, g, view, demand[gi], limit, cap, used, nSingle, nJoint, nFin, s->serial);
         }
     }
+    if (s->persistent) {
+        // the items go up on the copy stream; the batch is published to the
+        // running kernel once they are there
+        cudaStream_t cs = s->copy;
+        if (nSV)
+            cudaMemcpyAsync(L.dSV, L.hSV, nSV * sizeof(TableView), cudaMemcpyHostToDevice, cs);
+        if (nJV)
+            cudaMemcpyAsync(L.dJV, L.hJV, nJV * sizeof(panel::View), cudaMemcpyHostToDevice, cs);
+        if (nSingle)
+            cudaMemcpyAsync(L.dSingle, L.hSingle, nSingle * sizeof(WorkItem), cudaMemcpyHostToDevice, cs);
+        if (nJoint)
+            cudaMemcpyAsync(L.dJoint, L.hJoint, nJoint * sizeof(WorkItem), cudaMemcpyHostToDevice, cs);
+        if (nFin)
+            cudaMemcpyAsync(L.dFin, L.hFin, nFin * sizeof(FinItem), cudaMemcpyHostToDevice, cs);
+        cudaEventRecord(L.copied, cs);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            set_fatal(s, std::string("CUDA error in serving upload: ") + cudaGetErrorString(e));
+        L.nSingle = nSingle;
+        L.nJoint = nJoint;
+        L.nFin = nFin;
+        L.replays = 0;
+        L.seq = s->nextSeq++;
+        L.state = BatchState::Copying;
+        L.active = true;
+        s->st.launches++;
+        s->st.spans += nSingle + nJoint;
+        s->nextLaunch = (s->nextLaunch + 1) % kDepth;
+        pump(s);
+        return true;
+    }
     cudaStream_t st = s->comp;
     if (nSV)
         cudaMemcpyAsync(L.dSV, L.hSV, nSV * sizeof(TableView), cudaMemcpyHostToDevice, st);
@@ -783,13 +1253,13 @@ bool iterate(ibs_server *s)
     if (nSingle) {
         const int grid = (int)std::min<uint64_t>((nSingle + 7) / 8, (uint64_t)s->sms * 8);
         if (s->k == 25)
-            k_serve_single<kNB, 25><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq,
+            k_serve_single<kServeNB, 25><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq,
                                                           s->ref->dMask, L.dSums);
         else if (s->k == 31)
-            k_serve_single<kNB, 31><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq,
+            k_serve_single<kServeNB, 31><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq,
                                                           s->ref->dMask, L.dSums);
         else
-            k_serve_single<kNB, 0><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq,
+            k_serve_single<kServeNB, 0><<<grid, 256, 0, st>>>(L.dSV, L.dSingle, nSingle, s->ref->dSeq,
                                                          s->ref->dMask, L.dSums);
         IBS_LAUNCHED();
     }
@@ -832,6 +1302,19 @@ void loop(ibs_server *s)
         }
         if (iterate(s))
             continue;
+        if (s->persistent) {
+            // nothing to plan: keep the running batches moving and wait
+            // briefly for new requests (a request arriving now is published
+            // next to the batches in flight)
+            pump(s);
+            bool any = false;
+            for (auto &L : s->launches)
+                any |= L.state != BatchState::Idle;
+            std::unique_lock<std::mutex> lock(s->mu);
+            s->cv.wait_for(lock, any ? std::chrono::microseconds(20) : std::chrono::microseconds(1000),
+                           [&] { return s->stop || !s->queue.empty(); });
+            continue;
+        }
         // nothing runnable: finish what is in flight, then wait for work
         bool any = false;
         for (auto &L : s->launches)
@@ -928,7 +1411,10 @@ extern "C" ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t
     if (opts) {
         s->tableFormat = opts->table_format;
         s->keysPerBucket = opts->keys_per_bucket;
+        if (opts->idle_exit_us)
+            s->idleNs = (uint64_t)opts->idle_exit_us * 1000;
     }
+    s->persistent = !s->serial && !(opts && opts->iteration_launches);
     cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
     size_t fr = 0, tot = 0;
     IBS_CUDA(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
@@ -941,9 +1427,30 @@ extern "C" ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t
     IBS_CUDA(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking), "stream create");
     IBS_CUDA(cudaMalloc(&s->dRows, kRowPool * sizeof(ibs_window)), "row pool");
     IBS_CUDA(cudaMallocHost(&s->hRows, kRowPool * sizeof(ibs_window)), "pinned row pool");
+    IBS_CUDA(cudaHostGetDevicePointer(&s->dRowsMapped, s->hRows, 0), "mapped row pool");
+    if (s->persistent) {
+        IBS_CUDA(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking), "stream create");
+        IBS_CUDA(cudaHostAlloc(&s->ctrl, sizeof(Ctrl), cudaHostAllocMapped), "persistent control block");
+        IBS_CUDA(cudaHostAlloc(&s->status, sizeof(Status), cudaHostAllocMapped), "persistent status block");
+        memset(s->ctrl, 0, sizeof(Ctrl));
+        memset(s->status, 0, sizeof(Status));
+        IBS_CUDA(cudaHostGetDevicePointer(&s->dCtrl, s->ctrl, 0), "mapped control block");
+        IBS_CUDA(cudaHostGetDevicePointer(&s->dStatus, s->status, 0), "mapped status block");
+        IBS_CUDA(cudaMalloc(&s->ds, sizeof(DevState)), "persistent state");
+        IBS_CUDA(cudaEventCreateWithFlags(&s->kernelEnd, cudaEventDisableTiming), "event create");
+        int perSm = 0;
+        if (s->k == 25)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_serve_persistent<kServeNB, 25>, 256, 0);
+        else if (s->k == 31)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_serve_persistent<kServeNB, 31>, 256, 0);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_serve_persistent<kServeNB, 0>, 256, 0);
+        s->persistentGrid = s->sms * std::max(1, perSm);
+    }
     for (auto &L : s->launches) {
         IBS_CUDA(cudaEventCreate(&L.start), "event create");
         IBS_CUDA(cudaEventCreate(&L.stop), "event create");
+        IBS_CUDA(cudaEventCreateWithFlags(&L.copied, cudaEventDisableTiming), "event create");
         IBS_CUDA(cudaMallocHost(&L.hSingle, kSumCap * sizeof(WorkItem)), "pinned staging");
         IBS_CUDA(cudaMallocHost(&L.hJoint, kSumCap * sizeof(WorkItem)), "pinned staging");
         IBS_CUDA(cudaMallocHost(&L.hFin, kFinCap * sizeof(FinItem)), "pinned staging");
@@ -1190,6 +1697,8 @@ extern "C" void ibs_server_close(ibs_server *s)
         s->worker.join();
     {
         DeviceGuard guard(s->device);
+        if (s->ctrl) // the persistent kernel's waiting warps see the stop and return
+            __atomic_store_n(&s->ctrl->stop, 1u, __ATOMIC_RELEASE);
         cudaStreamSynchronize(s->comp);
         cudaStreamSynchronize(s->side);
         for (auto &g : s->groups) {
@@ -1220,6 +1729,17 @@ extern "C" void ibs_server_close(ibs_server *s)
         }
         cudaFree(s->dRows);
         cudaFreeHost(s->hRows);
+        if (s->copy) {
+            cudaStreamSynchronize(s->copy);
+            cudaStreamDestroy(s->copy);
+        }
+        for (auto &L : s->launches)
+            cudaEventDestroy(L.copied);
+        cudaFreeHost(s->ctrl);
+        cudaFreeHost(s->status);
+        cudaFree(s->ds);
+        if (s->kernelEnd)
+            cudaEventDestroy(s->kernelEnd);
         cudaStreamDestroy(s->comp);
         cudaStreamDestroy(s->side);
     }

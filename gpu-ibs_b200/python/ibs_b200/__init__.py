@@ -52,7 +52,8 @@ vp = C.c_void_p
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("memory_budget", C.c_uint64), ("max_spans_per_launch", C.c_uint32),
                 ("min_spans_per_request", C.c_uint32), ("one_request_per_launch", C.c_uint32),
-                ("table_format", C.c_uint32), ("keys_per_bucket", C.c_double), ("reserved", C.c_uint32 * 2)]
+                ("table_format", C.c_uint32), ("keys_per_bucket", C.c_double),
+                ("iteration_launches", C.c_uint32), ("idle_exit_us", C.c_uint32)]
 
 
 class RequestResult(C.Structure):
@@ -65,7 +66,8 @@ class ServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "launches", "spans", "probes", "reloads",
                                           "reload_bytes", "evictions", "resident_bytes", "resident_tables")] + \
                [(n, C.c_double) for n in ("busy_seconds", "latency_p50", "latency_p99", "latency_max")] + \
-               [(n, C.c_uint64) for n in ("failed", "queued", "running", "scanned", "sample_probes")]
+               [(n, C.c_uint64) for n in ("failed", "queued", "running", "scanned", "sample_probes",
+                                          "persistent_launches", "idle_exits", "wait_timeouts", "replays")]
 
 
 class Tuning(C.Structure):
@@ -627,10 +629,12 @@ class Server:
 
     def __init__(self, ref: Reference, W: int, k: int, memory_budget: int = 0, max_spans_per_launch: int = 0,
                  min_spans_per_request: int = 0, device: int = 0, one_request_per_launch: bool = False,
-                 table_format: int = 0, keys_per_bucket: float = 0.0):
+                 table_format: int = 0, keys_per_bucket: float = 0.0, iteration_launches: bool = False,
+                 idle_exit_us: int = 0):
         self.ref = ref
         opts = ServerOpts(device, memory_budget, max_spans_per_launch, min_spans_per_request,
-                          int(one_request_per_launch), table_format, keys_per_bucket)
+                          int(one_request_per_launch), table_format, keys_per_bucket, int(iteration_launches),
+                          idle_exit_us)
         h = vp()
         _check(_ibs_srv_create(ref.handle, W, k, C.byref(opts), C.byref(h)))
         self._h = h.value

@@ -266,7 +266,19 @@ void ibs_panel_table_close(ibs_panel_table *p);
  * request's rows are exactly the rows of the same windows in a full scan of
  * its sample (alone or in any mix).
  *
- * The server owns a background thread; submit/poll are thread-safe. */
+ * The server owns a background thread; submit/poll are thread-safe.
+ *
+ * Batched mode feeds ONE persistent kernel: the loop publishes each
+ * iteration's work (span items over the tables, then the rows to fold) as a
+ * batch into a ring in pinned host memory; the resident kernel's warps claim
+ * the work in order, fold rows straight into pinned host memory and stamp
+ * each batch done, so requests that arrive while others run are packed into
+ * the same launch. Every device wait is bounded: without new work for
+ * idle_exit_us the kernel ends (the next request launches it again), and a
+ * fold that waits too long for its batch's scans ends it with a timeout
+ * (counted in ibs_server_stats; unfinished batches are published to the
+ * next launch). One request per launch (the plain path) launches kernels
+ * per request instead. */
 typedef struct ibs_server ibs_server;
 
 typedef struct ibs_server_opts {
@@ -279,7 +291,10 @@ typedef struct ibs_server_opts {
                                    0 = the tuned default (ibs_tuning.table_format: minimizer lines for
                                    large tables), else as ibs_table_opts.force_format */
     double keys_per_bucket;     /* load of those tables (0 = the library default) */
-    uint32_t reserved[2];
+    uint32_t iteration_launches; /* batched mode: 1 = launch kernels per loop iteration instead of
+                                    feeding one persistent launch */
+    uint32_t idle_exit_us;      /* the persistent launch ends after this long without new work
+                                   (0 = 100 ms); the next request launches it again */
 } ibs_server_opts;
 
 typedef struct ibs_request_result {
@@ -304,6 +319,10 @@ typedef struct ibs_server_stats {
     uint64_t sample_probes;           /* positions x samples the scans answered: a joint-table scan of a
                                          window for three requesting samples counts its positions three
                                          times (two requests of one sample count once) */
+    uint64_t persistent_launches;     /* launches of the persistent kernel (batched mode) */
+    uint64_t idle_exits;              /* ... that ended after idle_exit_us without new work */
+    uint64_t wait_timeouts;           /* ... that ended because a bounded device wait ran out */
+    uint64_t replays;                 /* batches published again after their launch ended early */
 } ibs_server_stats;
 
 ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t k, const ibs_server_opts *opts,

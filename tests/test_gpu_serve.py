@@ -45,11 +45,13 @@ def expected(world, r):
     return rows[a:a + r["n_windows"]]
 
 
-def make_server(world, budget_tables=2.5, table_format=0, serial=False):
+def make_server(world, budget_tables=2.5, table_format=0, serial=False, iteration_launches=False,
+                idle_exit_us=0):
     sizes = [ib.table_bytes_for(len(c), K, force_format=table_format) for c in world["samples"]]
     budget = int(max(sizes) * budget_tables)
     srv = ib.Server(world["ref"], W, K, memory_budget=budget, max_spans_per_launch=512, min_spans_per_request=8,
-                    table_format=table_format, one_request_per_launch=serial)
+                    table_format=table_format, one_request_per_launch=serial,
+                    iteration_launches=iteration_launches, idle_exit_us=idle_exit_us)
     ids = [srv.add_codes(c, len(c), on_device=False) for c in world["samples"]]
     assert ids == list(range(len(world["samples"])))
     return srv
@@ -80,8 +82,11 @@ def test_requests_alone_equal_full_scan_rows(world):
     srv.close()
 
 
-def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world):
-    srv = make_server(world, budget_tables=2.2)
+@pytest.mark.parametrize("iteration_launches", [False, True])
+def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world, iteration_launches):
+    """Batched serving, through the persistent launch (default) and through
+    one launch per loop iteration."""
+    srv = make_server(world, budget_tables=2.2, iteration_launches=iteration_launches)
     reqs = random_requests(world, 300, 2) + [(s, 0, 0, 0) for s in range(6)]  # whole-contig requests too
     done = []
 
@@ -105,6 +110,33 @@ def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world):
     assert st["completed"] == len(reqs)
     assert st["evictions"] > 0 and st["reloads"] > 0, st
     assert st["latency_p99"] >= st["latency_p50"] > 0
+    if iteration_launches:
+        assert st["persistent_launches"] == 0
+    else:
+        # the whole burst went through a few resident launches, not one per iteration
+        assert 1 <= st["persistent_launches"] < st["launches"], st
+        assert st["wait_timeouts"] == 0, st
+    srv.close()
+
+
+def test_persistent_launch_ends_when_idle_and_comes_back(world):
+    """The persistent kernel's wait for new work is bounded: with no request
+    for longer than idle_exit_us the kernel ends by itself (the bound runs
+    out and the kernel reports it), and the next request launches it again;
+    results stay exact across the restarts."""
+    srv = make_server(world, idle_exit_us=2000)
+    reqs = random_requests(world, 6, 21)
+    for i, req in enumerate(reqs):
+        srv.submit(*req)
+        got = srv.poll(1, timeout_ms=60_000)
+        assert len(got) == 1 and got[0]["status"] == 0, (req, srv.stats())
+        assert np.array_equal(got[0]["rows"], expected(world, got[0])), req
+        time.sleep(0.05)  # 25x the idle limit: the kernel has ended
+        st = srv.stats()
+        assert st["idle_exits"] >= i + 1, st
+    st = srv.stats()
+    assert st["persistent_launches"] >= len(reqs), st
+    assert st["wait_timeouts"] == 0, st
     srv.close()
 
 
