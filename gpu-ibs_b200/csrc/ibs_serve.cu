@@ -316,8 +316,12 @@ struct Status {                    // pinned host memory, written by the kernel
 struct DevState {                  // device memory, zeroed before each launch
     unsigned long long ticket;
     unsigned long long scanDone[kRing], finDone[kRing];
+    unsigned long long published;  // device copy of the host's count (one warp at a time reads the host's)
     unsigned int draining;
+    unsigned int polling;          // held by the warp reading the host's count
 };
+
+
 
 __device__ __forceinline__ uint64_t ld_acquire_sys(const uint64_t *p)
 {
@@ -336,6 +340,23 @@ __device__ __forceinline__ uint64_t global_ns()
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// The published ticket count as this warp may rely on it: the device copy,
+// refreshed from pinned host memory by one warp at a time (the waiting warps
+// of a whole grid would otherwise flood the host link with reads).
+__device__ __forceinline__ uint64_t published_count(const Ctrl *ctrl, DevState *ds)
+{
+    uint64_t v = *(volatile unsigned long long *)&ds->published;
+    if (atomicCAS(&ds->polling, 0u, 1u) == 0u) {
+        const uint64_t h = ld_acquire_sys(&ctrl->published);
+        __threadfence_system();
+        atomicMax(&ds->published, (unsigned long long)h);
+        __threadfence();
+        atomicExch(&ds->polling, 0u);
+        v = h > v ? h : v;
+    }
+    return v;
 }
 
 template <int NB, uint32_t K>
@@ -359,18 +380,18 @@ __global__ void __launch_bounds__(256, 4) k_serve_persistent(const Ctrl *ctrl, S
                 // wait (bounded) until it is published
                 const uint64_t t0 = global_ns();
                 for (uint64_t spin = 0;; ++spin) {
-                    if (ld_acquire_sys(&ctrl->published) > t) {
+                    if (published_count(ctrl, ds) > t) {
                         go = 1;
                         break;
                     }
                     if (*(volatile unsigned int *)&ds->draining || *(volatile const uint32_t *)&ctrl->stop)
                         break;
-                    if (global_ns() - t0 > idleNs || spin > (idleNs >> 9) + 1024) {
+                    if (global_ns() - t0 > idleNs || spin > (idleNs >> 8) + 1024) {
                         if (atomicExch(&ds->draining, 1u) == 0u)
                             *(volatile uint32_t *)&status->exitReason = kExitIdle;
                         break;
                     }
-                    __nanosleep(1024);
+                    __nanosleep(spin < 64 ? 256 : 2048);
                 }
             }
         }
@@ -380,22 +401,31 @@ __global__ void __launch_bounds__(256, 4) k_serve_persistent(const Ctrl *ctrl, S
         t = __shfl_sync(dev::FULL_MASK, t, 0);
         if (t < dT0 || t >= dEnd) {
             // find the ticket's batch among the ring's descriptors: lane i
-            // looks at slot i
+            // looks at slot i; a descriptor read while the host rewrites it
+            // is read again (a bounded number of times)
+            __threadfence_system();
+            uint32_t hit = 0;
             uint64_t t0 = 0, n = 0;
-            if (lane < kRing) {
-                // a slot the host is rewriting shows seq 0 or a different seq
-                // on the second read (the host clears seq, writes the fields,
-                // then stores the new seq): only a slot read whole counts
-                const uint64_t *sp = &ctrl->slot[lane].seq;
-                const uint64_t sq = ld_acquire_sys(sp);
-                const volatile uint64_t *w = reinterpret_cast<const volatile uint64_t *>(&ctrl->slot[lane]);
-                t0 = w[1];
-                const uint64_t c0 = w[2], c1 = w[3];
-                asm volatile("fence.acq_rel.sys;" ::: "memory");
-                const uint64_t sq2 = *(const volatile uint64_t *)sp;
-                n = (sq && sq == sq2) ? (c0 & 0xffffffffu) + (c0 >> 32) + (c1 >> 32) : 0; // scan + fold tickets
+            for (int attempt = 0; attempt < 4096 && !hit; ++attempt) {
+                if (attempt)
+                    __nanosleep(256);
+                t0 = 0;
+                n = 0;
+                if (lane < kRing) {
+                    // a slot the host is rewriting shows seq 0 or a different seq
+                    // on the second read (the host clears seq, writes the fields,
+                    // then stores the new seq): only a slot read whole counts
+                    const uint64_t *sp = &ctrl->slot[lane].seq;
+                    const uint64_t sq = ld_acquire_sys(sp);
+                    const volatile uint64_t *w = reinterpret_cast<const volatile uint64_t *>(&ctrl->slot[lane]);
+                    t0 = w[1];
+                    const uint64_t c0 = w[2], c1 = w[3];
+                    asm volatile("fence.acq_rel.sys;" ::: "memory");
+                    const uint64_t sq2 = *(const volatile uint64_t *)sp;
+                    n = (sq && sq == sq2) ? (c0 & 0xffffffffu) + (c0 >> 32) + (c1 >> 32) : 0; // scan + fold tickets
+                }
+                hit = __ballot_sync(dev::FULL_MASK, lane < kRing && n && t >= t0 && t < t0 + n);
             }
-            const uint32_t hit = __ballot_sync(dev::FULL_MASK, lane < kRing && n && t >= t0 && t < t0 + n);
             if (!hit) { // published tickets always have a descriptor: stop rather than guess
                 if (lane == 0) {
                     atomicExch(&ds->draining, 1u);

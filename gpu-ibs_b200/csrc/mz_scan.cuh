@@ -55,9 +55,14 @@ __device__ __forceinline__ MzPos mz_pos(const uint64_t *__restrict__ seq, const 
     r.code = r.isFwd ? fwd : rc;
     const uint64_t f = y >> (64 - 2 * m);
     const uint64_t mr = ~x & key_mask(2 * m);
-    const uint64_t c = f < mr ? f : mr;
+    const bool fLess = f < mr;
+    const uint64_t c = fLess ? f : mr;
     const uint64_t lh = mz::line_hash(c, m);
-    r.gs = lh | (f > mr ? 1ull << 62 : 0ull) | (mr > f ? 1ull << 63 : 0ull);
+    // an m-mer of odd length is never its own reverse complement (its middle
+    // base would be its own complement), so one comparison gives both bits
+    const uint64_t orient = (m & 1) ? (fLess ? 1ull << 63 : 1ull << 62)
+                                    : ((f > mr ? 1ull << 62 : 0ull) | (fLess ? 1ull << 63 : 0ull));
+    r.gs = lh | orient;
     r.key = mz::rank_key_of(lh);
     return r;
 }
