@@ -78,7 +78,10 @@ IBS_HD uint64_t mulhi64(uint64_t a, uint64_t b)
 //   linear probing over buckets, EMPTY = ~0 (never a canonical code: the
 //   all-T k-mer's reverse complement, all-A, is smaller).
 // ---------------------------------------------------------------------------
-enum : uint32_t { FMT_B8X32 = 1, FMT_B6X40 = 2, FMT_PANEL = 3, FMT_MZ8 = 4, FMT_AUTO_HASH = 5, FMT_MZ6 = 6 };
+enum : uint32_t {
+    FMT_B8X32 = 1, FMT_B6X40 = 2, FMT_PANEL = 3, FMT_MZ8 = 4, FMT_AUTO_HASH = 5, FMT_MZ6 = 6,
+    FMT_PANEL_MZ = 7 // joint table: P5x48 sectors on minimizer lines (panel_core.cuh)
+};
 // Minimizer-line tables: B8x32 sectors (31-bit slot values) or B6x40 sectors
 // (40-bit slot values, for larger k).
 IBS_HD bool is_mz(uint32_t fmt) { return fmt == FMT_MZ8 || fmt == FMT_MZ6; }

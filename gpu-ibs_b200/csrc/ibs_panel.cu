@@ -1,6 +1,7 @@
 // Panel scan over the joint table of panel_core.cuh: build (two-phase
 // insertion per sample), the persistent span kernel and its CUDA graph, and
 // the ibs_panel_table_* entry points.
+#include "mz_scan.cuh"
 #include "panel_core.cuh"
 #include "scan_device.cuh"
 
@@ -12,53 +13,101 @@
 namespace ibs {
 namespace panel {
 
+// Default load of joint minimizer-line tables: keys per 5-slot sector (the
+// keys of one minimizer crowd its line, so the load stays below the hash
+// sectors' 3)
+constexpr double kPmKeysPerSector = 2.0;
 constexpr uint64_t kBuildChunk = 1ull << 27; // keys per build step (1 GiB of scratch each way)
+
+// Slot of fingerprint fp among sector w's first count slots, or -1.
+__device__ __forceinline__ int find_slot(const uint32_t *w, uint32_t fp)
+{
+    const uint32_t cnt = (w[7] >> 16) & 0xff;
+    int slot = -1;
+    for (uint32_t j = 0; j < cnt && j < kSlots; ++j)
+        if (w[j] == fp)
+            slot = (int)j;
+    return slot;
+}
+
+// ORs `bit` into the stash entry of `code`; false when the stash lacks it.
+__device__ __forceinline__ bool stash_or(const View &t, unsigned long long *stashWords, uint64_t code,
+                                         uint32_t bit)
+{
+    uint64_t b = stash_home(code, t.stashBuckets);
+    for (uint64_t s = 0; s < t.stashBuckets; ++s) {
+        unsigned long long *e = stashWords + 4 * b;
+        if (e[0] == code) {
+            atomicOr(e + 1, 1ull << bit);
+            return true;
+        }
+        if (e[2] == code) {
+            atomicOr(e + 3, 1ull << bit);
+            return true;
+        }
+        if (e[0] == kStashEmpty || e[2] == kStashEmpty)
+            return false;
+        b = (b + 1) & (t.stashBuckets - 1);
+    }
+    return false;
+}
+
+// Claims a free slot of sector w (bumps its count byte below kSlots) and
+// fills it with fp and the sample bit; false when the sector is full.
+__device__ __forceinline__ bool claim_slot(uint32_t *w, uint32_t fp, uint32_t bit)
+{
+    uint32_t old = w[7], slot = kSlots;
+    for (int tries = 0; tries < 1 << 20; ++tries) {
+        const uint32_t cnt = (old >> 16) & 0xff;
+        if (cnt >= kSlots)
+            break;
+        const uint32_t seen = atomicCAS(w + 7, old, old + (1u << 16));
+        if (seen == old) {
+            slot = cnt;
+            break;
+        }
+        old = seen;
+    }
+    if (slot >= kSlots)
+        return false;
+    w[slot] = fp;
+    atomicOr(w + 5 + slot / 2, (1u << bit) << (16 * (slot & 1)));
+    return true;
+}
 
 // ---- build: phase A finds keys already present and ORs in the sample bit;
 // phase B inserts the rest. Within one sample the keys are unique, so no
-// lookup races with an insert of the same key.
+// lookup races with an insert of the same key. A key is looked for where
+// phase B would have put it: its home sector, then (PM, flagged) the home's
+// partner sector, then (flagged) the stash.
 __global__ void k_find(View t, uint32_t *words, unsigned long long *stashWords, const uint64_t *codes,
                        uint64_t n, uint32_t bit, uint64_t *pending, unsigned long long *nPending)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t iters = (n + stride - 1) / stride;
+    const bool pm = t.g.format == FMT_PANEL_MZ;
     for (uint64_t it = 0; it < iters; ++it) {
         const uint64_t i = it * stride + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
         bool miss = false;
         uint64_t code = 0;
         if (i < n) {
             code = codes[i];
-            const uint64_t h = perm_hash(code, t.g.bits);
-            const uint64_t r = bucket_of(h, t.g);
-            const uint32_t fp = (uint32_t)fp_of(h, t.g);
+            uint64_t r;
+            uint32_t fp;
+            joint_place(t, code, r, fp);
             uint32_t *w = words + 8 * r;
-            const uint32_t cnt = (w[7] >> 16) & 0xff;
-            int slot = -1;
-            for (uint32_t j = 0; j < cnt && j < kSlots; ++j)
-                if (w[j] == fp)
-                    slot = (int)j;
-            if (slot >= 0) {
-                atomicOr(w + 5 + slot / 2, (1u << bit) << (16 * (slot & 1)));
-            } else if ((w[7] >> 24) & 1u) {
-                // in the stash?
-                uint64_t b = stash_home(code, t.stashBuckets);
-                bool found = false;
-                for (uint64_t s = 0; s < t.stashBuckets && !found; ++s) {
-                    unsigned long long *e = stashWords + 4 * b;
-                    if (e[0] == code) {
-                        atomicOr(e + 1, 1ull << bit);
-                        found = true;
-                    } else if (e[2] == code) {
-                        atomicOr(e + 3, 1ull << bit);
-                        found = true;
-                    } else if (e[0] == kStashEmpty || e[2] == kStashEmpty)
-                        break;
-                    b = (b + 1) & (t.stashBuckets - 1);
-                }
-                miss = !found;
-            } else
-                miss = true;
+            const uint32_t flags = w[7];
+            int slot = find_slot(w, fp);
+            uint32_t *where = w;
+            if (slot < 0 && pm && (flags & kPartnerFlag)) {
+                where = words + 8 * (r ^ 1);
+                slot = find_slot(where, fp);
+            }
+            if (slot >= 0)
+                atomicOr(where + 5 + slot / 2, (1u << bit) << (16 * (slot & 1)));
+            else
+                miss = !((flags & kStashFlag) && stash_or(t, stashWords, code, bit));
         }
         const uint32_t ballot = __ballot_sync(0xffffffffu, miss);
         if (!ballot)
@@ -75,32 +124,22 @@ __global__ void k_find(View t, uint32_t *words, unsigned long long *stashWords, 
 __global__ void k_insert(View t, uint32_t *words, unsigned long long *stashWords, const uint64_t *codes,
                          uint64_t n, uint32_t bit, uint64_t *failed, unsigned long long *nFailed)
 {
+    const bool pm = t.g.format == FMT_PANEL_MZ;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t code = codes[i];
-        const uint64_t h = perm_hash(code, t.g.bits);
-        const uint64_t r = bucket_of(h, t.g);
-        const uint32_t fp = (uint32_t)fp_of(h, t.g);
+        uint64_t r;
+        uint32_t fp;
+        joint_place(t, code, r, fp);
         uint32_t *w = words + 8 * r;
-        // claim a slot: bump the count byte while it is below kSlots
-        uint32_t old = w[7], slot = kSlots;
-        for (int tries = 0; tries < 1 << 20; ++tries) {
-            const uint32_t cnt = (old >> 16) & 0xff;
-            if (cnt >= kSlots)
-                break;
-            const uint32_t seen = atomicCAS(w + 7, old, old + (1u << 16));
-            if (seen == old) {
-                slot = cnt;
-                break;
-            }
-            old = seen;
-        }
-        if (slot < kSlots) {
-            w[slot] = fp;
-            atomicOr(w + 5 + slot / 2, (1u << bit) << (16 * (slot & 1)));
+        if (claim_slot(w, fp, bit))
             continue;
+        if (pm) { // the partner sector of the same line, flagged on the home sector
+            atomicOr(w + 7, kPartnerFlag);
+            if (claim_slot(words + 8 * (r ^ 1), fp, bit))
+                continue;
         }
-        atomicOr(w + 7, 1u << 24); // overflow flag
+        atomicOr(w + 7, kStashFlag);
         uint64_t b = stash_home(code, t.stashBuckets);
         bool placed = false;
         for (uint64_t s = 0; s < t.stashBuckets && !placed; ++s) {
@@ -155,7 +194,7 @@ __global__ void k_stash_move(const ulonglong2 *old, uint64_t oldEntries, unsigne
 // one range.
 enum : int { kScan = 0, kMaskPass = 1, kStats = 2 };
 
-template <int NB, int MODE>
+template <int NB, int MODE, bool PM>
 __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__restrict__ seq,
                                                      const uint64_t *__restrict__ mask,
                                                      const WinDesc *__restrict__ win,
@@ -166,10 +205,14 @@ __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__r
                                                      SegStats *__restrict__ out, uint16_t *__restrict__ masks,
                                                      uint64_t bLo, uint64_t bHi, bool firstPass)
 {
+    // PM tables locate a k-mer through its minimizer (one block of m-mers
+    // read ahead); the statistics pass only needs each position's validity
+    constexpr bool kMz = PM && MODE != kStats;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t k = t.g.k;
     const uint64_t kmask = key_mask(2 * k);
     const uint64_t kbits = (1ull << k) - 1;
+    const uint32_t w = kMz ? mz::w_of(k) : 1, m = kMz ? mz::m_of(k) : 0;
     for (;;) {
         unsigned long long s = 0;
         if (lane == 0)
@@ -191,26 +234,53 @@ __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__r
         const uint32_t p1 = min(p0 + spanLen, nPos);
         uint16_t *spanMasks = masks + s * spanLen - p0; // position q of the span at spanMasks[q]
         SegStats acc = seg_empty(); // lane j < nSamples: sample j
+        // PM: the last m-mer start the window's k-mers use; lanes past the
+        // span read up to it (inside the window's bases) and are masked out
+        const uint32_t lastM = nPos - 1 + (w - 1);
+        dev::MzPos next;
+        if constexpr (kMz)
+            next = dev::mz_pos(seq, mask, base + min(p0 + lane, lastM), k, m);
         for (uint32_t p = p0; p < p1; p += 32 * NB) {
             uint4 v0[NB], v1[NB];
-            uint64_t code[NB];
+            uint64_t code[NB], rr[NB];
             uint32_t fp[NB];
             bool valid[NB], mine[NB];
+            if constexpr (kMz) {
+                dev::MzPos ps[NB + 1];
+                ps[0] = next;
+#pragma unroll
+                for (int b = 1; b <= NB; ++b)
+                    ps[b] = dev::mz_pos(seq, mask, base + min(p + 32 * b + lane, lastM), k, m);
+                next = ps[NB];
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    const uint32_t q = p + 32 * b + lane;
+                    valid[b] = q < p1 && ps[b].acgt;
+                    uint64_t slot;
+                    dev::mz_locate_lane(ps[b], ps[b + 1], lane, k, w, t.g.nBuckets, t.g.fpBits, rr[b], slot);
+                    fp[b] = (uint32_t)slot;
+                    code[b] = ps[b].code;
+                }
+            } else {
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    const uint32_t q = p + 32 * b + lane;
+                    const bool inSpan = q < p1;
+                    const uint64_t G = base + (inSpan ? q : p0);
+                    bool acgt;
+                    code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
+                    valid[b] = inSpan && acgt;
+                    const uint64_t h = perm_hash(code[b], t.g.bits);
+                    rr[b] = bucket_of(h, t.g);
+                    fp[b] = (uint32_t)fp_of(h, t.g);
+                }
+            }
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
-                const uint32_t q = p + 32 * b + lane;
-                const bool inSpan = q < p1;
-                const uint64_t G = base + (inSpan ? q : p0);
-                bool acgt;
-                code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
-                valid[b] = inSpan && acgt;
-                const uint64_t h = perm_hash(code[b], t.g.bits);
-                const uint64_t r = bucket_of(h, t.g);
-                fp[b] = (uint32_t)fp_of(h, t.g);
-                mine[b] = valid[b] && (MODE != kMaskPass || (r >= bLo && r < bHi));
+                mine[b] = valid[b] && (MODE != kMaskPass || (rr[b] >= bLo && rr[b] < bHi));
                 if (MODE != kStats && mine[b]) {
-                    v0[b] = __ldg(t.buckets + 2 * r);
-                    v1[b] = __ldg(t.buckets + 2 * r + 1);
+                    v0[b] = __ldg(t.buckets + 2 * rr[b]);
+                    v1[b] = __ldg(t.buckets + 2 * rr[b] + 1);
                 } else {
                     v0[b] = make_uint4(0, 0, 0, 0);
                     v1[b] = make_uint4(0, 0, 0, 0);
@@ -224,9 +294,13 @@ __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__r
                     if (valid[b])
                         m = spanMasks[q];
                 } else if (mine[b]) {
-                    m = bucket_mask(v0[b], v1[b], fp[b]);
-                    if (m & 0x80000000u)
-                        m = stash_mask(t, code[b]);
+                    if constexpr (kMz) {
+                        m = pm_mask(t, v0[b], v1[b], rr[b], fp[b], code[b]);
+                    } else {
+                        m = bucket_mask(v0[b], v1[b], fp[b]);
+                        if (m & 0x80000000u)
+                            m = stash_mask(t, code[b]);
+                    }
                 }
                 if (MODE == kMaskPass) {
                     if (q < p1 && (firstPass || m))
@@ -352,15 +426,43 @@ extern "C" ibs_status ibs_panel_table_create(uint32_t k, uint64_t expected_keys,
     TableGeom &g = p->geom;
     g.k = k;
     g.bits = 2 * k;
-    g.format = 3;
-    const double lam = (opts && opts->keys_per_bucket > 0) ? opts->keys_per_bucket : tuning().panel_keys_per_bucket;
-    uint64_t nb = (uint64_t)((double)expected_keys / lam) + 1;
-    const uint64_t minN = g.bits > 32 ? (1ull << (g.bits - 32)) : 1;
-    nb = std::max(nb, minN);
-    if (g.bits < 64)
-        nb = std::min<uint64_t>(nb, 1ull << g.bits);
-    g.nBuckets = nb;
-    g.fpBits = (uint32_t)std::max<int>(1, (int)g.bits - (int)(63 - __builtin_clzll(nb)));
+    uint32_t fmt = opts ? opts->force_format : 0;
+    if (fmt != 0 && fmt != FMT_PANEL && fmt != FMT_PANEL_MZ) {
+        set_error("ibs_panel_table_create: joint tables are format 3 (hash sectors) or 7 (minimizer lines)");
+        return IBS_ERR_ARG;
+    }
+    if (fmt == FMT_PANEL_MZ && (k < 16 || k > 27)) {
+        set_error("joint minimizer-line tables (format 7) need 16 <= k <= 27");
+        return IBS_ERR_UNSUPPORTED;
+    }
+    // minimizer lines: 32-bit slot values need at least 2^(2k-28) lines
+    const double lamPm = (opts && opts->keys_per_bucket > 0) ? opts->keys_per_bucket : kPmKeysPerSector;
+    const uint64_t pmMinLines = 1ull << std::max<int>(0, 2 * (int)k - 28);
+    const uint64_t pmLines = (uint64_t)((double)expected_keys / lamPm / mz::kSectorsPerLine) + 1;
+    if (fmt == 0 && k >= 16 && k <= 27 && pmLines >= pmMinLines && pmLines < (1ull << 31))
+        fmt = FMT_PANEL_MZ; // the default where its minimum size does not oversize the table
+    if (fmt == 0)
+        fmt = FMT_PANEL;
+    g.format = fmt;
+    uint64_t nb;
+    double lam;
+    if (fmt == FMT_PANEL_MZ) {
+        lam = lamPm;
+        const uint64_t nLines = std::min<uint64_t>(std::max(pmLines, pmMinLines), (1ull << 31) - 1);
+        nb = nLines * mz::kSectorsPerLine;
+        g.nBuckets = nb;
+        g.fpBits = 2 * mz::m_of(k) - (uint32_t)(63 - __builtin_clzll(nLines));
+    } else {
+        lam = (opts && opts->keys_per_bucket > 0) ? opts->keys_per_bucket : tuning().panel_keys_per_bucket;
+        nb = (uint64_t)((double)expected_keys / lam) + 1;
+        const uint64_t minN = g.bits > 32 ? (1ull << (g.bits - 32)) : 1;
+        nb = std::max(nb, minN);
+        if (g.bits < 64)
+            nb = std::min<uint64_t>(nb, 1ull << g.bits);
+        g.nBuckets = nb;
+        g.fpBits = (uint32_t)std::max<int>(1, (int)g.bits - (int)(63 - __builtin_clzll(nb)));
+    }
+    (void)lam;
     // keys per bucket are ~Poisson(expected / nBuckets); the stash holds the
     // expected overflow at <= 2/3 load (it grows during the build if needed)
     const double over = (double)expected_keys * overflow_fraction((double)expected_keys / (double)nb);
@@ -620,14 +722,14 @@ static ibs_status panel_plan(ibs_panel_table *p, const ibs_reference *ref, uint3
 
 // The span kernel's launches of one scan: one launch, or one per
 // bucket-range pass and a statistics launch.
-template <int NB>
+template <int NB, bool PM>
 static ibs_status enqueue_spans(ibs_panel_table *p, const ibs_reference *ref, uint32_t passes, int grid,
                                 cudaStream_t st)
 {
     const ScanPlan &pl = p->plan;
     if (passes <= 1) {
         IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
-        k_panel_spans<NB, kScan><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
+        k_panel_spans<NB, kScan, PM><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
                                                        (uint32_t)pl.nWin, pl.nSpans, pl.spanLen, p->nSamples,
                                                        p->dCounters + 1, p->dSpans, nullptr, 0, 0, false);
         IBS_LAUNCHED();
@@ -636,13 +738,13 @@ static ibs_status enqueue_spans(ibs_panel_table *p, const ibs_reference *ref, ui
     const uint64_t nb = p->geom.nBuckets;
     for (uint32_t i = 0; i < passes; ++i) {
         IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
-        k_panel_spans<NB, kMaskPass><<<grid, 256, 0, st>>>(
+        k_panel_spans<NB, kMaskPass, PM><<<grid, 256, 0, st>>>(
             p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0, (uint32_t)pl.nWin, pl.nSpans, pl.spanLen,
             p->nSamples, p->dCounters + 1, p->dSpans, p->dMasks, nb * i / passes, nb * (i + 1) / passes, i == 0);
         IBS_LAUNCHED();
     }
     IBS_CUDA(cudaMemsetAsync(p->dCounters + 1, 0, 8, st), "panel work reset");
-    k_panel_spans<NB, kStats><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
+    k_panel_spans<NB, kStats, PM><<<grid, 256, 0, st>>>(p->view(), ref->dSeq, ref->dMask, pl.dWin, pl.dSpan0,
                                                     (uint32_t)pl.nWin, pl.nSpans, pl.spanLen, p->nSamples,
                                                     p->dCounters + 1, p->dSpans, p->dMasks, 0, 0, false);
     IBS_LAUNCHED();
@@ -657,8 +759,12 @@ static ibs_status panel_enqueue(ibs_panel_table *p, const ibs_reference *ref, ib
     if (pl.nSpans) {
         const ibs_tuning tu = tuning();
         const int grid = sm_count() * (int)tu.panel_ctas_per_sm;
-        const ibs_status s = tu.panel_blocks_in_flight == 2 ? enqueue_spans<2>(p, ref, passes, grid, st)
-                                                            : enqueue_spans<4>(p, ref, passes, grid, st);
+        const bool pm = p->geom.format == FMT_PANEL_MZ;
+        const ibs_status s = tu.panel_blocks_in_flight == 2
+                                 ? (pm ? enqueue_spans<2, true>(p, ref, passes, grid, st)
+                                       : enqueue_spans<2, false>(p, ref, passes, grid, st))
+                                 : (pm ? enqueue_spans<4, true>(p, ref, passes, grid, st)
+                                       : enqueue_spans<4, false>(p, ref, passes, grid, st));
         if (s != IBS_OK)
             return s;
     }

@@ -154,26 +154,55 @@ __device__ __forceinline__ void serve_joint_item(const WorkItem &it, const panel
     const uint64_t kmask = key_mask(2 * k);
     const uint64_t kbits = (1ull << k) - 1;
     const uint32_t want = it.mask & 0xffffu;
+    // minimizer-line joint tables (PM) locate a k-mer through its minimizer:
+    // m-mers read one block ahead, up to the span's last position's last
+    // m-mer (inside the window's bases)
+    const bool pm = t.g.format == FMT_PANEL_MZ;
+    const uint32_t w = pm ? mz::w_of(k) : 1, m = pm ? mz::m_of(k) : 0;
+    const uint32_t lastM = it.p1 - 1 + (w - 1);
+    dev::MzPos next;
+    if (pm)
+        next = dev::mz_pos(seq, mask, it.base + min(it.p0 + lane, lastM), k, m);
     SegStats acc = seg_empty();
     for (uint32_t p = it.p0; p < it.p1; p += 32 * NB) {
         uint4 v0[NB], v1[NB];
-        uint64_t code[NB];
+        uint64_t code[NB], rr[NB];
         uint32_t fp[NB];
         bool valid[NB];
+        if (pm) {
+            dev::MzPos ps[NB + 1];
+            ps[0] = next;
+#pragma unroll
+            for (int b = 1; b <= NB; ++b)
+                ps[b] = dev::mz_pos(seq, mask, it.base + min(p + 32 * b + lane, lastM), k, m);
+            next = ps[NB];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                valid[b] = p + 32 * b + lane < it.p1 && ps[b].acgt;
+                uint64_t slot;
+                dev::mz_locate_lane(ps[b], ps[b + 1], lane, k, w, t.g.nBuckets, t.g.fpBits, rr[b], slot);
+                fp[b] = (uint32_t)slot;
+                code[b] = ps[b].code;
+            }
+        } else {
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const uint32_t q = p + 32 * b + lane;
+                const bool in = q < it.p1;
+                const uint64_t G = it.base + (in ? q : it.p0);
+                bool acgt;
+                code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
+                valid[b] = in && acgt;
+                const uint64_t h = perm_hash(code[b], t.g.bits);
+                rr[b] = bucket_of(h, t.g);
+                fp[b] = (uint32_t)fp_of(h, t.g);
+            }
+        }
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            const uint32_t q = p + 32 * b + lane;
-            const bool in = q < it.p1;
-            const uint64_t G = it.base + (in ? q : it.p0);
-            bool acgt;
-            code[b] = dev::canonical_at(seq, mask, G, k, kmask, kbits, acgt);
-            valid[b] = in && acgt;
-            const uint64_t h = perm_hash(code[b], t.g.bits);
-            const uint64_t r = bucket_of(h, t.g);
-            fp[b] = (uint32_t)fp_of(h, t.g);
             if (valid[b]) {
-                v0[b] = __ldg(t.buckets + 2 * r);
-                v1[b] = __ldg(t.buckets + 2 * r + 1);
+                v0[b] = __ldg(t.buckets + 2 * rr[b]);
+                v1[b] = __ldg(t.buckets + 2 * rr[b] + 1);
             } else {
                 v0[b] = make_uint4(0, 0, 0, 0);
                 v1[b] = make_uint4(0, 0, 0, 0);
@@ -183,9 +212,13 @@ __device__ __forceinline__ void serve_joint_item(const WorkItem &it, const panel
         for (int b = 0; b < NB; ++b) {
             uint32_t m = 0;
             if (valid[b]) {
-                m = panel::bucket_mask(v0[b], v1[b], fp[b]);
-                if (m & 0x80000000u)
-                    m = panel::stash_mask(t, code[b]);
+                if (pm) {
+                    m = panel::pm_mask(t, v0[b], v1[b], rr[b], fp[b], code[b]);
+                } else {
+                    m = panel::bucket_mask(v0[b], v1[b], fp[b]);
+                    if (m & 0x80000000u)
+                        m = panel::stash_mask(t, code[b]);
+                }
             }
             const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
             uint32_t myH = 0;

@@ -67,6 +67,45 @@ __device__ __forceinline__ MzPos mz_pos(const uint64_t *__restrict__ seq, const 
     return r;
 }
 
+// Sector and slot value of this lane's k-mer (position q of a block) from
+// the block's positions (cur) and the next block's (nxt): its minimizer is
+// the smallest rank key over the w (<= 7) m-mers starting at q .. q+w-1,
+// found with one shuffle per offset, and its line hash and orientation come
+// from the keying lane.
+__device__ __forceinline__ void mz_locate_lane(const MzPos &cur, const MzPos &nxt, uint32_t lane, uint32_t k,
+                                               uint32_t w, uint64_t nBuckets, uint32_t fpBits, uint64_t &r,
+                                               uint64_t &slot)
+{
+    const bool isFwd = cur.isFwd;
+    // keys have their low 3 bits clear; j ^ flip there makes the smallest
+    // packed value the leftmost smallest key (forward k-mer) or the rightmost
+    // (reverse k-mer)
+    const uint32_t flip = isFwd ? 0u : 7u;
+    uint32_t best = 0xffffffffu;
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j) {
+        if (j < w) {
+            // key of position q + j: lanes below 32 - j read lane + j of this
+            // block, the others lane + j - 32 (< j) of the next, so a source
+            // lane offers its next-block key exactly when it is below j -- one
+            // shuffle per offset
+            const uint32_t offer = lane < j ? nxt.key : cur.key;
+            const uint32_t v = __shfl_sync(FULL_MASK, offer, lane + j); // source lane mod 32
+            best = min(best, v ^ j ^ flip);
+        }
+    }
+    const uint32_t jm = (best & 7u) ^ flip;
+    // the minimizer's line hash and orientation from the lane that keyed it:
+    // position q + jm
+    const uint32_t src = lane + jm;
+    const uint64_t ga = __shfl_sync(FULL_MASK, cur.gs, src);
+    const uint64_t gc = __shfl_sync(FULL_MASK, nxt.gs, src);
+    const uint64_t gs = src < 32 ? ga : gc;
+    const uint32_t sm = isFwd ? (uint32_t)(gs >> 62) & 1u : (uint32_t)(gs >> 63);
+    const uint32_t o = isFwd ? jm : (w - 1 - jm);
+    mz::place(cur.code, k, o, sm, gs & ((1ull << 62) - 1), nBuckets, fpBits, r, slot);
+}
+
 // Statistics of positions [p0, p1) of the window whose first base is packed
 // base `base`, against a minimizer-line table; the m-mer reads stop at
 // position lastM (the last m-mer start the window's k-mers use: lanes past
@@ -97,36 +136,8 @@ __device__ __forceinline__ SegStats mz_span_stats(const TableView &t, const uint
         for (int b = 0; b < NB; ++b) {
             const uint32_t q = p + 32 * b + lane;
             valid[b] = q < p1 && ps[b].acgt;
-            const bool isFwd = ps[b].isFwd;
-            // minimizer over the w (<= 7) m-mers starting at q .. q+w-1:
-            // keys have their low 3 bits clear; j ^ flip there makes the
-            // smallest packed value the leftmost smallest key (forward
-            // k-mer) or the rightmost (reverse k-mer)
-            const uint32_t flip = isFwd ? 0u : 7u;
-            uint32_t best = 0xffffffffu;
-#pragma unroll
-            for (uint32_t j = 0; j < 8; ++j) {
-                if (j < w) {
-                    // key of position q + j: lanes below 32 - j read lane + j of
-                    // this block, the others lane + j - 32 (< j) of the next, so
-                    // a source lane offers its next-block key exactly when it is
-                    // below j -- one shuffle per offset
-                    const uint32_t offer = lane < j ? ps[b + 1].key : ps[b].key;
-                    const uint32_t v = __shfl_sync(FULL_MASK, offer, lane + j); // source lane mod 32
-                    best = min(best, v ^ j ^ flip);
-                }
-            }
-            const uint32_t jm = (best & 7u) ^ flip;
-            // the minimizer's line hash and orientation from the lane that
-            // keyed it: position q + jm
-            const uint32_t src = lane + jm;
-            const uint64_t ga = __shfl_sync(FULL_MASK, ps[b].gs, src);
-            const uint64_t gc = __shfl_sync(FULL_MASK, ps[b + 1].gs, src);
-            const uint64_t gs = src < 32 ? ga : gc;
-            const uint32_t sm = isFwd ? (uint32_t)(gs >> 62) & 1u : (uint32_t)(gs >> 63);
-            const uint32_t o = isFwd ? jm : (w - 1 - jm);
             uint64_t &r = rb[b];
-            mz::place(ps[b].code, k, o, sm, gs & ((1ull << 62) - 1), t.g.nBuckets, t.g.fpBits, r, slot[b]);
+            mz_locate_lane(ps[b], ps[b + 1], lane, k, w, t.g.nBuckets, t.g.fpBits, r, slot[b]);
             if (valid[b]) {
                 v0[b] = __ldg(t.buckets + 2 * r);
                 v1[b] = __ldg(t.buckets + 2 * r + 1);

@@ -16,9 +16,20 @@
 // stash). The fingerprint is the same quotient of the bijective k-mer hash
 // as in the single-sample table, so it needs nBuckets >= 2^(2k-32).
 // Stash: {code, mask} pairs, two per 32-byte bucket, linear probing.
+//
+// Format PM (FMT_PANEL_MZ, 16 <= k <= 27): the same sectors laid out as the
+// minimizer lines of the single-sample MZ tables (mz_core.cuh): the line is
+// the k-mer's minimizer's, one of its four sectors is picked by the k-mer
+// itself, and the 32-bit slot value identifies the k-mer within its line
+// (at least 2^(2k-28) lines). Consecutive reference positions mostly share a
+// minimizer, so a warp's probes fall in few 128-byte lines instead of 32
+// random ones. A full sector keeps further keys in its partner sector (index
+// ^ 1, the same line; flag bit 25 of byte 31's word) and then in the stash
+// (bit 24).
 #pragma once
 
 #include "ibs_internal.cuh"
+#include "mz_core.cuh"
 
 #include <vector>
 
@@ -28,6 +39,8 @@ namespace panel {
 constexpr uint32_t kMaxSamples = IBS_PANEL_MAX_SAMPLES;
 constexpr uint32_t kSlots = 5;
 constexpr uint64_t kStashEmpty = ~0ull;
+constexpr uint32_t kStashFlag = 1u << 24;   // word 7: some key of this sector is in the stash
+constexpr uint32_t kPartnerFlag = 1u << 25; // word 7 (PM): some key of this sector is in its partner sector
 
 struct View {
     TableGeom g;
@@ -52,9 +65,9 @@ __device__ __forceinline__ uint32_t stash_mask(const View &t, uint64_t code)
     return 0;
 }
 
-// Sample mask of a k-mer given its bucket halves and fingerprint; bit 31
-// set = look in the stash.
-__device__ __forceinline__ uint32_t bucket_mask(const uint4 &v0, const uint4 &v1, uint32_t fp)
+// Sample mask of fingerprint (or slot value) fp in a sector's halves; 0
+// when no slot holds it.
+__device__ __forceinline__ uint32_t sector_mask(const uint4 &v0, const uint4 &v1, uint32_t fp)
 {
     const uint32_t cnt = (v1.w >> 16) & 0xff;
     uint32_t m = 0;
@@ -63,13 +76,60 @@ __device__ __forceinline__ uint32_t bucket_mask(const uint4 &v0, const uint4 &v1
     m |= (2 < cnt && v0.z == fp) ? (v1.z & 0xffff) : 0u;
     m |= (3 < cnt && v0.w == fp) ? (v1.z >> 16) : 0u;
     m |= (4 < cnt && v1.x == fp) ? (v1.w & 0xffff) : 0u;
-    if (!m && ((v1.w >> 24) & 1u))
+    return m;
+}
+
+// Sample mask of a k-mer given its bucket halves and fingerprint; bit 31
+// set = look in the stash.
+__device__ __forceinline__ uint32_t bucket_mask(const uint4 &v0, const uint4 &v1, uint32_t fp)
+{
+    uint32_t m = sector_mask(v0, v1, fp);
+    if (!m && (v1.w & kStashFlag))
         m = 0x80000000u;
     return m;
 }
 
+// PM: the mask of the k-mer `code` with slot value `slot` whose home
+// sector r has halves v0, v1: the home sector, then (flagged) its partner
+// sector, then (flagged) the stash.
+__device__ __forceinline__ uint32_t pm_mask(const View &t, const uint4 &v0, const uint4 &v1, uint64_t r,
+                                            uint32_t slot, uint64_t code)
+{
+    uint32_t m = sector_mask(v0, v1, slot);
+    if (m)
+        return m;
+    if (v1.w & kPartnerFlag) {
+        const uint4 w0 = __ldg(t.buckets + 2 * (r ^ 1)), w1 = __ldg(t.buckets + 2 * (r ^ 1) + 1);
+        m = sector_mask(w0, w1, slot);
+        if (m)
+            return m;
+    }
+    return (v1.w & kStashFlag) ? stash_mask(t, code) : 0u;
+}
+
+// Home sector and stored fingerprint (P5x48) or slot value (PM) of a key.
+__device__ __forceinline__ void joint_place(const View &t, uint64_t code, uint64_t &r, uint32_t &fp)
+{
+    if (t.g.format == FMT_PANEL_MZ) {
+        uint64_t slot;
+        mz::locate(code, t.g, r, slot);
+        fp = (uint32_t)slot;
+        return;
+    }
+    const uint64_t h = perm_hash(code, t.g.bits);
+    r = bucket_of(h, t.g);
+    fp = (uint32_t)fp_of(h, t.g);
+}
+
 __device__ __forceinline__ uint32_t lookup_mask(const View &t, uint64_t code)
 {
+    if (t.g.format == FMT_PANEL_MZ) {
+        uint64_t r;
+        uint32_t slot;
+        joint_place(t, code, r, slot);
+        const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);
+        return pm_mask(t, v0, v1, r, slot, code);
+    }
     const uint64_t h = perm_hash(code, t.g.bits);
     const uint64_t r = bucket_of(h, t.g);
     const uint4 v0 = __ldg(t.buckets + 2 * r), v1 = __ldg(t.buckets + 2 * r + 1);

@@ -317,8 +317,11 @@ class PanelTable:
 
     MAX_SAMPLES = 16
 
-    def __init__(self, k: int, expected_keys: int, device: int = 0, keys_per_bucket: float = 0.0):
-        opts = TableOpts(device, keys_per_bucket, 0)
+    def __init__(self, k: int, expected_keys: int, device: int = 0, keys_per_bucket: float = 0.0,
+                 force_format: int = 0):
+        """force_format: 0 = by size (minimizer lines for 16 <= k <= 27 when large
+        enough), 3 = hash sectors, 7 = minimizer lines."""
+        opts = TableOpts(device, keys_per_bucket, force_format)
         h = vp()
         _check(_ibs_pt_create(k, expected_keys, C.byref(opts), C.byref(h)))
         self._h = h.value

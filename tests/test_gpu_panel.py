@@ -20,18 +20,21 @@ def _samples(ref_spec, seq, mask, n, k=25):
     return out
 
 
-@pytest.mark.parametrize("n_samples,k", [(1, 25), (5, 25), (16, 25), (16, 31)])
-def test_panel_rows_equal_single_scans(n_samples, k):
+@pytest.mark.parametrize("n_samples,k,fmt", [(1, 25, 3), (5, 25, 3), (16, 25, 3), (16, 31, 0),
+                                             (1, 25, 7), (5, 25, 7), (16, 25, 7)])
+def test_panel_rows_equal_single_scans(n_samples, k, fmt):
+    """fmt 3: hash sectors; 7: minimizer lines; 0: by size (k = 31: hash)."""
     ref_spec = ib.RefSpec(seed=77, lens=[400_000, 123_457, 24, 31, 90_000], n_frac=0.003,
                           n_run=(1, 200), lower_frac=0.02)
     seq, mask = ref_spec.reference_host()
     samples = _samples(ref_spec, seq, mask, n_samples, k)
     union = len(np.unique(np.concatenate(samples)))
-    pt = ib.PanelTable(k, union)
+    pt = ib.PanelTable(k, union, force_format=fmt)
     for c in samples:
         pt.add_codes(c, len(c), on_device=False)
     info, ns = pt.info()
     assert ns == n_samples
+    assert info.format == (fmt or 3)
     # masks against set membership
     rng = np.random.default_rng(3)
     q = np.concatenate([rng.choice(np.concatenate(samples), 20_000), corpus.random_codes(rng, 20_000, k)])
@@ -142,4 +145,57 @@ def test_panel_scan_in_bucket_range_passes_equals_one_pass():
     assert ib.get_tuning().panel_pass_mb == 0
     assert np.array_equal(many, one)
     pt.close()
+    ref.free()
+
+
+@pytest.mark.parametrize("serial", [False, True])
+def test_dense_minimizer_line_panel_uses_partner_sectors_and_stash(serial):
+    """A crowded joint minimizer-line table (k = 20: a small minimum line
+    count, 4 keys per 5-slot sector): full sectors send keys to their
+    partner sector and the stash; masks, panel rows and served rows still
+    equal set membership and single-sample scans."""
+    k, W = 20, 3000
+    ref_spec = ib.RefSpec(seed=81, lens=[250_000, 60_000, 19, 20], n_frac=0.002, n_run=(1, 100))
+    seq, mask = ref_spec.reference_host()
+    samples = _samples(ref_spec, seq, mask, 16, k=k)
+    union = len(np.unique(np.concatenate(samples)))
+    pt = ib.PanelTable(k, union, keys_per_bucket=4.0, force_format=7)
+    for c in samples:
+        pt.add_codes(c, len(c), on_device=False)
+    info, ns = pt.info()
+    assert info.format == 7 and info.stash_buckets > 0
+    rng = np.random.default_rng(5)
+    q = np.concatenate([np.concatenate(samples), corpus.random_codes(rng, 20_000, k)])
+    want = np.zeros(len(q), np.uint32)
+    for i, c in enumerate(samples):
+        want |= np.isin(q, c).astype(np.uint32) << np.uint32(i)
+    assert np.array_equal(pt.probe(q), want)
+    ref = ib.Reference(seq, mask, ref_spec.lens)
+    panel = pt.scan(ref, W)
+    singles = []
+    for i, c in enumerate(samples):
+        t = ib.Table.from_codes(c, len(c), k, on_device=False)
+        singles.append(ib.scan(t, ref, W))
+        assert np.array_equal(panel[i], singles[i]), f"sample {i}"
+        t.close()
+    # the same table served: whole contigs for every sample, batched or one per launch
+    srv = ib.Server(ref, W, k, one_request_per_launch=serial)
+    assert srv.add_panel(pt, release=True) == list(range(16))
+    pt.close()
+    reqs = [(s, c, 0, 0) for s in range(16) for c in range(len(ref_spec.lens))]
+    for r in reqs:
+        srv.submit(*r)
+    done = []
+    import time
+    deadline = time.time() + 300
+    while len(done) < len(reqs) and time.time() < deadline:
+        done += srv.poll(64, timeout_ms=2000)
+    assert len(done) == len(reqs), srv.stats()
+    starts = np.concatenate([[0], np.cumsum([ib.window_count(ref_spec.lens[c:c + 1], W, k)
+                                             for c in range(len(ref_spec.lens))])])
+    for r in done:
+        assert r["status"] == 0
+        a = starts[r["contig"]]
+        assert np.array_equal(r["rows"], singles[r["sample"]][a:a + r["n_windows"]]), (r["sample"], r["contig"])
+    srv.close()
     ref.free()
