@@ -655,7 +655,11 @@ def panel_arm(args, rank: int):
 
     # batched: joint tables of as many samples as fit next to the build's
     # scratch (one sample's codes); all 16 in one table when memory allows
-    kpb = args.panel_keys_per_bucket or ib.get_tuning().panel_keys_per_bucket
+    # joint-table load: the flag, else the library's default for the layout it
+    # picks (minimizer lines at 2 keys per sector for 16 <= k <= 27, hash
+    # sectors at the tuned load otherwise)
+    kpb = args.panel_keys_per_bucket
+    kpb_est = kpb or (2.0 if 16 <= k <= 27 else ib.get_tuning().panel_keys_per_bucket)
     free, _ = torch.cuda.mem_get_info()
     max_codes = max(sample_codes_bound(i) for i in range(len(w.samples))) * 8
     rows_bytes = n_win * len(w.samples) * 24 + 64 * n_win * len(w.samples)
@@ -666,7 +670,7 @@ def panel_arm(args, rank: int):
     def joint_bytes(members):
         u = int(torch.unique(torch.cat([sampled[j] for j in members])).numel() * 64 * 1.02) + (1 << 20)
         union_of[tuple(members)] = u
-        return u / kpb * 32 * 1.15
+        return u / kpb_est * 32 * 1.15
 
     groups, cur = [], []
     for i in range(len(w.samples)):
@@ -681,6 +685,7 @@ def panel_arm(args, rank: int):
         f"union estimates {[union_of[tuple(m)] for m in groups]}")
     del sampled
     panel_ms, launches, table_gb, union_est, got = 0.0, 0, [], [], [None] * len(w.samples)
+    table_fmt = []
     build_s = 0.0
     for members in groups:
         tb = time.time()
@@ -693,6 +698,7 @@ def panel_arm(args, rank: int):
         info, ns = pt.info()
         build_s += time.time() - tb
         table_gb.append(info.device_bytes / 1e9)
+        table_fmt.append(int(info.format))
         union_est.append(union_of[tuple(members)])
         rows = torch.empty(max(n_win * ns, 1) * 6, dtype=torch.int32, device="cuda")
         for _ in range(args.warmup):
@@ -732,7 +738,8 @@ def panel_arm(args, rank: int):
     out = {"workload": w.name, "samples": ns, "sample_kmers": sizes, "k": k, "window": W,
            "reference_bp": int(sum(map(int, lens))), "positions": int(positions),
            "groups": groups, "union_keys_estimate": union_est, "joint_table_gb": table_gb,
-           "keys_per_bucket": kpb, "build_s": build_s, "setup_s": t_build,
+           "joint_table_format": table_fmt,
+           "keys_per_bucket": kpb_est, "build_s": build_s, "setup_s": t_build,
            "batched_probes_per_s": probes / (panel_ms * 1e-3), "batched_ms_per_scan": panel_ms,
            "plain_probes_per_s": probes / (plain_ms * 1e-3), "plain_ms_all_samples": plain_ms,
            "speedup_vs_plain": plain_ms / panel_ms, "graph_launches_per_scan": launches / args.steps,
@@ -899,7 +906,11 @@ def served_arm(args, rank: int):
     torch.cuda.empty_cache()
 
     # batched: joint panel tables (as many samples per table as memory allows)
-    kpb = args.panel_keys_per_bucket or ib.get_tuning().panel_keys_per_bucket
+    # joint-table load: the flag, else the library's default for the layout it
+    # picks (minimizer lines at 2 keys per sector for 16 <= k <= 27, hash
+    # sectors at the tuned load otherwise)
+    kpb = args.panel_keys_per_bucket
+    kpb_est = kpb or (2.0 if 16 <= k <= 27 else ib.get_tuning().panel_keys_per_bucket)
     free, _ = torch.cuda.mem_get_info()
     budget = free - max_bound * 8 - (4 << 30) - (8 << 30)
     union_of = {}
@@ -907,7 +918,7 @@ def served_arm(args, rank: int):
     def joint_bytes(members):
         u = int(torch.unique(torch.cat([sampled[j] for j in members])).numel() * 64 * 1.02) + (1 << 20)
         union_of[tuple(members)] = u
-        return u / kpb * 32 * 1.15
+        return u / kpb_est * 32 * 1.15
 
     groups, cur = [], []
     for i in range(n_samples):
@@ -918,7 +929,7 @@ def served_arm(args, rank: int):
     groups.append(cur)
     del sampled
     srv = ib.Server(ref, W, k, memory_budget=int(free - max_bound * 8 - (8 << 30)))
-    id_of = {}
+    id_of, joint_fmt = {}, []
     for members in groups:
         pt = ib.PanelTable(k, union_of[tuple(members)], keys_per_bucket=kpb)
         for i in members:
@@ -926,12 +937,14 @@ def served_arm(args, rank: int):
             pt.add_codes(buf.data_ptr(), n, on_device=True)
             del buf
             torch.cuda.empty_cache()
+        joint_fmt.append(int(pt.info()[0].format))
         for i, sid in zip(members, srv.add_panel(pt, release=True)):
             id_of[i] = sid
         pt.close()
         torch.cuda.empty_cache()
     assert all(id_of[i] == i for i in range(n_samples))
     out["batched_groups"] = groups
+    out["batched_table_format"] = joint_fmt
     out["batched_tables_gb"] = srv.stats()["resident_bytes"] / 1e9
     for r in rates:
         out[f"batched_poisson_{r:g}"] = run(srv, r)
