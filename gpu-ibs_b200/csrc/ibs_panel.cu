@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(256) k_panel_spans(View t, const uint64_t *__r
                     const uint32_t q = p + 32 * b + lane;
                     valid[b] = q < p1 && ps[b].acgt;
                     uint64_t slot;
-                    dev::mz_locate_lane(ps[b], ps[b + 1], lane, k, w, t.g.nBuckets, t.g.fpBits, rr[b], slot);
+                    dev::mz_locate_lane<true>(ps[b], ps[b + 1], lane, k, w, t.g.nBuckets, t.g.fpBits, rr[b], slot);
                     fp[b] = (uint32_t)slot;
                     code[b] = ps[b].code;
                 }

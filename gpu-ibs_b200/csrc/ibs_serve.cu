@@ -180,7 +180,7 @@ __device__ __forceinline__ void serve_joint_item(const WorkItem &it, const panel
             for (int b = 0; b < NB; ++b) {
                 valid[b] = p + 32 * b + lane < it.p1 && ps[b].acgt;
                 uint64_t slot;
-                dev::mz_locate_lane(ps[b], ps[b + 1], lane, k, w, t.g.nBuckets, t.g.fpBits, rr[b], slot);
+                dev::mz_locate_lane<true>(ps[b], ps[b + 1], lane, k, w, t.g.nBuckets, t.g.fpBits, rr[b], slot);
                 fp[b] = (uint32_t)slot;
                 code[b] = ps[b].code;
             }

@@ -155,6 +155,18 @@ IBS_HD void place(uint64_t C, uint32_t k, uint32_t o, uint32_t s, uint64_t g, ui
     slot = ((uint64_t)slot_high(C, k, o, s) << hbits) | (g & key_mask(hbits));
 }
 
+// The same as place() where the slot value fits 32 bits (MZ8 sectors, joint
+// minimizer lines: hbits < 32 and the slot below 2^32 by their line counts),
+// in 32-bit arithmetic. Only bits 0 .. 2m-1 of g are read, so flag bits above
+// them do not matter.
+IBS_HD void place32(uint64_t C, uint32_t k, uint32_t o, uint32_t s, uint64_t g, uint64_t nBuckets,
+                    uint32_t hbits, uint64_t &bucket, uint64_t &slot)
+{
+    bucket = line_of(g, m_of(k), nBuckets / kSectorsPerLine) * kSectorsPerLine + sector_of(C);
+    const uint32_t low = (uint32_t)g & ((1u << hbits) - 1u);
+    slot = (slot_high(C, k, o, s) << hbits) | low;
+}
+
 // Slot value and bucket of a canonical k-mer (the build side, and single
 // probes): everything from C itself.
 IBS_HD void locate(uint64_t C, const TableGeom &g, uint64_t &bucket, uint64_t &slot)

@@ -72,6 +72,8 @@ __device__ __forceinline__ MzPos mz_pos(const uint64_t *__restrict__ seq, const 
 // the smallest rank key over the w (<= 7) m-mers starting at q .. q+w-1,
 // found with one shuffle per offset, and its line hash and orientation come
 // from the keying lane.
+// SLOT32: the table's slot values fit 32 bits (MZ8, joint minimizer lines).
+template <bool SLOT32>
 __device__ __forceinline__ void mz_locate_lane(const MzPos &cur, const MzPos &nxt, uint32_t lane, uint32_t k,
                                                uint32_t w, uint64_t nBuckets, uint32_t fpBits, uint64_t &r,
                                                uint64_t &slot)
@@ -103,7 +105,12 @@ __device__ __forceinline__ void mz_locate_lane(const MzPos &cur, const MzPos &nx
     const uint64_t gs = src < 32 ? ga : gc;
     const uint32_t sm = isFwd ? (uint32_t)(gs >> 62) & 1u : (uint32_t)(gs >> 63);
     const uint32_t o = isFwd ? jm : (w - 1 - jm);
-    mz::place(cur.code, k, o, sm, gs & ((1ull << 62) - 1), nBuckets, fpBits, r, slot);
+    // place() and place32() read bits 0 .. 2m-1 of the line hash: the
+    // orientation bits 62 and 63 above them need no masking
+    if constexpr (SLOT32)
+        mz::place32(cur.code, k, o, sm, gs, nBuckets, fpBits, r, slot);
+    else
+        mz::place(cur.code, k, o, sm, gs, nBuckets, fpBits, r, slot);
 }
 
 // Statistics of positions [p0, p1) of the window whose first base is packed
@@ -137,7 +144,7 @@ __device__ __forceinline__ SegStats mz_span_stats(const TableView &t, const uint
             const uint32_t q = p + 32 * b + lane;
             valid[b] = q < p1 && ps[b].acgt;
             uint64_t &r = rb[b];
-            mz_locate_lane(ps[b], ps[b + 1], lane, k, w, t.g.nBuckets, t.g.fpBits, r, slot[b]);
+            mz_locate_lane<false>(ps[b], ps[b + 1], lane, k, w, t.g.nBuckets, t.g.fpBits, r, slot[b]);
             if (valid[b]) {
                 v0[b] = __ldg(t.buckets + 2 * r);
                 v1[b] = __ldg(t.buckets + 2 * r + 1);
