@@ -53,8 +53,9 @@ constexpr uint64_t kFinCap = 1ull << 20;   // (request, window) rows finalized p
 constexpr uint64_t kRowPool = 4ull << 20;  // rows of admitted requests (24 B each): 96 MiB
 constexpr uint32_t kMaxGroups = 4096;
 constexpr int kDepth = 4;                  // iterations (batches) in flight
-constexpr int kServeNB = 2;                // blocks in flight per lane of the single-table and persistent
-                                           // kernels (64 registers, four CTAs of 256 per SM)
+constexpr int kServeNB = 2;                // blocks in flight per lane of the single-table kernel (64
+                                           // registers, four CTAs of 256 per SM) and of the persistent
+                                           // kernel (80 registers without spills, three CTAs per SM)
 
 struct WorkItem {
     uint64_t base;   // packed base offset of the window's first base
@@ -393,7 +394,7 @@ __device__ __forceinline__ uint64_t published_count(const Ctrl *ctrl, DevState *
 }
 
 template <int NB, uint32_t K>
-__global__ void __launch_bounds__(256, 4) k_serve_persistent(const Ctrl *ctrl, Status *status, DevState *ds,
+__global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, Status *status, DevState *ds,
                                                              const uint64_t *__restrict__ seq,
                                                              const uint64_t *__restrict__ mask, int k,
                                                              ibs_window *rows, uint64_t idleNs, uint64_t waitNs)
