@@ -13,7 +13,10 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
+#include <unistd.h>
 
 namespace ibs {
 
@@ -709,17 +712,42 @@ ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_
     ibs_status s = check_device_ordinal(dev);
     if (s != IBS_OK)
         return s;
+    // The records go up in chunks through a ring of kSlots pinned buffers:
+    // kReaders host threads read chunks ahead (pread, in parallel), and this
+    // thread uploads and decodes them in order; a buffer is read into again
+    // once the upload of its previous chunk has finished.
+    constexpr int kSlots = 8, kReaders = 4;
     uint64_t *dCodes = nullptr, *dLut = nullptr;
-    uint8_t *dRaw[2] = {nullptr, nullptr};
-    uint8_t *hRaw[2] = {nullptr, nullptr};
+    uint8_t *dRaw[kSlots] = {};
+    uint8_t *hRaw[kSlots] = {};
+    cudaEvent_t done[kSlots] = {};
     cudaStream_t st = nullptr;
-    cudaEvent_t done[2] = {nullptr, nullptr};
+    const uint64_t total = h.total;
+    const uint64_t chunkRecs = std::max<uint64_t>(1, (128ull << 20) / recBytes);
+    const uint64_t chunkBytes = chunkRecs * recBytes;
+    const uint64_t nChunks = (total + chunkRecs - 1) / chunkRecs;
+    const int nSlots = (int)std::min<uint64_t>(kSlots, std::max<uint64_t>(nChunks, 1));
+    // ring state: chunk filled[i] is in slot i ready for upload; consumed[i]
+    // is the last chunk whose upload from slot i was enqueued
+    std::mutex mu;
+    std::condition_variable cv;
+    std::vector<int64_t> filled(nSlots, -1), consumed(nSlots, -1);
+    bool readFailed = false, stopReading = false;
+    std::vector<std::thread> readers;
     auto cleanup = [&]() {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            stopReading = true;
+        }
+        cv.notify_all();
+        for (auto &t : readers)
+            t.join();
+        readers.clear();
         if (st)
             cudaStreamSynchronize(st);
         cudaFree(dCodes);
         cudaFree(dLut);
-        for (int i = 0; i < 2; i++) {
+        for (int i = 0; i < nSlots; i++) {
             cudaFree(dRaw[i]);
             cudaFreeHost(hRaw[i]);
             if (done[i])
@@ -728,15 +756,12 @@ ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_
         if (st)
             cudaStreamDestroy(st);
     };
-    const uint64_t total = h.total;
-    const uint64_t chunkRecs = std::max<uint64_t>(1, (256ull << 20) / recBytes);
-    const uint64_t chunkBytes = chunkRecs * recBytes;
     cudaError_t e = cudaMalloc(&dCodes, std::max<uint64_t>(total, 1) * 8);
     if (e == cudaSuccess)
         e = cudaMalloc(&dLut, lut.size() * 8);
     if (e == cudaSuccess)
         e = cudaMemcpy(dLut, lut.data(), lut.size() * 8, cudaMemcpyHostToDevice);
-    for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+    for (int i = 0; i < nSlots && e == cudaSuccess; i++) {
         e = cudaMalloc(&dRaw[i], chunkBytes);
         if (e == cudaSuccess)
             e = cudaMallocHost(&hRaw[i], chunkBytes);
@@ -749,36 +774,77 @@ ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_
         cleanup();
         return cuda_fail(e, "KMC decode buffers");
     }
-    // Double-buffered: read chunk i into pinned buffer i%2 while chunk i-1
-    // uploads and decodes.
-    if (fseeko(sf.f, 4, SEEK_SET) != 0) {
-        cleanup();
-        set_error("KMC: seek failed in " + suf);
-        return IBS_ERR_IO;
-    }
+    const int fd = fileno(sf.f);
+    int device = 0;
+    cudaGetDevice(&device);
+    auto reader = [&](int r) {
+        cudaSetDevice(device);
+        for (uint64_t c = r; c < nChunks; c += kReaders) {
+            const int slot = (int)(c % nSlots);
+            {
+                // the slot's previous chunk (c - nSlots) must have been enqueued
+                std::unique_lock<std::mutex> lock(mu);
+                cv.wait(lock, [&] {
+                    return stopReading || (c < (uint64_t)nSlots ? true : consumed[slot] == (int64_t)(c - nSlots));
+                });
+                if (stopReading)
+                    return;
+            }
+            if (c >= (uint64_t)nSlots && cudaEventSynchronize(done[slot]) != cudaSuccess) {
+                std::lock_guard<std::mutex> lock(mu);
+                readFailed = true;
+                cv.notify_all();
+                return;
+            }
+            const uint64_t r0 = c * chunkRecs;
+            const uint64_t bytes = std::min(chunkRecs, total - r0) * recBytes;
+            uint64_t got = 0;
+            while (got < bytes) {
+                const ssize_t n = pread(fd, hRaw[slot] + got, bytes - got, (off_t)(4 + r0 * recBytes + got));
+                if (n <= 0)
+                    break;
+                got += (uint64_t)n;
+            }
+            std::lock_guard<std::mutex> lock(mu);
+            if (got != bytes)
+                readFailed = true;
+            else
+                filled[slot] = (int64_t)c;
+            cv.notify_all();
+            if (got != bytes)
+                return;
+        }
+    };
+    for (int r = 0; r < kReaders && (uint64_t)r < nChunks; ++r)
+        readers.emplace_back(reader, r);
     const uint64_t lutN = lut.size() - 1;
     const uint64_t prefixMask = (1ull << (2 * h.p)) - 1;
-    int slot = 0;
-    for (uint64_t r0 = 0; r0 < total; r0 += chunkRecs, slot ^= 1) {
-        const uint64_t nRec = std::min(chunkRecs, total - r0);
-        e = cudaEventSynchronize(done[slot]);
-        if (e != cudaSuccess)
-            break;
-        if (fread(hRaw[slot], 1, nRec * recBytes, sf.f) != nRec * recBytes) {
-            cleanup();
-            set_error("KMC: short read of suffix records in " + suf);
-            return IBS_ERR_IO;
+    for (uint64_t c = 0; c < nChunks && e == cudaSuccess; ++c) {
+        const int slot = (int)(c % nSlots);
+        {
+            std::unique_lock<std::mutex> lock(mu);
+            cv.wait(lock, [&] { return readFailed || filled[slot] == (int64_t)c; });
+            if (readFailed) {
+                lock.unlock();
+                cleanup();
+                set_error("KMC: short read of suffix records in " + suf);
+                return IBS_ERR_IO;
+            }
         }
+        const uint64_t r0 = c * chunkRecs;
+        const uint64_t nRec = std::min(chunkRecs, total - r0);
         e = cudaMemcpyAsync(dRaw[slot], hRaw[slot], nRec * recBytes, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess)
             break;
-        k_decode<<<grid_for(nRec, 256), 256, 0, st>>>(dRaw[slot], r0, nRec, recBytes, sufBytes,
-                                                      dLut, lutN, prefixMask, 2 * (h.k - h.p),
-                                                      dCodes);
+        k_decode<<<grid_for(nRec, 256), 256, 0, st>>>(dRaw[slot], r0, nRec, recBytes, sufBytes, dLut, lutN,
+                                                      prefixMask, 2 * (h.k - h.p), dCodes);
         IBS_LAUNCHED();
         e = cudaEventRecord(done[slot], st);
-        if (e != cudaSuccess)
-            break;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            consumed[slot] = (int64_t)c;
+        }
+        cv.notify_all();
     }
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(st);
@@ -788,14 +854,6 @@ ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_
         cleanup();
         return cuda_fail(e, "KMC decode");
     }
-    for (int i = 0; i < 2; i++) {
-        cudaFree(dRaw[i]);
-        dRaw[i] = nullptr;
-        cudaFreeHost(hRaw[i]);
-        hRaw[i] = nullptr;
-    }
-    cudaFree(dLut);
-    dLut = nullptr;
     *dCodesOut = dCodes;
     dCodes = nullptr;
     *nOut = total;
