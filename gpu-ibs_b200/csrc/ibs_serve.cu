@@ -352,7 +352,8 @@ struct DevState {                  // device memory, zeroed before each launch
     unsigned long long scanDone[kRing], finDone[kRing];
     unsigned long long published;  // device copy of the host's count (one warp at a time reads the host's)
     unsigned int draining;
-    unsigned int polling;          // held by the warp reading the host's count
+    unsigned int polling;          // held by the warp reading the host's control block
+    unsigned int stop;             // device copy of the host's stop flag
 };
 
 
@@ -377,15 +378,19 @@ __device__ __forceinline__ uint64_t global_ns()
 }
 
 // The published ticket count as this warp may rely on it: the device copy,
-// refreshed from pinned host memory by one warp at a time (the waiting warps
-// of a whole grid would otherwise flood the host link with reads).
+// refreshed (with the stop flag) from pinned host memory by one warp at a
+// time. Waiting warps read only device memory: a whole grid polling the host
+// would flood the host link, slowing the very uploads it waits for.
 __device__ __forceinline__ uint64_t published_count(const Ctrl *ctrl, DevState *ds)
 {
     uint64_t v = *(volatile unsigned long long *)&ds->published;
     if (atomicCAS(&ds->polling, 0u, 1u) == 0u) {
         const uint64_t h = ld_acquire_sys(&ctrl->published);
+        const uint32_t stop = *(volatile const uint32_t *)&ctrl->stop;
         __threadfence_system();
         atomicMax(&ds->published, (unsigned long long)h);
+        if (stop)
+            atomicExch(&ds->stop, 1u);
         __threadfence();
         atomicExch(&ds->polling, 0u);
         v = h > v ? h : v;
@@ -409,7 +414,7 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
         unsigned long long t = 0;
         uint32_t go = 0;
         if (lane == 0) {
-            if (!*(volatile unsigned int *)&ds->draining && !*(volatile const uint32_t *)&ctrl->stop) {
+            if (!*(volatile unsigned int *)&ds->draining && !*(volatile unsigned int *)&ds->stop) {
                 t = atomicAdd(&ds->ticket, 1ull);
                 // wait (bounded) until it is published
                 const uint64_t t0 = global_ns();
@@ -418,7 +423,7 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                         go = 1;
                         break;
                     }
-                    if (*(volatile unsigned int *)&ds->draining || *(volatile const uint32_t *)&ctrl->stop)
+                    if (*(volatile unsigned int *)&ds->draining || *(volatile unsigned int *)&ds->stop)
                         break;
                     if (global_ns() - t0 > idleNs || spin > (idleNs >> 8) + 1024) {
                         if (atomicExch(&ds->draining, 1u) == 0u)
@@ -471,10 +476,9 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
             dT0 = __shfl_sync(dev::FULL_MASK, t0, slot);
             dEnd = dT0 + __shfl_sync(dev::FULL_MASK, n, slot);
             word = 0;
-            if (lane < kDescWords) {
-                (void)ld_acquire_sys(&ctrl->published);
+            asm volatile("fence.acq_rel.sys;" ::: "memory"); // after the acquiring reads of the slot search
+            if (lane < kDescWords)
                 word = reinterpret_cast<const volatile uint64_t *>(&ctrl->slot[slot])[lane];
-            }
         }
         // the descriptor's fields, from the lanes holding them
         BatchDesc d;
