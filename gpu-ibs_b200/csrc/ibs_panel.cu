@@ -806,7 +806,7 @@ extern "C" ibs_status ibs_panel_table_scan_async(ibs_panel_table *p, ibs_referen
     // the work reset, the span kernel and the finalizer as one graph.
     const void *key[3] = {ref, rows_dev, stream};
     const ibs_tuning tu = tuning();
-    const uint32_t shape[2] = {tu.panel_ctas_per_sm, tu.panel_blocks_in_flight};
+    const uint32_t shape[3] = {tu.panel_ctas_per_sm, tu.panel_blocks_in_flight, pass_count(p)};
     if (p->graph && p->graphW == W && !memcmp(key, p->graphKey, sizeof key) &&
         !memcmp(shape, p->graphShape, sizeof shape)) {
         IBS_CUDA(cudaGraphLaunch(p->graph, st), "panel graph launch");

@@ -201,7 +201,7 @@ struct ibs_panel_table {
     // captured scan graph for (reference, W, rows, stream)
     cudaGraphExec_t graph = nullptr;
     const void *graphKey[3] = {nullptr, nullptr, nullptr};
-    uint32_t graphShape[2] = {0, 0}; // launch shape it was captured with: CTAs per SM, blocks in flight
+    uint32_t graphShape[3] = {0, 0, 0}; // what it was captured with: CTAs per SM, blocks in flight, passes
     uint32_t graphW = 0;
     View view() const { return View{geom, buckets, stash, stashBuckets}; }
 };
