@@ -147,6 +147,28 @@ public:
         const auto t0 = std::chrono::steady_clock::now();
         std::cout << "Reading sequences" << std::endl;
         const bool compressed = refPath.find(".gz") != std::string::npos;
+        if (!compressed) {
+            // plain FASTA goes to the device parser straight from the mapped file
+            ibs_host::MappedFile mf(refPath);
+            if (mf.data && mf.size && mf.data[0] == '>') {
+                ibs_reference *dref = nullptr;
+                meta = PackedReference();
+                const auto t1 = std::chrono::steady_clock::now();
+                check(ibs_reference_from_fasta(mf.data, mf.size, gpuOptions().device, &dref),
+                      "ibs_reference_from_fasta");
+                const uint32_t n = ibs_reference_contig_count(dref);
+                for (uint32_t c = 0; c < n; ++c) {
+                    uint64_t len = 0;
+                    const char *id = nullptr;
+                    ibs_reference_contig(dref, c, &len, &id);
+                    meta.lens.push_back(len);
+                    meta.ids.emplace_back(id);
+                }
+                meta.readSec = std::chrono::duration<double>(t1 - t0).count();
+                meta.packSec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+                return dref;
+            }
+        }
         std::string text = ibs_host::read_file_text(refPath, compressed);
         const auto t1 = std::chrono::steady_clock::now();
         ibs_reference *dref = nullptr;

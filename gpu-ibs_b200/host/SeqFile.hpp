@@ -9,6 +9,10 @@
 //   - a truncated or corrupt gzip stream is an error.
 #pragma once
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <zlib.h>
 
 #include <cstdio>
@@ -64,6 +68,38 @@ inline std::string read_plain(const std::string &path)
     data.resize(got);
     return data;
 }
+
+// A plain file mapped read-only, for readers that only look at its bytes
+// (the device FASTA parser copies them through its own pinned staging, so
+// the text needs no copy of its own in host memory). Empty when the file
+// cannot be mapped; the caller then reads it.
+struct MappedFile {
+    const char *data = nullptr;
+    size_t size = 0;
+    explicit MappedFile(const std::string &path)
+    {
+        const int fd = open(path.c_str(), O_RDONLY);
+        if (fd < 0)
+            return;
+        struct stat st {};
+        if (fstat(fd, &st) == 0 && st.st_size > 0) {
+            void *p = mmap(nullptr, (size_t)st.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+            if (p != MAP_FAILED) {
+                madvise(p, (size_t)st.st_size, MADV_SEQUENTIAL | MADV_WILLNEED);
+                data = static_cast<const char *>(p);
+                size = (size_t)st.st_size;
+            }
+        }
+        close(fd);
+    }
+    ~MappedFile()
+    {
+        if (data)
+            munmap(const_cast<char *>(data), size);
+    }
+    MappedFile(const MappedFile &) = delete;
+    MappedFile &operator=(const MappedFile &) = delete;
+};
 
 inline std::string read_file_text(const std::string &path, bool compressed)
 {
