@@ -659,7 +659,7 @@ def panel_arm(args, rank: int):
     # picks (minimizer lines at 2 keys per sector for 16 <= k <= 27, hash
     # sectors at the tuned load otherwise)
     kpb = args.panel_keys_per_bucket
-    kpb_est = kpb or (2.0 if 16 <= k <= 27 else ib.get_tuning().panel_keys_per_bucket)
+    kpb_est = kpb or (1.5 if 16 <= k <= 27 else ib.get_tuning().panel_keys_per_bucket)
     free, _ = torch.cuda.mem_get_info()
     max_codes = max(sample_codes_bound(i) for i in range(len(w.samples))) * 8
     rows_bytes = n_win * len(w.samples) * 24 + 64 * n_win * len(w.samples)
@@ -910,7 +910,7 @@ def served_arm(args, rank: int):
     # picks (minimizer lines at 2 keys per sector for 16 <= k <= 27, hash
     # sectors at the tuned load otherwise)
     kpb = args.panel_keys_per_bucket
-    kpb_est = kpb or (2.0 if 16 <= k <= 27 else ib.get_tuning().panel_keys_per_bucket)
+    kpb_est = kpb or (1.5 if 16 <= k <= 27 else ib.get_tuning().panel_keys_per_bucket)
     free, _ = torch.cuda.mem_get_info()
     budget = free - max_bound * 8 - (4 << 30) - (8 << 30)
     union_of = {}

@@ -16,7 +16,7 @@ namespace panel {
 // Default load of joint minimizer-line tables: keys per 5-slot sector (the
 // keys of one minimizer crowd its line, so the load stays below the hash
 // sectors' 3)
-constexpr double kPmKeysPerSector = 2.0;
+constexpr double kPmKeysPerSector = 1.5;
 constexpr uint64_t kBuildChunk = 1ull << 27; // keys per build step (1 GiB of scratch each way)
 
 // Slot of fingerprint fp among sector w's first count slots, or -1.

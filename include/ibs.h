@@ -235,9 +235,9 @@ ibs_status ibs_scan_panel(ibs_table *const *tables, uint32_t n_tables, ibs_refer
  * sample masks per 32-byte sector, any k); 7 = the same sectors on minimizer
  * lines (16 <= k <= 27, at least 2^(2k-28) lines; consecutive positions
  * share 128-byte lines, a full sector spills into its partner sector, then
- * the stash; default load 2 keys per sector); 0 = 7 where it applies and its
+ * the stash; default load 1.5 keys per sector); 0 = 7 where it applies and its
  * minimum size does not oversize the table, else 3. opts->keys_per_bucket: keys
- * per sector (0 = the tuned panel_keys_per_bucket for 3, 2.0 for 7). Samples are added one at a
+ * per sector (0 = the tuned panel_keys_per_bucket for 3, 1.5 for 7). Samples are added one at a
  * time (sample i = the i-th call); rows are sample-major:
  * rows[i * n_windows + w]. The scan is a persistent kernel over a work queue
  * of (window, position-range) spans; ibs_panel_table_scan_async captures it
