@@ -321,6 +321,7 @@ __global__ void k_serve_finalize(const FinItem *__restrict__ fin, uint32_t n, co
 constexpr int kRing = kDepth;
 constexpr uint32_t kFinPerTicket = 256;
 enum : uint32_t { kExitNone = 0, kExitIdle = 1, kExitStop = 2, kExitTimeout = 3 };
+constexpr uint64_t kMaxWaitNs = 60ull * 1000000000ull; // the longest any one warp waits for its ticket
 
 struct BatchDesc {                 // host-written
     uint64_t seq;                  // batch number, from 1 (0: slot unused)
@@ -354,6 +355,7 @@ struct DevState {                  // device memory, zeroed before each launch
     unsigned int draining;
     unsigned int polling;          // held by the warp reading the host's control block
     unsigned int stop;             // device copy of the host's stop flag
+    unsigned long long lastGrowNs; // global time at which the poller last saw the count grow
 };
 
 
@@ -388,6 +390,8 @@ __device__ __forceinline__ uint64_t published_count(const Ctrl *ctrl, DevState *
         const uint64_t h = ld_acquire_sys(&ctrl->published);
         const uint32_t stop = *(volatile const uint32_t *)&ctrl->stop;
         __threadfence_system();
+        if (h > v)
+            atomicMax(&ds->lastGrowNs, (unsigned long long)global_ns());
         atomicMax(&ds->published, (unsigned long long)h);
         if (stop)
             atomicExch(&ds->stop, 1u);
@@ -416,8 +420,12 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
         if (lane == 0) {
             if (!*(volatile unsigned int *)&ds->draining && !*(volatile unsigned int *)&ds->stop) {
                 t = atomicAdd(&ds->ticket, 1ull);
-                // wait (bounded) until it is published
+                // wait (bounded) until it is published. The kernel is idle when
+                // the count has not grown for idleNs (tickets far ahead of the
+                // count wait through steady traffic); no single wait exceeds
+                // kMaxWaitNs; the spin count bounds the idle stretch as well
                 const uint64_t t0 = global_ns();
+                uint64_t idleFrom = t0;
                 for (uint64_t spin = 0;; ++spin) {
                     if (published_count(ctrl, ds) > t) {
                         go = 1;
@@ -425,13 +433,23 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                     }
                     if (*(volatile unsigned int *)&ds->draining || *(volatile unsigned int *)&ds->stop)
                         break;
-                    if (global_ns() - t0 > idleNs || spin > (idleNs >> 8) + 1024) {
+                    const uint64_t now = global_ns();
+                    const uint64_t grew = *(volatile unsigned long long *)&ds->lastGrowNs;
+                    if (grew > idleFrom) {
+                        idleFrom = grew;
+                        spin = 0;
+                    }
+                    if (now - idleFrom > idleNs || spin > (idleNs >> 8) + 1024 || now - t0 > kMaxWaitNs) {
                         if (atomicExch(&ds->draining, 1u) == 0u)
                             *(volatile uint32_t *)&status->exitReason = kExitIdle;
                         break;
                     }
                     __nanosleep(spin < 64 ? 256 : 2048);
                 }
+                // leaving: the ticket may have been published after the last
+                // refresh of the device copy; the host's count decides
+                if (!go && ld_acquire_sys(&ctrl->published) > t)
+                    go = 1;
             }
         }
         go = __shfl_sync(dev::FULL_MASK, go, 0);
