@@ -857,11 +857,12 @@ def served_arm(args, rank: int):
             n = len(reqs)
             for req in reqs:
                 srv.submit(*req)
-        deadline = time.time() + 1800
+        deadline = time.time() + 600
         while len(done) < n and time.time() < deadline:
             done += srv.poll(256, timeout_ms=1000)
         assert len(done) == n, f"served requests unfinished: {srv.stats()}"
         makespan = srv.now() - t_start
+        log(f"[served] rate {rate}: {n} requests in {makespan:.1f} s; stats {srv.stats()}")
         st = srv.stats()
         lat = np.array([r["done_time"] - r["submit_time"] for r in done])
         for r in done:

@@ -322,6 +322,8 @@ constexpr int kRing = kDepth;
 constexpr uint32_t kFinPerTicket = 256;
 enum : uint32_t { kExitNone = 0, kExitIdle = 1, kExitStop = 2, kExitTimeout = 3 };
 constexpr uint64_t kMaxWaitNs = 60ull * 1000000000ull; // the longest any one warp waits for its ticket
+constexpr uint64_t kDrainStallNs = 2000000ull;           // a fold gives up after the spans stall this long
+                                                         // while the kernel drains
 
 struct BatchDesc {                 // host-written
     uint64_t seq;                  // batch number, from 1 (0: slot unused)
@@ -524,12 +526,29 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                 atomicAdd(&ds->scanDone[slot], 1ull);
             continue;
         }
-        // a fold ticket: wait (bounded) for the batch's scans
+        // a fold ticket: wait (bounded) for the batch's scans. While the
+        // kernel drains, a scan ticket of this batch may have been given up
+        // by a leaving warp: when the count stops moving for kDrainStallNs
+        // the fold gives up too, and the host publishes the batch again to
+        // the next launch
         uint32_t ready = 1;
         if (lane == 0) {
             const uint64_t t0 = global_ns();
-            for (uint64_t spin = 0; *(volatile unsigned long long *)&ds->scanDone[slot] < nScan; ++spin) {
-                if (global_ns() - t0 > waitNs || spin > (waitNs >> 8) + 1024) {
+            uint64_t seen = 0, movedAt = t0;
+            for (uint64_t spin = 0;; ++spin) {
+                const uint64_t doneNow = *(volatile unsigned long long *)&ds->scanDone[slot];
+                if (doneNow >= nScan)
+                    break;
+                const uint64_t now = global_ns();
+                if (doneNow != seen) {
+                    seen = doneNow;
+                    movedAt = now;
+                }
+                if (*(volatile unsigned int *)&ds->draining && now - movedAt > kDrainStallNs) {
+                    ready = 0;
+                    break;
+                }
+                if (now - t0 > waitNs || spin > (waitNs >> 8) + 1024) {
                     ready = 0;
                     atomicExch(&ds->draining, 1u);
                     *(volatile uint32_t *)&status->exitReason = kExitTimeout;
