@@ -13,6 +13,9 @@
 namespace ibs {
 namespace panel {
 
+// Stash buckets an insert looks at before it fails (the stash then grows).
+constexpr uint64_t kStashProbe = 64;
+
 // Default load of joint minimizer-line tables: keys per 5-slot sector (the
 // keys of one minimizer crowd its line, so the load stays below the hash
 // sectors' 3)
@@ -142,7 +145,12 @@ __global__ void k_insert(View t, uint32_t *words, unsigned long long *stashWords
         atomicOr(w + 7, kStashFlag);
         uint64_t b = stash_home(code, t.stashBuckets);
         bool placed = false;
-        for (uint64_t s = 0; s < t.stashBuckets && !placed; ++s) {
+        // at most kStashProbe buckets from home: a crowded stash fails the
+        // insert (the host doubles it and inserts again) instead of costing a
+        // scan of the whole stash per key; lookups still stop at the first
+        // empty entry, which lies beyond every key placed this way
+        const uint64_t probes = t.stashBuckets < kStashProbe ? t.stashBuckets : kStashProbe;
+        for (uint64_t s = 0; s < probes && !placed; ++s) {
             for (int e = 0; e < 2 && !placed; ++e) {
                 unsigned long long *entry = stashWords + 4 * b + 2 * e;
                 const unsigned long long prev = atomicCAS(entry, kStashEmpty, (unsigned long long)code);
@@ -462,10 +470,14 @@ extern "C" ibs_status ibs_panel_table_create(uint32_t k, uint64_t expected_keys,
         g.nBuckets = nb;
         g.fpBits = (uint32_t)std::max<int>(1, (int)g.bits - (int)(63 - __builtin_clzll(nb)));
     }
-    (void)lam;
     // keys per bucket are ~Poisson(expected / nBuckets); the stash holds the
     // expected overflow at <= 2/3 load (it grows during the build if needed)
-    const double over = (double)expected_keys * overflow_fraction((double)expected_keys / (double)nb);
+    // minimizer lines: the keys of one minimizer crowd its line, so far more
+    // than a Poisson share of them overflows (about 2% at 1.5 keys per
+    // sector, 10% at 3); sized here for twice that, the stash grows if needed
+    const double over = fmt == FMT_PANEL_MZ
+                            ? (double)expected_keys * std::min(0.5, 0.04 * lam / 1.5 * lam / 1.5 + 0.01)
+                            : (double)expected_keys * overflow_fraction((double)expected_keys / (double)nb);
     p->stashBuckets = next_pow2(std::max<uint64_t>(1u << 12, (uint64_t)(over * 0.75) + 1));
     g.stashBuckets = p->stashBuckets;
     IBS_CUDA(cudaMalloc(&p->buckets, nb * 32), "panel table alloc");

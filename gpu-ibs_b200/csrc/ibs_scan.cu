@@ -33,9 +33,10 @@ static std::mutex g_tuneMu;
 // plain 2 Gbp x 2.19e9 k-mers): minimizer table at 1.5 keys per 32-byte
 // sector, spans of 2048 positions, 2 blocks in flight, 512 threads, 16 CTAs
 // per SM.
-// Joint-table scans: spans of 8192 positions, 6 CTAs of 256 threads per SM,
-// 4 blocks in flight, 3 keys per 5-slot bucket.
-static ibs_tuning g_tune = {2048, 2, 512, 16, 1.5, FMT_MZ8, 0, 8192, 6, 3.0, 4, {0, 0, 0}};
+// Joint-table scans (the autotuner's best point on the 16-sample panel at
+// half size): spans of 8192 positions, 4 CTAs of 256 threads per SM, 2
+// blocks in flight, 3 keys per 5-slot bucket.
+static ibs_tuning g_tune = {2048, 2, 512, 16, 1.5, FMT_MZ8, 0, 8192, 4, 3.0, 2, {0, 0, 0}};
 
 const ibs_tuning &tuning() { return g_tune; }
 

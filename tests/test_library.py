@@ -162,6 +162,12 @@ def test_library_defaults_are_the_committed_tuning():
                 "table_format"):
         assert t[key] == best[key], key
     assert best["rows_equal"]
+    res = json.loads((ib.PKG_DIR / "tuning" / "b200.json").read_text())
+    pb = res["panel_best"]
+    for key in ("panel_span_len", "panel_ctas_per_sm", "panel_keys_per_bucket", "panel_blocks_in_flight",
+                "panel_pass_mb"):
+        assert t[key] == pb[key], key
+    assert res["panel"]["all_rows_equal"]
 
 
 def test_python_structs_match_the_c_header(tmp_path):
