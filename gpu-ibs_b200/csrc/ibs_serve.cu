@@ -358,6 +358,7 @@ struct DevState {                  // device memory, zeroed before each launch
     unsigned int polling;          // held by the warp reading the host's control block
     unsigned int stop;             // device copy of the host's stop flag
     unsigned long long lastGrowNs; // global time at which the poller last saw the count grow
+    BatchDesc desc[kRing];         // device copy of the ring's descriptors (seq 0 while rewritten)
 };
 
 
@@ -392,8 +393,32 @@ __device__ __forceinline__ uint64_t published_count(const Ctrl *ctrl, DevState *
         const uint64_t h = ld_acquire_sys(&ctrl->published);
         const uint32_t stop = *(volatile const uint32_t *)&ctrl->stop;
         __threadfence_system();
-        if (h > v)
+        if (h > v) {
+            // new batches: copy the ring's descriptors into device memory
+            // before the device count covers them. A host slot read while the
+            // host rewrites it (seq 0 or changed between the two reads) holds
+            // a batch not yet published and is left for a later copy
+            for (int i = 0; i < kRing; ++i) {
+                const uint64_t *src = reinterpret_cast<const uint64_t *>(&ctrl->slot[i]);
+                uint64_t w[kDescWords];
+                const uint64_t sq = ld_acquire_sys(src);
+                for (int j = 1; j < kDescWords; ++j)
+                    w[j] = *(const volatile uint64_t *)(src + j);
+                asm volatile("fence.acq_rel.sys;" ::: "memory");
+                const uint64_t sq2 = *(const volatile uint64_t *)src;
+                uint64_t *dst = reinterpret_cast<uint64_t *>(&ds->desc[i]);
+                if (!sq || sq != sq2 || *(volatile uint64_t *)dst == sq)
+                    continue;
+                *(volatile uint64_t *)dst = 0; // readers skip the slot while it changes
+                __threadfence();
+                for (int j = 1; j < kDescWords; ++j)
+                    *(volatile uint64_t *)(dst + j) = w[j];
+                __threadfence();
+                *(volatile uint64_t *)dst = sq;
+            }
+            __threadfence();
             atomicMax(&ds->lastGrowNs, (unsigned long long)global_ns());
+        }
         atomicMax(&ds->published, (unsigned long long)h);
         if (stop)
             atomicExch(&ds->stop, 1u);
@@ -471,16 +496,16 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                 t0 = 0;
                 n = 0;
                 if (lane < kRing) {
-                    // a slot the host is rewriting shows seq 0 or a different seq
-                    // on the second read (the host clears seq, writes the fields,
-                    // then stores the new seq): only a slot read whole counts
-                    const uint64_t *sp = &ctrl->slot[lane].seq;
-                    const uint64_t sq = ld_acquire_sys(sp);
-                    const volatile uint64_t *w = reinterpret_cast<const volatile uint64_t *>(&ctrl->slot[lane]);
+                    // the device copy of slot `lane`: a slot being rewritten
+                    // shows seq 0 or a different seq on the second read, and
+                    // only a slot read whole counts
+                    const volatile uint64_t *w = reinterpret_cast<const volatile uint64_t *>(&ds->desc[lane]);
+                    const uint64_t sq = w[0];
+                    __threadfence();
                     t0 = w[1];
                     const uint64_t c0 = w[2], c1 = w[3];
-                    asm volatile("fence.acq_rel.sys;" ::: "memory");
-                    const uint64_t sq2 = *(const volatile uint64_t *)sp;
+                    __threadfence();
+                    const uint64_t sq2 = w[0];
                     n = (sq && sq == sq2) ? (c0 & 0xffffffffu) + (c0 >> 32) + (c1 >> 32) : 0; // scan + fold tickets
                 }
                 hit = __ballot_sync(dev::FULL_MASK, lane < kRing && n && t >= t0 && t < t0 + n);
@@ -496,9 +521,9 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
             dT0 = __shfl_sync(dev::FULL_MASK, t0, slot);
             dEnd = dT0 + __shfl_sync(dev::FULL_MASK, n, slot);
             word = 0;
-            asm volatile("fence.acq_rel.sys;" ::: "memory"); // after the acquiring reads of the slot search
-            if (lane < kDescWords)
-                word = reinterpret_cast<const volatile uint64_t *>(&ctrl->slot[slot])[lane];
+            __threadfence();
+            if (lane < kDescWords) // a live batch's device slot does not change
+                word = reinterpret_cast<const volatile uint64_t *>(&ds->desc[slot])[lane];
         }
         // the descriptor's fields, from the lanes holding them
         BatchDesc d;
