@@ -358,6 +358,7 @@ struct DevState {                  // device memory, zeroed before each launch
     unsigned int polling;          // held by the warp reading the host's control block
     unsigned int stop;             // device copy of the host's stop flag
     unsigned long long lastGrowNs; // global time at which the poller last saw the count grow
+    unsigned long long lastWorkNs; // global time at which a warp last finished a ticket
     BatchDesc desc[kRing];         // device copy of the ring's descriptors (seq 0 while rewritten)
 };
 
@@ -460,10 +461,14 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                     }
                     if (*(volatile unsigned int *)&ds->draining || *(volatile unsigned int *)&ds->stop)
                         break;
+                    // idle: neither new work published nor any ticket finished
+                    // (a long batch keeps the kernel busy, not idle)
                     const uint64_t now = global_ns();
                     const uint64_t grew = *(volatile unsigned long long *)&ds->lastGrowNs;
-                    if (grew > idleFrom) {
-                        idleFrom = grew;
+                    const uint64_t worked = *(volatile unsigned long long *)&ds->lastWorkNs;
+                    const uint64_t active = grew > worked ? grew : worked;
+                    if (active > idleFrom) {
+                        idleFrom = active;
                         spin = 0;
                     }
                     if (now - idleFrom > idleNs || spin > (idleNs >> 8) + 1024 || now - t0 > kMaxWaitNs) {
@@ -474,9 +479,15 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                     __nanosleep(spin < 64 ? 256 : 2048);
                 }
                 // leaving: the ticket may have been published after the last
-                // refresh of the device copy; the host's count decides
+                // refresh of the device copy; the host's count decides, and
+                // then the device copy (descriptors included) is refreshed
                 if (!go && ld_acquire_sys(&ctrl->published) > t)
-                    go = 1;
+                    for (int a = 0; a < (1 << 16) && !go; ++a) {
+                        if (published_count(ctrl, ds) > t)
+                            go = 1;
+                        else
+                            __nanosleep(256);
+                    }
             }
         }
         go = __shfl_sync(dev::FULL_MASK, go, 0);
@@ -547,8 +558,10 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
             }
             __threadfence(); // every lane's summaries are visible before the count
             __syncwarp();
-            if (lane == 0)
+            if (lane == 0) {
                 atomicAdd(&ds->scanDone[slot], 1ull);
+                atomicMax(&ds->lastWorkNs, (unsigned long long)global_ns());
+            }
             continue;
         }
         // a fold ticket: wait (bounded) for the batch's scans. While the
@@ -593,6 +606,7 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
         __threadfence_system(); // every lane's rows reach host memory before the batch is stamped done
         __syncwarp();
         if (lane == 0) {
+            atomicMax(&ds->lastWorkNs, (unsigned long long)global_ns());
             if (atomicAdd(&ds->finDone[slot], 1ull) + 1 == d.nFinTickets) {
                 // the batch's last fold: its counters are free for the slot's next batch
                 ds->scanDone[slot] = 0;
