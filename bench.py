@@ -850,7 +850,10 @@ def served_arm(args, rank: int):
             for req, g in zip(reqs[:n], unit_gaps[:n] / rate):
                 t_next += g
                 while time.perf_counter() < t_next:
-                    done += srv.poll(256, timeout_ms=0)
+                    try:
+                        done += srv.poll(256, timeout_ms=0)
+                    except ib.IbsError as e:
+                        raise RuntimeError(f"{e}; stats {srv.stats()}") from e
                     time.sleep(0.0002)
                 srv.submit(*req)
         else:
@@ -891,20 +894,21 @@ def served_arm(args, rank: int):
     # plain path: per-sample tables in the plain scan's layout (minimizer
     # lines at the tuned load), one request per launch. The budget leaves
     # room for registering a sample (its codes and a transient table)
-    free, _ = torch.cuda.mem_get_info()
-    transient = max_bound * 8 + ib.table_bytes_for(max(n_keys), k) * 2 + (4 << 30)
-    srv = ib.Server(ref, W, k, memory_budget=int(free - transient), one_request_per_launch=True)
-    for i in range(n_samples):
-        buf, n = codes(i)
-        srv.add_codes(buf.data_ptr(), n, on_device=True)
-        del buf
+    if "plain" in args.serve_modes:
+        free, _ = torch.cuda.mem_get_info()
+        transient = max_bound * 8 + ib.table_bytes_for(max(n_keys), k) * 2 + (4 << 30)
+        srv = ib.Server(ref, W, k, memory_budget=int(free - transient), one_request_per_launch=True)
+        for i in range(n_samples):
+            buf, n = codes(i)
+            srv.add_codes(buf.data_ptr(), n, on_device=True)
+            del buf
+            torch.cuda.empty_cache()
+        out["plain_tables_gb"] = srv.stats()["resident_bytes"] / 1e9
+        for r in rates:
+            out[f"plain_poisson_{r:g}"] = run(srv, r)
+        out["plain_saturated"] = run(srv, None)
+        srv.close()
         torch.cuda.empty_cache()
-    out["plain_tables_gb"] = srv.stats()["resident_bytes"] / 1e9
-    for r in rates:
-        out[f"plain_poisson_{r:g}"] = run(srv, r)
-    out["plain_saturated"] = run(srv, None)
-    srv.close()
-    torch.cuda.empty_cache()
 
     # batched: joint panel tables (as many samples per table as memory allows)
     # joint-table load: the flag, else the library's default for the layout it
@@ -951,6 +955,8 @@ def served_arm(args, rank: int):
         out[f"batched_poisson_{r:g}"] = run(srv, r)
     out["batched_saturated"] = run(srv, None)
     srv.close()
+    if "plain" not in args.serve_modes:
+        return out
     out["saturated_speedup_vs_plain"] = (out["batched_saturated"]["probes_per_s"] /
                                          out["plain_saturated"]["probes_per_s"])
     out["p99_ratio_batched_over_plain"] = {f"{r:g}": out[f"batched_poisson_{r:g}"]["latency_p99_s"] /
@@ -1249,6 +1255,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rates", default="5,20,50",
                     help="Poisson arrival rates (req/s); the highest runs every request")
+    ap.add_argument("--serve-modes", default="plain,batched",
+                    help="which servers the served stream runs (plain: one request per launch)")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="arrival time of the request prefix run at the lower rates")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="reference length scale")

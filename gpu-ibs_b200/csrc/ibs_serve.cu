@@ -348,6 +348,8 @@ struct Status {                    // pinned host memory, written by the kernel
     uint64_t doneSeq[kRing];       // last batch completed in each slot
     uint64_t tFirst[kRing], tDone[kRing]; // global timer (ns) of a batch's first claim and its completion
     uint32_t exitReason, pad;
+    unsigned long long lookupFailures; // published tickets whose batch descriptor was not found
+    unsigned long long foldGiveups;    // folds that gave up on stalled spans while the launch drained
 };
 
 struct DevState {                  // device memory, zeroed before each launch
@@ -525,6 +527,7 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                 if (lane == 0) {
                     atomicExch(&ds->draining, 1u);
                     *(volatile uint32_t *)&status->exitReason = kExitTimeout;
+                    atomicAdd_system(&status->lookupFailures, 1ull);
                 }
                 return;
             }
@@ -584,6 +587,7 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                 }
                 if (*(volatile unsigned int *)&ds->draining && now - movedAt > kDrainStallNs) {
                     ready = 0;
+                    atomicAdd_system(&status->foldGiveups, 1ull);
                     break;
                 }
                 if (now - t0 > waitNs || spin > (waitNs >> 8) + 1024) {
@@ -1013,6 +1017,8 @@ void pump(ibs_server *s)
             s->st.idle_exits++;
         else if (why == kExitTimeout)
             s->st.wait_timeouts++;
+        s->st.lookup_failures = *(volatile unsigned long long *)&s->status->lookupFailures;
+        s->st.fold_giveups = *(volatile unsigned long long *)&s->status->foldGiveups;
     }
     // batches the kernel stamped done, completed in batch order: a request's
     // rows can come from several batches, and it completes with the last

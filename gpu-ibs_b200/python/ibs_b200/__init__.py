@@ -67,7 +67,8 @@ class ServerStats(C.Structure):
                                           "reload_bytes", "evictions", "resident_bytes", "resident_tables")] + \
                [(n, C.c_double) for n in ("busy_seconds", "latency_p50", "latency_p99", "latency_max")] + \
                [(n, C.c_uint64) for n in ("failed", "queued", "running", "scanned", "sample_probes",
-                                          "persistent_launches", "idle_exits", "wait_timeouts", "replays")]
+                                          "persistent_launches", "idle_exits", "wait_timeouts", "replays",
+                                          "lookup_failures", "fold_giveups")]
 
 
 class Tuning(C.Structure):

@@ -330,6 +330,8 @@ typedef struct ibs_server_stats {
     uint64_t idle_exits;              /* ... that ended after idle_exit_us without new work */
     uint64_t wait_timeouts;           /* ... that ended because a bounded device wait ran out */
     uint64_t replays;                 /* batches published again after their launch ended early */
+    uint64_t lookup_failures;         /* published tickets whose batch the kernel did not find (ends it) */
+    uint64_t fold_giveups;            /* folds that gave up on stalled spans while a launch was ending */
 } ibs_server_stats;
 
 ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t k, const ibs_server_opts *opts,
