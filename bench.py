@@ -933,7 +933,9 @@ def served_arm(args, rank: int):
         cur.append(i)
     groups.append(cur)
     del sampled
-    srv = ib.Server(ref, W, k, memory_budget=int(free - max_bound * 8 - (8 << 30)))
+    persistent = "persistent" in args.serve_modes
+    srv = ib.Server(ref, W, k, memory_budget=int(free - max_bound * 8 - (8 << 30)), persistent_launch=persistent)
+    out["batched_launch"] = "one persistent launch" if persistent else "per loop iteration"
     id_of, joint_fmt = {}, []
     for members in groups:
         pt = ib.PanelTable(k, union_of[tuple(members)], keys_per_bucket=kpb)
@@ -1256,7 +1258,8 @@ def main():
     ap.add_argument("--serve-rates", default="5,20,50",
                     help="Poisson arrival rates (req/s); the highest runs every request")
     ap.add_argument("--serve-modes", default="plain,batched",
-                    help="which servers the served stream runs (plain: one request per launch)")
+                    help="which servers the served stream runs (plain: one request per launch; "
+                         "adding persistent feeds the batched server's work to one persistent launch)")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="arrival time of the request prefix run at the lower rates")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="reference length scale")

@@ -464,7 +464,9 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                     if (*(volatile unsigned int *)&ds->draining || *(volatile unsigned int *)&ds->stop)
                         break;
                     // idle: neither new work published nor any ticket finished
-                    // (a long batch keeps the kernel busy, not idle)
+                    // (a long batch keeps the kernel busy, not idle). Another
+                    // warp may stamp its work after `now` was read: the quiet
+                    // time is then zero, not a wrapped difference
                     const uint64_t now = global_ns();
                     const uint64_t grew = *(volatile unsigned long long *)&ds->lastGrowNs;
                     const uint64_t worked = *(volatile unsigned long long *)&ds->lastWorkNs;
@@ -473,7 +475,8 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                         idleFrom = active;
                         spin = 0;
                     }
-                    if (now - idleFrom > idleNs || spin > (idleNs >> 8) + 1024 || now - t0 > kMaxWaitNs) {
+                    const uint64_t quietNs = now > idleFrom ? now - idleFrom : 0;
+                    if (quietNs > idleNs || spin > (idleNs >> 8) + 1024 || now - t0 > kMaxWaitNs) {
                         if (atomicExch(&ds->draining, 1u) == 0u)
                             *(volatile uint32_t *)&status->exitReason = kExitIdle;
                         break;

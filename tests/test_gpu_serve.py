@@ -141,6 +141,41 @@ def test_persistent_launch_ends_when_idle_and_comes_back(world):
     srv.close()
 
 
+def test_persistent_launch_batches_larger_than_its_grid(world):
+    """Batches of more span tickets than the persistent grid has warps (every
+    contig of every sample at once, all tables resident, no cap on the spans
+    of a batch): warps go round for further tickets while others wait, and
+    a warp that stamps its work while another reads the clock must not make
+    the launch look idle. Every batch finishes in its first launch (no
+    replay, no idle end before the stream is done), rows exact."""
+    lens = world["ref_spec"].lens
+    sizes = [ib.table_bytes_for(len(c), K) for c in world["samples"]]
+    srv = ib.Server(world["ref"], W, K, memory_budget=int(sum(sizes) * 1.3), persistent_launch=True)
+    for c in world["samples"]:
+        srv.add_codes(c, len(c), on_device=False)
+    reqs = []
+    for rnd in range(3):
+        for s in range(len(world["samples"])):
+            for c in range(len(lens)):
+                nw = ib.window_count(lens[c:c + 1], W, K)
+                if nw:
+                    reqs.append((s, c, 0, nw))
+    for req in reqs:
+        srv.submit(*req)
+    done, deadline = [], time.time() + 300
+    while len(done) < len(reqs) and time.time() < deadline:
+        done += srv.poll(64, timeout_ms=2000)
+    st = srv.stats()
+    assert len(done) == len(reqs), ("requests left unfinished", st)
+    for r in done:
+        assert r["status"] == 0
+        assert np.array_equal(r["rows"], expected(world, r)), (r["sample"], r["contig"])
+    # two span items per 5 kbp window: about 13,000 per round of requests
+    assert st["persistent_launches"] >= 1 and st["spans"] >= 10_000, st
+    assert st["replays"] == 0 and st["wait_timeouts"] == 0 and st["lookup_failures"] == 0, st
+    srv.close()
+
+
 @pytest.mark.parametrize("table_format,serial", [(4, False), (4, True), (6, False)])
 def test_minimizer_tables_alone_and_in_a_mix(world, table_format, serial):
     """The server's single-sample tables in the minimizer-line layouts (MZ8,
