@@ -894,21 +894,28 @@ def served_arm(args, rank: int):
     # plain path: per-sample tables in the plain scan's layout (minimizer
     # lines at the tuned load), one request per launch. The budget leaves
     # room for registering a sample (its codes and a transient table)
-    if "plain" in args.serve_modes:
+    # single: the same per-sample tables under the batching server (windows
+    # shared by pending requests of one sample are scanned once; no joint
+    # table), optional
+    for mode, serial in (("plain", True), ("single", False)):
+        if mode not in args.serve_modes:
+            continue
         free, _ = torch.cuda.mem_get_info()
         transient = max_bound * 8 + ib.table_bytes_for(max(n_keys), k) * 2 + (4 << 30)
-        srv = ib.Server(ref, W, k, memory_budget=int(free - transient), one_request_per_launch=True)
+        srv = ib.Server(ref, W, k, memory_budget=int(free - transient), one_request_per_launch=serial)
         for i in range(n_samples):
             buf, n = codes(i)
             srv.add_codes(buf.data_ptr(), n, on_device=True)
             del buf
             torch.cuda.empty_cache()
-        out["plain_tables_gb"] = srv.stats()["resident_bytes"] / 1e9
+        out[f"{mode}_tables_gb"] = srv.stats()["resident_bytes"] / 1e9
         for r in rates:
-            out[f"plain_poisson_{r:g}"] = run(srv, r)
-        out["plain_saturated"] = run(srv, None)
+            out[f"{mode}_poisson_{r:g}"] = run(srv, r)
+        out[f"{mode}_saturated"] = run(srv, None)
         srv.close()
         torch.cuda.empty_cache()
+    if "batched" not in args.serve_modes:
+        return out
 
     # batched: joint panel tables (as many samples per table as memory allows)
     # joint-table load: the flag, else the library's default for the layout it
@@ -963,6 +970,11 @@ def served_arm(args, rank: int):
                                          out["plain_saturated"]["probes_per_s"])
     out["p99_ratio_batched_over_plain"] = {f"{r:g}": out[f"batched_poisson_{r:g}"]["latency_p99_s"] /
                                            out[f"plain_poisson_{r:g}"]["latency_p99_s"] for r in rates}
+    if "single" in args.serve_modes:
+        out["single_saturated_speedup_vs_plain"] = (out["single_saturated"]["probes_per_s"] /
+                                                    out["plain_saturated"]["probes_per_s"])
+        out["p99_ratio_single_over_plain"] = {f"{r:g}": out[f"single_poisson_{r:g}"]["latency_p99_s"] /
+                                              out[f"plain_poisson_{r:g}"]["latency_p99_s"] for r in rates}
     out["parity"] = {"status": "bit-exact" if ref_check is None or ref_check["status"] == "bit-exact"
                      else "MISMATCH",
                      "single_sample": "every served row equals the same window of its sample's full "
@@ -1259,6 +1271,7 @@ def main():
                     help="Poisson arrival rates (req/s); the highest runs every request")
     ap.add_argument("--serve-modes", default="plain,batched",
                     help="which servers the served stream runs (plain: one request per launch; "
+                         "batched: joint tables; single: the batching server over per-sample tables; "
                          "adding persistent feeds the batched server's work to one persistent launch)")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="arrival time of the request prefix run at the lower rates")
