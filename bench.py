@@ -940,9 +940,10 @@ def served_arm(args, rank: int):
         cur.append(i)
     groups.append(cur)
     del sampled
-    persistent = "persistent" in args.serve_modes
-    srv = ib.Server(ref, W, k, memory_budget=int(free - max_bound * 8 - (8 << 30)), persistent_launch=persistent)
-    out["batched_launch"] = "one persistent launch" if persistent else "per loop iteration"
+    per_iteration = "iterations" in args.serve_modes
+    srv = ib.Server(ref, W, k, memory_budget=int(free - max_bound * 8 - (8 << 30)),
+                    iteration_launches=per_iteration)
+    out["batched_launch"] = "per loop iteration" if per_iteration else "one persistent launch"
     id_of, joint_fmt = {}, []
     for members in groups:
         pt = ib.PanelTable(k, union_of[tuple(members)], keys_per_bucket=kpb)
@@ -1272,7 +1273,8 @@ def main():
     ap.add_argument("--serve-modes", default="plain,batched",
                     help="which servers the served stream runs (plain: one request per launch; "
                          "batched: joint tables; single: the batching server over per-sample tables; "
-                         "adding persistent feeds the batched server's work to one persistent launch)")
+                         "adding iterations launches the batched server's kernels per loop iteration "
+                         "instead of feeding one persistent launch)")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="arrival time of the request prefix run at the lower rates")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="reference length scale")

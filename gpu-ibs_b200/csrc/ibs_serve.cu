@@ -762,7 +762,7 @@ struct ibs_server {
     Launch launches[kDepth];
     int nextLaunch = 0;
     int sms = 148;
-    // the persistent launch (batched mode with persistent_launch)
+    // the persistent launch (batched mode unless iteration_launches)
     bool persistent = false;
     cudaStream_t copy = nullptr;          // item uploads while the kernel runs
     Ctrl *ctrl = nullptr;                 // pinned, mapped
@@ -1567,7 +1567,7 @@ extern "C" ibs_status ibs_server_create(ibs_reference *ref, uint32_t W, uint32_t
         if (opts->idle_exit_us)
             s->idleNs = (uint64_t)opts->idle_exit_us * 1000;
     }
-    s->persistent = !s->serial && opts && opts->persistent_launch;
+    s->persistent = !s->serial && !(opts && opts->iteration_launches);
     cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
     size_t fr = 0, tot = 0;
     IBS_CUDA(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");

@@ -53,7 +53,7 @@ class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("memory_budget", C.c_uint64), ("max_spans_per_launch", C.c_uint32),
                 ("min_spans_per_request", C.c_uint32), ("one_request_per_launch", C.c_uint32),
                 ("table_format", C.c_uint32), ("keys_per_bucket", C.c_double),
-                ("persistent_launch", C.c_uint32), ("idle_exit_us", C.c_uint32)]
+                ("iteration_launches", C.c_uint32), ("idle_exit_us", C.c_uint32)]
 
 
 class RequestResult(C.Structure):
@@ -633,11 +633,11 @@ class Server:
 
     def __init__(self, ref: Reference, W: int, k: int, memory_budget: int = 0, max_spans_per_launch: int = 0,
                  min_spans_per_request: int = 0, device: int = 0, one_request_per_launch: bool = False,
-                 table_format: int = 0, keys_per_bucket: float = 0.0, persistent_launch: bool = False,
+                 table_format: int = 0, keys_per_bucket: float = 0.0, iteration_launches: bool = False,
                  idle_exit_us: int = 0):
         self.ref = ref
         opts = ServerOpts(device, memory_budget, max_spans_per_launch, min_spans_per_request,
-                          int(one_request_per_launch), table_format, keys_per_bucket, int(persistent_launch),
+                          int(one_request_per_launch), table_format, keys_per_bucket, int(iteration_launches),
                           idle_exit_us)
         h = vp()
         _check(_ibs_srv_create(ref.handle, W, k, C.byref(opts), C.byref(h)))

@@ -275,7 +275,7 @@ void ibs_panel_table_close(ibs_panel_table *p);
  *
  * The server owns a background thread; submit/poll are thread-safe.
  *
- * With persistent_launch, batched mode feeds ONE persistent kernel: the loop publishes each
+ * Batched mode feeds ONE persistent kernel: the loop publishes each
  * iteration's work (span items over the tables, then the rows to fold) as a
  * batch into a ring in pinned host memory; the resident kernel's warps claim
  * the work in order, fold rows straight into pinned host memory and stamp
@@ -284,10 +284,8 @@ void ibs_panel_table_close(ibs_panel_table *p);
  * idle_exit_us the kernel ends (the next request launches it again), and a
  * fold that waits too long for its batch's scans ends it with a timeout
  * (counted in ibs_server_stats; unfinished batches are published to the
- * next launch). By default batched mode launches the span, joint and fold
- * kernels once per loop iteration, each launch carrying the work of every
- * runnable request; one request per launch (the plain path) launches them
- * per request. */
+ * next launch). One request per launch (the plain path) launches kernels
+ * per request instead. */
 typedef struct ibs_server ibs_server;
 
 typedef struct ibs_server_opts {
@@ -300,8 +298,8 @@ typedef struct ibs_server_opts {
                                    0 = the tuned default (ibs_tuning.table_format: minimizer lines for
                                    large tables), else as ibs_table_opts.force_format */
     double keys_per_bucket;     /* load of those tables (0 = the library default) */
-    uint32_t persistent_launch; /* batched mode: 1 = feed one persistent launch (below) instead of
-                                   launching kernels per loop iteration (0, the default) */
+    uint32_t iteration_launches; /* batched mode: 1 = launch kernels per loop iteration instead of
+                                    feeding one persistent launch */
     uint32_t idle_exit_us;      /* the persistent launch ends after this long without new work
                                    (0 = 100 ms); the next request launches it again */
 } ibs_server_opts;

@@ -45,13 +45,13 @@ def expected(world, r):
     return rows[a:a + r["n_windows"]]
 
 
-def make_server(world, budget_tables=2.5, table_format=0, serial=False, persistent_launch=False,
+def make_server(world, budget_tables=2.5, table_format=0, serial=False, iteration_launches=False,
                 idle_exit_us=0):
     sizes = [ib.table_bytes_for(len(c), K, force_format=table_format) for c in world["samples"]]
     budget = int(max(sizes) * budget_tables)
     srv = ib.Server(world["ref"], W, K, memory_budget=budget, max_spans_per_launch=512, min_spans_per_request=8,
                     table_format=table_format, one_request_per_launch=serial,
-                    persistent_launch=persistent_launch, idle_exit_us=idle_exit_us)
+                    iteration_launches=iteration_launches, idle_exit_us=idle_exit_us)
     ids = [srv.add_codes(c, len(c), on_device=False) for c in world["samples"]]
     assert ids == list(range(len(world["samples"])))
     return srv
@@ -82,11 +82,11 @@ def test_requests_alone_equal_full_scan_rows(world):
     srv.close()
 
 
-@pytest.mark.parametrize("persistent_launch", [False, True])
-def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world, persistent_launch):
-    """Batched serving, through one launch per loop iteration (the default)
-    and through the persistent launch."""
-    srv = make_server(world, budget_tables=2.2, persistent_launch=persistent_launch)
+@pytest.mark.parametrize("iteration_launches", [False, True])
+def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world, iteration_launches):
+    """Batched serving, through the persistent launch (default) and through
+    one launch per loop iteration."""
+    srv = make_server(world, budget_tables=2.2, iteration_launches=iteration_launches)
     reqs = random_requests(world, 300, 2) + [(s, 0, 0, 0) for s in range(6)]  # whole-contig requests too
     done = []
 
@@ -110,7 +110,7 @@ def test_requests_in_a_concurrent_mix_equal_full_scan_rows(world, persistent_lau
     assert st["completed"] == len(reqs)
     assert st["evictions"] > 0 and st["reloads"] > 0, st
     assert st["latency_p99"] >= st["latency_p50"] > 0
-    if not persistent_launch:
+    if iteration_launches:
         assert st["persistent_launches"] == 0
     else:
         # the whole burst went through a few resident launches, not one per iteration
@@ -124,7 +124,7 @@ def test_persistent_launch_ends_when_idle_and_comes_back(world):
     for longer than idle_exit_us the kernel ends by itself (the bound runs
     out and the kernel reports it), and the next request launches it again;
     results stay exact across the restarts."""
-    srv = make_server(world, idle_exit_us=2000, persistent_launch=True)
+    srv = make_server(world, idle_exit_us=2000)
     # requests on contigs with windows (a request on the empty contig completes
     # at submission, without a launch)
     reqs = [r for r in random_requests(world, 12, 21) if world["ref_spec"].lens[r[1]] > 0][:6]
@@ -150,7 +150,7 @@ def test_persistent_launch_batches_larger_than_its_grid(world):
     replay, no idle end before the stream is done), rows exact."""
     lens = world["ref_spec"].lens
     sizes = [ib.table_bytes_for(len(c), K) for c in world["samples"]]
-    srv = ib.Server(world["ref"], W, K, memory_budget=int(sum(sizes) * 1.3), persistent_launch=True)
+    srv = ib.Server(world["ref"], W, K, memory_budget=int(sum(sizes) * 1.3))
     for c in world["samples"]:
         srv.add_codes(c, len(c), on_device=False)
     reqs = []
