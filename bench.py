@@ -932,9 +932,14 @@ def served_arm(args, rank: int):
         union_of[tuple(members)] = u
         return u / kpb_est * 32 * 1.15
 
+    # a joint table holds as many samples as memory allows, or (--serve-group-gb)
+    # as fit under a size cap: a smaller table keeps a lone request's random
+    # probes inside the GPU's address-translation reach
+    cap = args.serve_group_gb * 1e9 if args.serve_group_gb else float("inf")
     groups, cur = [], []
     for i in range(n_samples):
-        if cur and sum(joint_bytes(g) for g in groups) + joint_bytes(cur + [i]) > budget:
+        if cur and (sum(joint_bytes(g) for g in groups) + joint_bytes(cur + [i]) > budget or
+                    joint_bytes(cur + [i]) > cap):
             groups.append(cur)
             cur = []
         cur.append(i)
@@ -1278,6 +1283,9 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="arrival time of the request prefix run at the lower rates")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="reference length scale")
+    ap.add_argument("--serve-group-gb", type=float, default=0.0,
+                    help="largest joint table of the batched server (GB; 0: as many samples per table "
+                         "as memory allows)")
     ap.add_argument("--admitted-only", action="store_true",
                     help="memory-admitted serving: 48 samples, tables ~3x the server's budget")
     ap.add_argument("--admit-samples", type=int, default=48)
