@@ -142,29 +142,62 @@ __device__ __forceinline__ void serve_single_item(const WorkItem &it, const Tabl
         sums[it.out] = acc;
 }
 
+// A run of up to 32 blocks of one sample, lane i holding block i's valid
+// (v) and hit (h) masks (empty past the run): the run's statistics, appended
+// to acc in lane 0 (the plain scan's lane-parallel fold, dev::LaneFold,
+// without its own accumulator).
+__device__ __forceinline__ void fold_run_into(SegStats &acc, uint32_t v, uint32_t h, int k)
+{
+    Seg32 s = block_seg32(v, h, k);
+#pragma unroll
+    for (uint32_t off = 1; off < 32; off <<= 1) {
+        Seg32 o;
+        o.total = __shfl_down_sync(dev::FULL_MASK, s.total, off);
+        o.obs = __shfl_down_sync(dev::FULL_MASK, s.obs, off);
+        o.lead = __shfl_down_sync(dev::FULL_MASK, s.lead, off);
+        o.trail = __shfl_down_sync(dev::FULL_MASK, s.trail, off);
+        o.gaps = __shfl_down_sync(dev::FULL_MASK, s.gaps, off);
+        o.dist = __shfl_down_sync(dev::FULL_MASK, s.dist, off);
+        s = seg32_combine(s, o, k);
+    }
+    acc = seg_combine(acc, seg_of(s), k);
+}
+
 // One work item over a joint table: one bucket load per position; lane j
 // keeps the statistics of sample j when j is in the item's mask, and the
-// requesting samples' summaries go to sums[it.out + rank].
-template <int NB>
+// requesting samples' summaries go to sums[it.out + rank]. An item that
+// requests one sample (a lone request's windows) folds it lane-parallel
+// instead: lane i keeps block i of every 32 and the run is summarised at
+// once, where the per-sample serial block summaries would leave 31 lanes
+// idle. K > 0 is the server's k, which every table of the server has (the
+// server refuses a table of another k): the minimizer window and masks are
+// then compile-time, and the minimizer-line layout is pruned where k rules
+// it out.
+template <int NB, uint32_t K = 0>
 __device__ __forceinline__ void serve_joint_item(const WorkItem &it, const panel::View &t,
                                                  const uint64_t *__restrict__ seq,
                                                  const uint64_t *__restrict__ mask, SegStats *__restrict__ sums,
                                                  uint32_t lane)
 {
-    const uint32_t k = t.g.k;
+    const uint32_t k = K ? K : t.g.k;
     const uint64_t kmask = key_mask(2 * k);
     const uint64_t kbits = (1ull << k) - 1;
     const uint32_t want = it.mask & 0xffffu;
+    const bool one = (want & (want - 1u)) == 0u; // warp-uniform
+    const uint32_t j0 = __ffs(want) - 1;
     // minimizer-line joint tables (PM) locate a k-mer through its minimizer:
     // m-mers read one block ahead, up to the span's last position's last
-    // m-mer (inside the window's bases)
-    const bool pm = t.g.format == FMT_PANEL_MZ;
+    // m-mer (inside the window's bases); that layout exists only for
+    // 16 <= k <= 27
+    constexpr bool kPmPossible = K == 0 || (K >= 16 && K <= 27);
+    const bool pm = kPmPossible && t.g.format == FMT_PANEL_MZ;
     const uint32_t w = pm ? mz::w_of(k) : 1, m = pm ? mz::m_of(k) : 0;
     const uint32_t lastM = it.p1 - 1 + (w - 1);
     dev::MzPos next;
     if (pm)
         next = dev::mz_pos(seq, mask, it.base + min(it.p0 + lane, lastM), k, m);
     SegStats acc = seg_empty();
+    uint32_t fv = 0, fh = 0; // one sample: this lane's block of the current run
     for (uint32_t p = it.p0; p < it.p1; p += 32 * NB) {
         uint4 v0[NB], v1[NB];
         uint64_t code[NB], rr[NB];
@@ -222,6 +255,19 @@ __device__ __forceinline__ void serve_joint_item(const WorkItem &it, const panel
                 }
             }
             const uint32_t V = __ballot_sync(dev::FULL_MASK, valid[b]);
+            if (one) {
+                const uint32_t H = __ballot_sync(dev::FULL_MASK, (m >> j0) & 1u);
+                const uint32_t blk = (((p - it.p0) >> 5) + b) & 31u; // warp-uniform
+                if (lane == blk) {
+                    fv = V;
+                    fh = H;
+                }
+                if (blk == 31u) {
+                    fold_run_into(acc, fv, fh, (int)k);
+                    fv = fh = 0;
+                }
+                continue;
+            }
             uint32_t myH = 0;
             for (uint32_t rest = want; rest; rest &= rest - 1) { // warp-uniform
                 const uint32_t j = __ffs(rest) - 1;
@@ -232,6 +278,14 @@ __device__ __forceinline__ void serve_joint_item(const WorkItem &it, const panel
             if ((want >> lane) & 1u)
                 acc = seg_combine(acc, panel::block_stats_serial(V, myH, (int)k), (int)k);
         }
+    }
+    if (one) {
+        // the last, partial run (lanes past it hold empty blocks)
+        if (__any_sync(dev::FULL_MASK, fv != 0))
+            fold_run_into(acc, fv, fh, (int)k);
+        if (lane == 0)
+            sums[it.out] = acc;
+        return;
     }
     if ((want >> lane) & 1u)
         sums[it.out + __popc(want & ((1u << lane) - 1u))] = acc;
@@ -560,7 +614,7 @@ __global__ void __launch_bounds__(256, 3) k_serve_persistent(const Ctrl *ctrl, S
                 serve_single_item<NB, K>(it, d.sv[it.view], seq, mask, d.sums, lane);
             } else {
                 const WorkItem it = d.joint[local - d.nSingle];
-                serve_joint_item<NB>(it, d.jv[it.view], seq, mask, d.sums, lane);
+                serve_joint_item<NB, K>(it, d.jv[it.view], seq, mask, d.sums, lane);
             }
             __threadfence(); // every lane's summaries are visible before the count
             __syncwarp();

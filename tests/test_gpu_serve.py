@@ -204,11 +204,14 @@ def test_minimizer_tables_alone_and_in_a_mix(world, table_format, serial):
     srv.close()
 
 
-def make_panel_server(world, serial=False):
-    """The six samples as one joint panel table, plus sample 0 once more as a
-    single-sample table (id 6), in one server."""
+def make_panel_server(world, serial=False, force_format=0):
+    """The six samples as one joint panel table (the library's layout for k,
+    or force_format), plus sample 0 once more as a single-sample table (id
+    6), in one server."""
     union = len(np.unique(np.concatenate(world["samples"])))
-    pt = ib.PanelTable(K, union)
+    pt = ib.PanelTable(K, union, force_format=force_format)
+    if force_format:
+        assert pt.info()[0].format == force_format
     for c in world["samples"]:
         pt.add_codes(c, len(c), on_device=False)
     srv = ib.Server(world["ref"], W, K, one_request_per_launch=serial)
@@ -231,9 +234,12 @@ def expected_any(world, r):
     return rows[a:a + r["n_windows"]]
 
 
-@pytest.mark.parametrize("serial", [False, True])
-def test_panel_server_alone_and_in_a_mix(world, serial):
-    srv = make_panel_server(world, serial)
+@pytest.mark.parametrize("serial,force_format", [(False, 0), (True, 0), (False, 3), (True, 3)])
+def test_panel_server_alone_and_in_a_mix(world, serial, force_format):
+    """Lone requests (one sample per work item: the lane-parallel fold) and
+    overlapping bursts (several samples per item) over a joint table, in the
+    minimizer-line layout (the default for k = 25) and in hash sectors."""
+    srv = make_panel_server(world, serial, force_format)
     # alone
     for req in random_requests(world, 10, 3):
         srv.submit(*req)
