@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(256, 4) k_serve_single(const TableView *__rest
     }
 }
 
-template <int NB>
+template <int NB, uint32_t K>
 __global__ void __launch_bounds__(256) k_serve_joint(const panel::View *__restrict__ views,
                                                      const WorkItem *__restrict__ items, uint32_t nItems,
                                                      const uint64_t *__restrict__ seq,
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(256) k_serve_joint(const panel::View *__restri
     const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = warp; i < nItems; i += nWarps) {
         const WorkItem it = items[i];
-        serve_joint_item<NB>(it, views[it.view], seq, mask, sums, lane);
+        serve_joint_item<NB, K>(it, views[it.view], seq, mask, sums, lane);
     }
 }
 
@@ -1472,8 +1472,15 @@ bool iterate(ibs_server *s)
     }
     if (nJoint) {
         const int grid = (int)std::min<uint64_t>((nJoint + 7) / 8, (uint64_t)s->sms * 8);
-        k_serve_joint<kNB><<<grid, 256, 0, st>>>(L.dJV, L.dJoint, nJoint, s->ref->dSeq, s->ref->dMask,
-                                                 L.dSums);
+        if (s->k == 25)
+            k_serve_joint<kNB, 25><<<grid, 256, 0, st>>>(L.dJV, L.dJoint, nJoint, s->ref->dSeq, s->ref->dMask,
+                                                         L.dSums);
+        else if (s->k == 31)
+            k_serve_joint<kNB, 31><<<grid, 256, 0, st>>>(L.dJV, L.dJoint, nJoint, s->ref->dSeq, s->ref->dMask,
+                                                         L.dSums);
+        else
+            k_serve_joint<kNB, 0><<<grid, 256, 0, st>>>(L.dJV, L.dJoint, nJoint, s->ref->dSeq, s->ref->dMask,
+                                                        L.dSums);
         IBS_LAUNCHED();
     }
     if (nFin) {
