@@ -80,7 +80,8 @@ IBS_HD uint64_t mulhi64(uint64_t a, uint64_t b)
 // ---------------------------------------------------------------------------
 enum : uint32_t {
     FMT_B8X32 = 1, FMT_B6X40 = 2, FMT_PANEL = 3, FMT_MZ8 = 4, FMT_AUTO_HASH = 5, FMT_MZ6 = 6,
-    FMT_PANEL_MZ = 7 // joint table: P5x48 sectors on minimizer lines (panel_core.cuh)
+    FMT_PANEL_MZ = 7, // joint table: P5x48 sectors on minimizer lines (panel_core.cuh)
+    FMT_WIDE = 8      // 33 <= k <= 64: whole 128-bit keys on 128-byte lines (wide_core.cuh)
 };
 // Minimizer-line tables: B8x32 sectors (31-bit slot values) or B6x40 sectors
 // (40-bit slot values, for larger k).
@@ -96,7 +97,7 @@ constexpr uint32_t B8_OVERFLOW_STASH = 0xfffffffdu;
 constexpr uint64_t STASH_EMPTY = ~0ull;
 
 struct TableGeom {
-    uint32_t k;        // k-mer length (<= 32)
+    uint32_t k;        // k-mer length (<= 32; <= 64 for FMT_WIDE)
     uint32_t bits;     // 2k
     uint32_t fpBits;   // stored fingerprint width
     uint32_t format;   // FMT_*

@@ -12,6 +12,7 @@
 #include "../../include/ibs.h"
 #include "ibs_core.cuh"
 #include "mz_core.cuh"
+#include "wide_core.cuh"
 
 namespace ibs {
 
@@ -39,8 +40,18 @@ ibs_status check_device_ordinal(int dev);
 // IBS_ERR_ARG with a message naming the contig instead.
 ibs_status check_contig_lengths(const uint64_t *lens, uint32_t n, const char *what);
 constexpr uint64_t kMaxContigLen = 2147483647ull;
-// Decodes a KMC 3 database into canonical codes in device memory (caller frees).
+// Decodes a KMC 3 database into canonical codes in device memory (caller
+// frees). decode_kmc takes k <= 32 (one word per code); decode_kmc_any also
+// takes 33 <= k <= 64, whose codes are two words each ({lo, hi}).
 ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodes, uint64_t *n, uint32_t *k);
+ibs_status decode_kmc_any(const char *prefix, int dev, uint64_t **dCodes, uint64_t *n, uint32_t *k);
+// Wide-key tables (ibs_wide.cu): the build from device codes ({lo, hi} per
+// key; the device must be current), membership counts, and the release of
+// the levels.
+ibs_status build_wide(ibs_table *t, const ulonglong2 *dCodes, uint64_t n, uint32_t k, const ibs_table_opts *o);
+ibs_status count_present_wide(ibs_table *t, const ulonglong2 *dCodes, uint64_t n, uint64_t *count);
+void free_wide(ibs_table *t);
+constexpr uint32_t kMaxWideK = 64;
 // Packed base offset of each contig (roundup64 of the lengths before it) and
 // the seq / mask word counts with their tail padding.
 void packed_offsets(const uint64_t *lens, uint32_t n, std::vector<uint64_t> &off, uint64_t &seqWords,
@@ -178,6 +189,7 @@ struct ibs_table {
     uint64_t nKeys = 0, stashKeys = 0;
     double buildSeconds = 0;
     uint64_t deviceBytes = 0;
+    ibs::wide::View wide{}; // the levels of a wide-key table (geom.format == FMT_WIDE)
     ibs::TableView view() const { return ibs::TableView{geom, buckets, stash}; }
 };
 

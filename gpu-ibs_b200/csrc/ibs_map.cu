@@ -5,7 +5,8 @@
 // :1544-1581). The reference accumulates +1/-1 into a per-contig difference
 // array and prefix-sums it; here a warp probes 32 starts per step and each
 // lane counts the hits among the k starts that cover its base straight from
-// the current and previous hit ballots (k <= 32). The output text (per
+// the current and previous hit ballots (k <= 32; three ballots for the
+// wide-key tables of 33 <= k <= 64). The output text (per
 // contig: the id, a newline, the coverage values joined by commas, a
 // newline; src/KmerDatabase.hpp:754-772, :1195-1203) is also written on the
 // device: each 8192-value tile is sized, the tile offsets are summed on the
@@ -75,6 +76,57 @@ __global__ void __launch_bounds__(256) k_map_spans(TableView t, const uint64_t *
             if (p + lane < sp.b)
                 cov[sp.out + p + lane] = (uint8_t)__popcll((M >> (33 + lane - k)) & kbits);
             prev = H;
+        }
+    }
+}
+
+// The same for a wide-key table (33 <= k <= 64): a base is covered by up to
+// 64 starts, so each lane counts from the current ballot and the two before
+// it (starts p - 64 .. p + 31). The reference's string-path mapper
+// (getMappingFromSequenceLegacy, src/KmerDatabase.hpp:803-848) adds 1 to the
+// k bases of every start whose canonical k-mer string the database holds.
+__device__ __forceinline__ bool hit_at_wide(const wide::View &t, const uint64_t *__restrict__ seq,
+                                            const uint64_t *__restrict__ mask, const Span &sp, uint32_t s, uint32_t k)
+{
+    if (s >= sp.nPos)
+        return false;
+    bool acgt;
+    uint64_t lo, hi;
+    wide::canonical_at(seq, mask, sp.base + s, k, acgt, lo, hi);
+    return acgt && wide::lookup(t, lo, hi);
+}
+
+__global__ void __launch_bounds__(256) k_map_spans_wide(wide::View t, const uint64_t *__restrict__ seq,
+                                                        const uint64_t *__restrict__ mask,
+                                                        const Span *__restrict__ spans, uint64_t nSpans,
+                                                        uint8_t *__restrict__ cov)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t k = t.k;
+    const uint64_t kbits = key_mask(k);
+    for (uint64_t i = warp; i < nSpans; i += nWarps) {
+        const Span sp = spans[i];
+        // hits of the 64 starts before the span (spans start at 0 or at a
+        // multiple of kSpan >= 64)
+        uint32_t prev1 = 0, prev2 = 0; // starts p - 32 .. p - 1 and p - 64 .. p - 33
+        if (sp.a >= 64) {
+            prev2 = __ballot_sync(dev::FULL_MASK, hit_at_wide(t, seq, mask, sp, sp.a - 64 + lane, k));
+            prev1 = __ballot_sync(dev::FULL_MASK, hit_at_wide(t, seq, mask, sp, sp.a - 32 + lane, k));
+        }
+        for (uint32_t p = sp.a; p < sp.b; p += 32) {
+            const uint32_t H = __ballot_sync(dev::FULL_MASK, hit_at_wide(t, seq, mask, sp, p + lane, k));
+            // bit j of (H : prev1 : prev2) is start p - 64 + j; base p + lane
+            // is covered by bits 65 + lane - k .. 64 + lane (1 <= low <= 96)
+            const uint64_t lowWord = ((uint64_t)prev1 << 32) | prev2;
+            const uint32_t low = 65 + lane - k;
+            const uint64_t x = low >= 64 ? ((uint64_t)H >> (low - 64))
+                                         : ((lowWord >> low) | ((uint64_t)H << (64 - low)));
+            if (p + lane < sp.b)
+                cov[sp.out + p + lane] = (uint8_t)__popcll(x & kbits);
+            prev2 = prev1;
+            prev1 = H;
         }
     }
 }
@@ -174,7 +226,9 @@ ibs_status coverage_device(ibs_table *t, const ibs_reference *ref, uint8_t *dCov
              "mapper span upload");
     const int grid = grid_for(spans.size(), 8); // 8 warps per block
     const TableView v = t->view();
-    if (t->geom.format == FMT_B8X32)
+    if (t->geom.format == FMT_WIDE)
+        k_map_spans_wide<<<grid, 256>>>(t->wide, ref->dSeq, ref->dMask, dSpans, spans.size(), dCov);
+    else if (t->geom.format == FMT_B8X32)
         k_map_spans<FMT_B8X32><<<grid, 256>>>(v, ref->dSeq, ref->dMask, dSpans, spans.size(), dCov);
     else if (t->geom.format == FMT_MZ8)
         k_map_spans<FMT_MZ8><<<grid, 256>>>(v, ref->dSeq, ref->dMask, dSpans, spans.size(), dCov);

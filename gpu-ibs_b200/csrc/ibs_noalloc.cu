@@ -287,7 +287,8 @@ extern "C" ibs_status ibs_scan_noalloc(ibs_table *t, const uint64_t *seq2bit_dev
         return IBS_ERR_ARG;
     }
     if (t->geom.format != FMT_B8X32 && t->geom.format != FMT_B6X40 && !is_mz(t->geom.format)) {
-        set_error("ibs_scan_noalloc: unknown table format");
+        set_error(t->geom.format == FMT_WIDE ? "ibs_scan_noalloc: wide-key tables (k > 32) take ibs_scan"
+                                             : "ibs_scan_noalloc: unknown table format");
         return IBS_ERR_UNSUPPORTED;
     }
     const uint32_t k = t->geom.k;

@@ -131,6 +131,51 @@ __global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t 
     }
 }
 
+// The scan over a wide-key table (33 <= k <= 64, format FMT_WIDE): the span
+// loop of k_scan_spans with each lane's k-mer read as a 128-bit canonical
+// code from three packed words and looked up level by level (wide_core.cuh).
+// Restates the reference's string path for these k: canonical k-mer strings
+// of the window (getCanonicalKmersLegacy, src/Utils.hpp:102-125: toupper,
+// k-mers with a non-ACGT byte skipped, the smaller of the k-mer and its
+// reverse complement) each looked up in the database
+// (getStatsFromSequenceLegacy, src/KmerDatabase.hpp:675-708), with the same
+// statistics fold.
+__global__ void __launch_bounds__(256) k_scan_spans_wide(wide::View t, const uint64_t *__restrict__ seq,
+                                                         const uint64_t *__restrict__ mask,
+                                                         const WinDesc *__restrict__ win,
+                                                         const uint32_t *__restrict__ span0, uint32_t nWin,
+                                                         uint64_t s0, uint64_t s1, uint32_t spanLen,
+                                                         SegStats *__restrict__ out)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t k = t.k;
+    for (uint64_t s = s0 + warp; s < s1; s += nWarps) {
+        const uint32_t w = window_of_span(span0, nWin, s);
+        const uint64_t base = win[w].base;
+        const uint32_t nPos = win[w].nPos;
+        const uint32_t p0 = (uint32_t)(s - __ldg(span0 + w)) * spanLen;
+        const uint32_t p1 = min(p0 + spanLen, nPos);
+        dev::LaneFold fold;
+        for (uint32_t p = p0; p < p1; p += 32) {
+            const uint32_t q = p + lane;
+            const bool inSpan = q < p1;
+            // lanes past the span read a position inside it and are masked out
+            const uint64_t G = base + (inSpan ? q : p0);
+            bool acgt;
+            uint64_t lo, hi;
+            wide::canonical_at(seq, mask, G, k, acgt, lo, hi);
+            const bool valid = inSpan && acgt;
+            const bool hit = valid && wide::lookup(t, lo, hi);
+            fold.push(__ballot_sync(FULL, valid), __ballot_sync(FULL, hit), lane, (int)k);
+        }
+        const SegStats acc = fold.finish((int)k);
+        if (lane == 0)
+            out[s] = acc;
+    }
+}
+
 // The scan over a minimizer-line table (formats MZ8 and MZ6): one warp per
 // span, the span's statistics from mz_span_stats (mz_scan.cuh). K > 0 fixes
 // k at compile time (the shifts and masks fold); K = 0 reads it from the
@@ -279,13 +324,27 @@ static void launch_spans_fmt(const ibs_table *t, const uint64_t *dSeq, const uin
     }
 }
 
+// The wide-key scan: 256 threads, enough CTAs for 64 warps per SM.
+static void launch_spans_wide(const ibs_table *t, const uint64_t *dSeq, const uint64_t *dMask, const ScanPlan &p,
+                              uint64_t s0, uint64_t s1, SegStats *dSpans, cudaStream_t st)
+{
+    const int threads = 256;
+    const uint64_t want = (s1 - s0 + 7) / 8;
+    const uint64_t cap = (uint64_t)sm_count() * 8;
+    const int grid = (int)std::max<uint64_t>(1, std::min(want, cap));
+    k_scan_spans_wide<<<grid, threads, 0, st>>>(t->wide, dSeq, dMask, p.dWin, p.dSpan0, (uint32_t)p.nWin, s0, s1,
+                                                p.spanLen, dSpans);
+}
+
 static ibs_status launch_spans(const ibs_table *t, const uint64_t *dSeq, const uint64_t *dMask,
                                const ScanPlan &p, uint64_t s0, uint64_t s1, SegStats *dSpans,
                                cudaStream_t st)
 {
     if (s1 <= s0)
         return IBS_OK;
-    if (t->geom.format == FMT_B8X32)
+    if (t->geom.format == FMT_WIDE)
+        launch_spans_wide(t, dSeq, dMask, p, s0, s1, dSpans, st);
+    else if (t->geom.format == FMT_B8X32)
         launch_spans_fmt<FMT_B8X32>(t, dSeq, dMask, p, s0, s1, dSpans, st);
     else if (t->geom.format == FMT_MZ8)
         launch_spans_fmt<FMT_MZ8>(t, dSeq, dMask, p, s0, s1, dSpans, st);

@@ -320,6 +320,40 @@ __global__ void k_decode(const uint8_t *__restrict__ raw, uint64_t r0, uint64_t 
     }
 }
 
+// The same for 33 <= k <= 64: the suffix (up to 16 bytes) and the prefix
+// shifted above it as a 128-bit code {lo, hi}; sufBits = 2 (k - p) > 0.
+__global__ void k_decode_wide(const uint8_t *__restrict__ raw, uint64_t r0, uint64_t nRec, uint32_t recBytes,
+                              uint32_t sufBytes, const uint64_t *__restrict__ lut, uint64_t lutN,
+                              uint64_t prefixMask, uint32_t sufBits, ulonglong2 *__restrict__ out)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nRec;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = r0 + i;
+        uint64_t lo = 0, hi = lutN - 1;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(lut + mid) <= r)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const uint8_t *q = raw + i * recBytes;
+        uint64_t slo = 0, shi = 0;
+        for (uint32_t b = 0; b < sufBytes; ++b) {
+            shi = (shi << 8) | (slo >> 56);
+            slo = (slo << 8) | q[b];
+        }
+        const uint64_t prefix = lo & prefixMask;
+        if (sufBits >= 64) {
+            shi |= prefix << (sufBits - 64);
+        } else {
+            slo |= prefix << sufBits;
+            shi |= prefix >> (64 - sufBits);
+        }
+        out[r] = make_ulonglong2(slo, shi);
+    }
+}
+
 template <uint32_t FMT>
 __global__ void k_probe(TableView t, const uint64_t *__restrict__ codes, uint64_t n,
                         uint8_t *__restrict__ hits)
@@ -485,7 +519,9 @@ static ibs_status check_markers(FILE *f, uint64_t size, const char *marker, cons
     return IBS_OK;
 }
 
-static ibs_status read_kmc_header(FILE *f, const std::string &path, KmcHeader &h)
+// maxK: 32 for the callers that take one-word codes, 64 for those that also
+// take wide-key codes.
+static ibs_status read_kmc_header(FILE *f, const std::string &path, KmcHeader &h, uint32_t maxK = 32)
 {
     h.fileBytes = file_size(f);
     ibs_status s = check_markers(f, h.fileBytes, "KMCP", path);
@@ -529,11 +565,12 @@ static ibs_status read_kmc_header(FILE *f, const std::string &path, KmcHeader &h
         set_error("KMC: Quake-compatible counters are not supported");
         return IBS_ERR_UNSUPPORTED;
     }
-    if (h.k == 0 || h.k > 32) {
-        set_error("KMC: k=" + std::to_string(h.k) + " is not supported (k must be 1..32)");
+    if (h.k == 0 || h.k > maxK) {
+        set_error("KMC: k=" + std::to_string(h.k) + " is not supported (k must be 1.." + std::to_string(maxK) +
+                  (maxK < kMaxWideK ? " here; wide-key tables take k up to 64)" : ")"));
         return IBS_ERR_UNSUPPORTED;
     }
-    if (h.p > h.k || (h.k - h.p) % 4 != 0 || h.k - h.p > 32) {
+    if (h.p > h.k || (h.k - h.p) % 4 != 0 || h.k - h.p > maxK || h.p > 31) {
         set_error("KMC: unexpected suffix geometry");
         return IBS_ERR_FORMAT;
     }
@@ -596,6 +633,17 @@ extern "C" uint64_t ibs_launch_count(void) { return launch_counter().load(); }
 
 static ibs_status check_format(uint32_t k, const ibs_table_opts *o)
 {
+    if (o && o->force_format == FMT_WIDE && k <= 32) {
+        set_error("wide-key tables (format 8) need 33 <= k <= 64");
+        return IBS_ERR_UNSUPPORTED;
+    }
+    if (k > 32) {
+        if (o && o->force_format && o->force_format != FMT_WIDE) {
+            set_error("k=" + std::to_string(k) + " > 32 takes only the wide-key table layout (format 8)");
+            return IBS_ERR_UNSUPPORTED;
+        }
+        return IBS_OK;
+    }
     if (o && o->force_format == FMT_MZ8 && (k < 16 || k > 27)) {
         set_error("minimizer-bucketed tables (format 4) need 16 <= k <= 27");
         return IBS_ERR_UNSUPPORTED;
@@ -604,7 +652,7 @@ static ibs_status check_format(uint32_t k, const ibs_table_opts *o)
         set_error("minimizer-bucketed tables with 40-bit slots (format 6) need 16 <= k <= 31");
         return IBS_ERR_UNSUPPORTED;
     }
-    if (o && (o->force_format > FMT_MZ6 || o->force_format == FMT_PANEL)) {
+    if (o && ((o->force_format > FMT_MZ6 && o->force_format != FMT_WIDE) || o->force_format == FMT_PANEL)) {
         set_error("unknown table format " + std::to_string(o->force_format));
         return IBS_ERR_ARG;
     }
@@ -617,7 +665,8 @@ extern "C" ibs_status ibs_table_from_codes(const uint64_t *codes, uint64_t n, ui
 {
     clear_error();
     if (!out || (!codes && n) || k == 0 || k > 32) {
-        set_error("ibs_table_from_codes: bad argument");
+        set_error(k > 32 ? "ibs_table_from_codes: k > 32 codes take two words (ibs_table_from_codes128)"
+                         : "ibs_table_from_codes: bad argument");
         return IBS_ERR_ARG;
     }
     *out = nullptr;
@@ -671,8 +720,10 @@ ibs_status ibs::check_device_ordinal(int dev)
 
 namespace ibs {
 // Decodes <prefix>.kmc_pre/.kmc_suf into canonical codes in device memory
-// (cudaMalloc'd; the caller frees *dCodes). The device must be current.
-ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_t *nOut, uint32_t *kOut)
+// (cudaMalloc'd; the caller frees *dCodes): one word per code for k <= 32,
+// {lo, hi} for 33 <= k <= maxK. The device must be current.
+static ibs_status decode_kmc_impl(const char *prefix, int dev, uint64_t **dCodesOut, uint64_t *nOut,
+                                  uint32_t *kOut, uint32_t maxK)
 {
     *dCodesOut = nullptr;
     const std::string pre = std::string(prefix) + ".kmc_pre";
@@ -685,7 +736,7 @@ ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_
             set_error("KMC: cannot open " + pre);
             return IBS_ERR_IO;
         }
-        ibs_status s = read_kmc_header(f.f, pre, h);
+        ibs_status s = read_kmc_header(f.f, pre, h, maxK);
         if (s != IBS_OK)
             return s;
         s = read_kmc_lut(f.f, pre, h, lut);
@@ -756,7 +807,8 @@ ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_
         if (st)
             cudaStreamDestroy(st);
     };
-    cudaError_t e = cudaMalloc(&dCodes, std::max<uint64_t>(total, 1) * 8);
+    const uint32_t codeWords = h.k > 32 ? 2 : 1;
+    cudaError_t e = cudaMalloc(&dCodes, std::max<uint64_t>(total, 1) * 8 * codeWords);
     if (e == cudaSuccess)
         e = cudaMalloc(&dLut, lut.size() * 8);
     if (e == cudaSuccess)
@@ -836,8 +888,13 @@ ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_
         e = cudaMemcpyAsync(dRaw[slot], hRaw[slot], nRec * recBytes, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess)
             break;
-        k_decode<<<grid_for(nRec, 256), 256, 0, st>>>(dRaw[slot], r0, nRec, recBytes, sufBytes, dLut, lutN,
-                                                      prefixMask, 2 * (h.k - h.p), dCodes);
+        if (codeWords == 2)
+            k_decode_wide<<<grid_for(nRec, 256), 256, 0, st>>>(dRaw[slot], r0, nRec, recBytes, sufBytes, dLut, lutN,
+                                                               prefixMask, 2 * (h.k - h.p),
+                                                               reinterpret_cast<ulonglong2 *>(dCodes));
+        else
+            k_decode<<<grid_for(nRec, 256), 256, 0, st>>>(dRaw[slot], r0, nRec, recBytes, sufBytes, dLut, lutN,
+                                                          prefixMask, 2 * (h.k - h.p), dCodes);
         IBS_LAUNCHED();
         e = cudaEventRecord(done[slot], st);
         {
@@ -861,6 +918,16 @@ ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodesOut, uint64_
     cleanup();
     return IBS_OK;
 }
+
+ibs_status decode_kmc(const char *prefix, int dev, uint64_t **dCodes, uint64_t *n, uint32_t *k)
+{
+    return decode_kmc_impl(prefix, dev, dCodes, n, k, 32);
+}
+
+ibs_status decode_kmc_any(const char *prefix, int dev, uint64_t **dCodes, uint64_t *n, uint32_t *k)
+{
+    return decode_kmc_impl(prefix, dev, dCodes, n, k, kMaxWideK);
+}
 } // namespace ibs
 
 extern "C" ibs_status ibs_open(const char *prefix, const ibs_table_opts *opts, ibs_table **out)
@@ -881,7 +948,7 @@ extern "C" ibs_status ibs_open(const char *prefix, const ibs_table_opts *opts, i
             set_error(std::string("KMC: cannot open ") + prefix + ".kmc_pre");
             return IBS_ERR_IO;
         }
-        ibs_status s = read_kmc_header(f.f, std::string(prefix) + ".kmc_pre", h);
+        ibs_status s = read_kmc_header(f.f, std::string(prefix) + ".kmc_pre", h, kMaxWideK);
         if (s != IBS_OK)
             return s;
         s = check_format(h.k, opts);
@@ -894,12 +961,15 @@ extern "C" ibs_status ibs_open(const char *prefix, const ibs_table_opts *opts, i
     DeviceGuard guard(dev);
     uint64_t *dCodes = nullptr, total = 0;
     uint32_t k = 0;
-    s = decode_kmc(prefix, dev, &dCodes, &total, &k);
+    s = decode_kmc_any(prefix, dev, &dCodes, &total, &k);
     if (s != IBS_OK)
         return s;
     std::unique_ptr<ibs_table> t(new ibs_table);
     t->device = dev;
-    s = build_from_device_codes(t.get(), dCodes, total, k, opts);
+    if (k > 32)
+        s = build_wide(t.get(), reinterpret_cast<const ulonglong2 *>(dCodes), total, k, opts);
+    else
+        s = build_from_device_codes(t.get(), dCodes, total, k, opts);
     cudaFree(dCodes);
     if (s != IBS_OK) {
         ibs_close(t.release());
@@ -936,6 +1006,10 @@ extern "C" ibs_status ibs_probe(ibs_table *t, const uint64_t *codes, uint64_t n,
     clear_error();
     if (!t || (n && (!codes || !hits))) {
         set_error("ibs_probe: bad argument");
+        return IBS_ERR_ARG;
+    }
+    if (t->geom.format == FMT_WIDE) {
+        set_error("ibs_probe: a wide-key table (k > 32) takes ibs_probe128");
         return IBS_ERR_ARG;
     }
     if (!n)
@@ -1004,6 +1078,11 @@ extern "C" ibs_status ibs_count_present(ibs_table *t, const uint64_t *codes, uin
         set_error("ibs_count_present: bad argument");
         return IBS_ERR_ARG;
     }
+    if (t->geom.format == FMT_WIDE) {
+        set_error("ibs_count_present: takes the 64-bit codes of k <= 32 tables (a wide-key table counts "
+                  "through ibs_count_present_kmc)");
+        return IBS_ERR_ARG;
+    }
     DeviceGuard guard(t->device);
     if (codes_on_device || !n)
         return count_present_device(t, codes, n, count);
@@ -1024,7 +1103,7 @@ extern "C" ibs_status ibs_count_present_kmc(ibs_table *t, const char *kmc_prefix
     DeviceGuard guard(t->device);
     uint64_t *d = nullptr, n = 0;
     uint32_t k = 0;
-    ibs_status s = decode_kmc(kmc_prefix, t->device, &d, &n, &k);
+    ibs_status s = decode_kmc_any(kmc_prefix, t->device, &d, &n, &k);
     if (s != IBS_OK)
         return s;
     std::unique_ptr<uint64_t, cudaError_t (*)(void *)> guard2(d, cudaFree);
@@ -1032,13 +1111,21 @@ extern "C" ibs_status ibs_count_present_kmc(ibs_table *t, const char *kmc_prefix
         set_error("K-mer lengths do not match");
         return IBS_ERR_ARG;
     }
+    if (t->geom.format == FMT_WIDE)
+        return count_present_wide(t, reinterpret_cast<const ulonglong2 *>(d), n, count);
     return count_present_device(t, d, n, count);
 }
 
 extern "C" uint64_t ibs_table_bytes_for(uint64_t n_keys, uint32_t k, const ibs_table_opts *opts)
 {
-    if (k == 0 || k > 32)
+    if (k == 0 || k > kMaxWideK)
         return 0;
+    if (k > 32) {
+        // level 0 at the load, plus about 1% for the later levels
+        const double lam = (opts && opts->keys_per_bucket > 0) ? opts->keys_per_bucket : 4.0;
+        const uint64_t lines = (uint64_t)((double)n_keys / lam) + 1;
+        return (lines + lines / 100 + 1) * wide::kSlots * 16;
+    }
     return choose_geometry(n_keys, k, opts).nBuckets * 32;
 }
 
@@ -1066,6 +1153,7 @@ extern "C" void ibs_close(ibs_table *t)
         DeviceGuard guard(t->device);
         cudaFree(t->buckets);
         cudaFree(t->stash);
+        free_wide(t);
     }
     delete t;
 }

@@ -343,10 +343,11 @@ template <typename T> struct DevBuf {
 // ---------------------------------------------------------------------------
 // KMC writer core
 // ---------------------------------------------------------------------------
-ibs_status check_kmc_spec(const ibs_kmc_spec *s)
+ibs_status check_kmc_spec(const ibs_kmc_spec *s, uint32_t maxK = 32)
 {
-    if (!s || s->k == 0 || s->k > 32 || s->p > s->k || (s->k - s->p) % 4 != 0 || s->p > 15)
-        return fail(IBS_ERR_ARG, "kmc spec: need k <= 32, p <= 15 and (k - p) % 4 == 0");
+    if (!s || s->k == 0 || s->k > maxK || s->p > s->k || (s->k - s->p) % 4 != 0 || s->p > 15)
+        return fail(IBS_ERR_ARG, "kmc spec: need k <= " + std::to_string(maxK) +
+                                     ", p <= 15 and (k - p) % 4 == 0");
     if (s->counter_size > 4)
         return fail(IBS_ERR_ARG, "kmc spec: counter_size must be 0..4");
     if (s->version != 0 && s->version != 0x200)
@@ -880,6 +881,82 @@ extern "C" ibs_status ibs_kmc_write(const char *prefix, const ibs_kmc_spec *s, c
     ok = ok && fwrite("KMCS", 1, 4, f) == 4;
     ok = (fclose(f) == 0) && ok;
     TCUDA(e, "kmc records");
+    if (!ok)
+        return fail(IBS_ERR_IO, "short write to " + suf);
+    if (n_written)
+        *n_written = total;
+    return write_pre(pre, s, lut, total);
+}
+
+// The writer for 33 <= k <= 64 (host only): the same files with 128-bit
+// codes. The signature of a k-mer (its KMC2 bin) is the smallest normalised
+// sig_len-mer over its bases, first base first, as for k <= 32.
+extern "C" ibs_status ibs_kmc_write128(const char *prefix, const ibs_kmc_spec *s, const ibs_code128 *codes,
+                                       uint64_t n, uint64_t *n_written)
+{
+    ibs_status st = check_kmc_spec(s, 64);
+    if (st != IBS_OK)
+        return st;
+    if (!prefix || (n && !codes))
+        return fail(IBS_ERR_ARG, "ibs_kmc_write128: bad argument");
+    if (s->k <= 32)
+        return fail(IBS_ERR_ARG, "ibs_kmc_write128: k <= 32 codes take ibs_kmc_write");
+    typedef unsigned __int128 u128;
+    const uint32_t k = s->k, p = s->p;
+    const uint32_t sufBytes = (k - p) / 4, sufBits = 2 * (k - p);
+    const uint32_t rec = sufBytes + s->counter_size;
+    const uint64_t single = 1ull << (2 * p);
+    const uint32_t nBins = s->version == 0x200 ? s->n_bins : 1;
+    const uint32_t sigLen = s->version == 0x200 ? s->sig_len : 0;
+    const uint32_t maxCount = max_count_of(s);
+    const std::string pre = std::string(prefix) + ".kmc_pre", suf = std::string(prefix) + ".kmc_suf";
+    const std::vector<uint32_t> norm = sigLen ? norm_table(sigLen) : std::vector<uint32_t>();
+    auto wide = [](const ibs_code128 &c) { return ((u128)c.hi << 64) | c.lo; };
+    auto signature = [&](u128 code) {
+        const uint32_t mmask = (1u << (2 * sigLen)) - 1;
+        uint32_t str = 0, best = 0xffffffffu;
+        for (uint32_t i = 0; i < k; ++i) {
+            str = ((str << 2) | (uint32_t)((code >> (2 * (k - 1 - i))) & 3)) & mmask;
+            if (i + 1 >= sigLen)
+                best = std::min(best, norm[str]);
+        }
+        return best;
+    };
+    // (bin, code) order, duplicates removed
+    std::vector<std::pair<uint32_t, u128>> keys(n);
+    parallel_for((n + (1 << 16) - 1) >> 16, hw_threads(), [&](uint64_t piece) {
+        const uint64_t a = piece << 16, b = std::min<uint64_t>(n, a + (1 << 16));
+        for (uint64_t i = a; i < b; ++i) {
+            const u128 c = wide(codes[i]);
+            keys[i] = {sigLen ? bin_of_signature(signature(c), nBins) : 0u, c};
+        }
+    });
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    std::vector<uint64_t> lut((uint64_t)nBins * single + 1, 0);
+    for (const auto &kv : keys)
+        lut[(uint64_t)kv.first * single + (uint64_t)(kv.second >> sufBits) + 1]++;
+    for (uint64_t i = 0; i + 1 < lut.size(); ++i)
+        lut[i + 1] += lut[i];
+    const uint64_t total = keys.size();
+    FILE *f = fopen(suf.c_str(), "wb");
+    if (!f)
+        return fail(IBS_ERR_IO, "cannot write " + suf);
+    bool ok = fwrite("KMCS", 1, 4, f) == 4;
+    std::vector<uint8_t> buf(std::max<uint64_t>(total, 1) * rec);
+    for (uint64_t i = 0; i < total; ++i) {
+        uint8_t *q = buf.data() + i * rec;
+        const u128 c = keys[i].second;
+        for (uint32_t x = 0; x < sufBytes; ++x)
+            q[x] = (uint8_t)(c >> (8 * (sufBytes - 1 - x)));
+        uint32_t cnt = count_of(s->count_seed, (uint64_t)c ^ (uint64_t)(c >> 64) * 0x9e3779b97f4a7c15ull);
+        cnt = cnt > maxCount ? maxCount : cnt;
+        for (uint32_t x = 0; x < s->counter_size; ++x)
+            q[sufBytes + x] = (uint8_t)(cnt >> (8 * x));
+    }
+    ok = ok && fwrite(buf.data(), 1, total * rec, f) == total * rec;
+    ok = ok && fwrite("KMCS", 1, 4, f) == 4;
+    ok = (fclose(f) == 0) && ok;
     if (!ok)
         return fail(IBS_ERR_IO, "short write to " + suf);
     if (n_written)

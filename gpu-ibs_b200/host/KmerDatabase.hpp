@@ -63,10 +63,24 @@ public:
     {
         info = ibs_host::read_kmc_info(this->sourcePath);
         kmerSize = info.kmerLength;
-        if (kmerSize > 32)
+        if (kmerSize > 64)
             throw std::runtime_error("k=" + std::to_string(kmerSize) +
-                                     " > 32: this scan packs a k-mer into 64 bits; the reference's "
-                                     "string path for k > 32 is not part of it");
+                                     " > 64: the device tables hold a k-mer in at most 128 bits");
+        if (kmerSize > 32)
+            announceWideKeys(kmerSize);
+    }
+
+    // k > 32: where the reference takes its string path for the whole process
+    // and says so once (routeToStringPath, src/KmerDatabase.hpp:114-124),
+    // the scan here builds a wide-key table (128-bit codes) on the device.
+    static void announceWideKeys(unsigned k)
+    {
+        static bool said = false;
+        if (said)
+            return;
+        said = true;
+        std::cerr << "[fastibs] k=" << k << " > 32: wide-key device tables (128-bit codes); "
+                  << "the --cpu and --probe options do not apply" << std::endl;
     }
 
     ~KmerDatabase() { releaseGpuIndex(); }

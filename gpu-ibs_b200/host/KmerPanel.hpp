@@ -43,6 +43,11 @@ public:
                                          members[0].name + " has k=" +
                                          std::to_string(members[0].db->getKmerSize()) +
                                          "; a panel shares one k");
+            // joint tables hold 64-bit codes; fastibs scans a k > 32 panel
+            // as single runs instead, as the reference does
+            if (m.db->getKmerSize() > 32)
+                throw std::runtime_error("KmerPanel: k=" + std::to_string(m.db->getKmerSize()) +
+                                         " > 32 has no panel path");
             members.push_back(std::move(m));
         }
     }

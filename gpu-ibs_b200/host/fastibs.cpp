@@ -188,6 +188,31 @@ int run_panel(vector<string> dirs, const vector<fs::path> &refs, const string &r
         names.push_back(name);
         prefixes.push_back(prefix);
     }
+    // k > 32: no joint table holds such k-mers, so the databases are scanned
+    // one at a time, writing the files a panel would (src/FastIBS.cpp:155-180);
+    // every member's k is read first, as a panel shares one k
+    try {
+        const uint32_t k = ibs_host::read_kmc_info(prefixes[0]).kmerLength;
+        for (size_t i = 1; i < prefixes.size(); i++) {
+            const uint32_t ki = ibs_host::read_kmc_info(prefixes[i]).kmerLength;
+            if (ki != k) {
+                cerr << "Error: KmerPanel: " << names[i] << " has k=" << ki << " but " << names[0] << " has k=" << k
+                     << "; a panel shares one k" << endl;
+                return 1;
+            }
+        }
+        if (k > 32) {
+            cout << "[panel] k=" << k << " > 32 has no panel path; scanning the " << dirs.size()
+                 << " databases one at a time" << endl;
+            int status = 0;
+            for (const string &dir : dirs)
+                status |= run_single(dir, refs, refPath, results, W);
+            return status;
+        }
+    } catch (const std::exception &e) {
+        cerr << "Error: " << e.what() << endl;
+        return 1;
+    }
     cout << "****Panel: " << dirs.size() << " databases" << endl;
     for (size_t i = 0; i < prefixes.size(); i++)
         cout << "  " << names[i] << " (" << prefixes[i] << ")" << endl;

@@ -49,7 +49,7 @@ void usage(const char *argv0)
          << "  database (by k-mer count) is decoded into a device table and every k-mer of\n"
          << "  the smaller one is probed against it on the GPU.\n\n"
          << "Notes:\n"
-         << "  - The databases must have the same k-mer size (k <= 32).\n"
+         << "  - The databases must have the same k-mer size (k <= 64; k > 32 builds a wide-key table).\n"
          << "  - Exit status: 0 with the count on stdout; 1 on a bad command line or\n"
          << "    database (one error line on stderr).\n"
          << "  - FASTIBS_GPU_DEVICE=N picks the CUDA device (default 0).\n"
@@ -89,8 +89,8 @@ int run(int argc, char **argv)
         cerr << "Error: K-mer lengths do not match" << endl;
         return 1;
     }
-    if (h1.kmerLength > 32) {
-        cerr << "Error: k = " << h1.kmerLength << " is above 32, which this program does not handle" << endl;
+    if (h1.kmerLength > 64) {
+        cerr << "Error: k = " << h1.kmerLength << " is above 64, which this program does not handle" << endl;
         return 1;
     }
     // small (enumerated) = db1, big (probed) = db2 after the reference's rule

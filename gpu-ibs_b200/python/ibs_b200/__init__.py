@@ -128,6 +128,9 @@ _ibs_from_codes = _sig(_lib, "ibs_table_from_codes", C.c_int,
                        [vp, C.c_uint64, C.c_uint32, C.c_int, C.POINTER(TableOpts), C.POINTER(vp)])
 _ibs_info = _sig(_lib, "ibs_table_info_get", C.c_int, [vp, C.POINTER(TableInfo)])
 _ibs_probe = _sig(_lib, "ibs_probe", C.c_int, [vp, vp, C.c_uint64, vp])
+_ibs_from_codes128 = _sig(_lib, "ibs_table_from_codes128", C.c_int,
+                          [vp, C.c_uint64, C.c_uint32, C.c_int, C.POINTER(TableOpts), C.POINTER(vp)])
+_ibs_probe128 = _sig(_lib, "ibs_probe128", C.c_int, [vp, vp, C.c_uint64, vp])
 _ibs_close = _sig(_lib, "ibs_close", None, [vp])
 _ibs_count_present = _sig(_lib, "ibs_count_present", C.c_int, [vp, vp, C.c_uint64, C.c_int, u64p])
 _ibs_count_present_kmc = _sig(_lib, "ibs_count_present_kmc", C.c_int, [vp, C.c_char_p, u64p])
@@ -198,6 +201,7 @@ _t_write_fasta = _sig(_tools, "ibs_synth_write_fasta", C.c_int,
 _t_sample_codes = _sig(_tools, "ibs_synth_sample_codes", C.c_int,
                        [C.POINTER(SynthRefSpec), C.POINTER(SynthSampleSpec), vp, vp, C.c_int, vp,
                         C.c_uint64, u64p])
+_t_kmc_write128 = _sig(_tools, "ibs_kmc_write128", C.c_int, [C.c_char_p, C.POINTER(KmcSpec), vp, C.c_uint64, u64p])
 _t_kmc_write = _sig(_tools, "ibs_kmc_write", C.c_int,
                     [C.c_char_p, C.POINTER(KmcSpec), vp, C.c_uint64, C.c_int, u64p])
 _t_sort_unique = _sig(_tools, "ibs_sort_unique_host", C.c_uint64, [vp, C.c_uint64, C.c_int])
@@ -271,6 +275,16 @@ class Table:
         _check(_ibs_from_codes(_ptr(codes), n, k, int(on_device), C.byref(opts), C.byref(h)))
         return cls(h.value)
 
+    @classmethod
+    def from_codes128(cls, lo, hi, k: int, device: int = 0, keys_per_bucket: float = 0.0) -> "Table":
+        """A wide-key table (33 <= k <= 64) from canonical codes given as their
+        low and high 64-bit words (host arrays)."""
+        codes = pairs128(lo, hi)
+        opts = TableOpts(device, keys_per_bucket, 0)
+        h = vp()
+        _check(_ibs_from_codes128(_ptr(codes), len(codes) // 2, k, 0, C.byref(opts), C.byref(h)))
+        return cls(h.value)
+
     @property
     def handle(self) -> int:
         return self._h
@@ -279,6 +293,13 @@ class Table:
         i = TableInfo()
         _check(_ibs_info(self._h, C.byref(i)))
         return i
+
+    def probe128(self, lo, hi) -> np.ndarray:
+        """Membership of wide codes (low / high words) in a wide-key table."""
+        codes = pairs128(lo, hi)
+        hits = np.zeros(len(codes) // 2, dtype=np.uint8)
+        _check(_ibs_probe128(self._h, _ptr(codes), len(codes) // 2, _ptr(hits)))
+        return hits
 
     def count_present(self, codes, n: int | None = None, on_device: bool = False) -> int:
         """How many of the codes the table holds (ibs_count_present)."""
@@ -612,6 +633,30 @@ def kmc_write(prefix: str, codes, n: int, k: int, p: int, sig_len: int = 9, n_bi
     out = C.c_uint64()
     _check(_t_kmc_write(str(prefix).encode(), C.byref(spec), _ptr(codes), n, int(on_device),
                         C.byref(out)), tools=True)
+    return out.value
+
+
+def pairs128(lo, hi) -> np.ndarray:
+    """Low / high word arrays -> the interleaved {lo, hi} layout of ibs_code128."""
+    lo = np.ascontiguousarray(lo, dtype=np.uint64)
+    hi = np.ascontiguousarray(hi, dtype=np.uint64)
+    if lo.shape != hi.shape:
+        raise ValueError("lo and hi differ in length")
+    out = np.empty(2 * len(lo), dtype=np.uint64)
+    out[0::2] = lo
+    out[1::2] = hi
+    return out
+
+
+def kmc_write128(prefix: str, lo, hi, k: int, p: int, sig_len: int = 9, n_bins: int = 512,
+                 counter_size: int = 1, version: int = 0x200, min_count: int = 2, max_count: int = 255,
+                 count_seed: int = 7) -> int:
+    """KMC 3 database of 33 <= k <= 64 k-mers given as low / high words (host)."""
+    spec = KmcSpec(k, p, sig_len, n_bins, counter_size, version, min_count, max_count, count_seed)
+    codes = pairs128(lo, hi)
+    out = C.c_uint64()
+    _check(_t_kmc_write128(str(prefix).encode(), C.byref(spec), _ptr(codes), len(codes) // 2, C.byref(out)),
+           tools=True)
     return out.value
 
 

@@ -40,7 +40,7 @@ typedef enum ibs_status {
     IBS_ERR_FORMAT = 3,      /* not a KMC 3 database this library reads */
     IBS_ERR_CUDA = 4,        /* CUDA runtime error or no usable device */
     IBS_ERR_NOMEM = 5,       /* device or pinned host allocation failed */
-    IBS_ERR_UNSUPPORTED = 6, /* k > 32, Quake-mode counters, ... */
+    IBS_ERR_UNSUPPORTED = 6, /* k > 64, Quake-mode counters, ... */
     IBS_ERR_CAPACITY = 7,    /* request beyond a fixed capacity */
     IBS_ERR_TIMEOUT = 8,     /* a bounded device wait gave up */
     IBS_ERR_STATE = 9        /* handle in the wrong state for the call */
@@ -63,7 +63,8 @@ typedef struct ibs_table_opts {
     uint32_t force_format;  /* 0 = the tuned default (ibs_tuning.table_format), 1 = B8x32,
                                2 = B6x40, 4 = minimizer lines of B8x32 sectors (16 <= k <= 27),
                                5 = hash buckets, B8x32 or B6x40 by size,
-                               6 = minimizer lines of B6x40 sectors (16 <= k <= 31) */
+                               6 = minimizer lines of B6x40 sectors (16 <= k <= 31),
+                               8 = wide-key lines (33 <= k <= 64, and the only layout there) */
     uint32_t reserved[5];
 } ibs_table_opts;
 
@@ -79,9 +80,14 @@ typedef struct ibs_table_info {
 
 /* ---- tables -------------------------------------------------------------
  * ibs_open: decode <prefix>.kmc_pre / <prefix>.kmc_suf (KMC 3 formats 0 and
- * 0x200, k <= 32) once and build the device table. Counters are ignored, as
+ * 0x200, k <= 64) once and build the device table. Counters are ignored, as
  * the reference's KmcRaIndex strips them (src/gpu/KmcRaIndex.hpp:596-708).
- * Replaces KmcRaIndex(prefix) + DeviceKmerIndex(host, dev, shard). */
+ * Replaces KmcRaIndex(prefix) + DeviceKmerIndex(host, dev, shard) for
+ * k <= 32, and for 33 <= k <= 64 the KMC API random-access view that the
+ * reference's string path probes (CKMCFile::IsKmer via
+ * getStatsFromSequenceLegacy, src/KmerDatabase.hpp:675-708): such a table
+ * holds whole 128-bit keys (format 8) and every scan entry point except the
+ * joint-table, serving, mapper and no-alloc ones takes it. */
 ibs_status ibs_open(const char *kmc_prefix, const ibs_table_opts *opts, ibs_table **out);
 
 /* Build a table from canonical codes (host or device pointer; duplicates
@@ -91,6 +97,26 @@ ibs_status ibs_table_from_codes(const uint64_t *codes, uint64_t n, uint32_t k,
                                 ibs_table **out);
 
 ibs_status ibs_table_info_get(const ibs_table *t, ibs_table_info *info);
+
+/* A canonical code of a k-mer with 33 <= k <= 64: the 2k-bit code, first
+ * base most significant (A=0 C=1 G=2 T=3), as its low and high 64 bits. The
+ * reference compares such k-mers as strings (getCanonicalKmersLegacy,
+ * src/Utils.hpp:102-125); the order of the codes is the same. */
+typedef struct ibs_code128 {
+    uint64_t lo, hi;
+} ibs_code128;
+
+/* ibs_table_from_codes for 33 <= k <= 64 (a wide-key table, format 8):
+ * canonical codes on the host or the device, duplicates allowed (removed on
+ * the host before the build). */
+ibs_status ibs_table_from_codes128(const ibs_code128 *codes, uint64_t n, uint32_t k,
+                                   int codes_on_device, const ibs_table_opts *opts, ibs_table **out);
+
+/* Membership of n wide canonical codes (host array) in a wide-key table,
+ * one byte per code: CKMCFile::IsKmer of the string path
+ * (src/KmerDatabase.hpp:689-693). ibs_probe / ibs_count_present take the
+ * 64-bit codes of k <= 32 tables only. */
+ibs_status ibs_probe128(ibs_table *t, const ibs_code128 *codes, uint64_t n, uint8_t *hits);
 
 /* Membership of n canonical codes (host arrays), one byte per code.
  * The probe of KmcRaIndex::probe (src/gpu/KmcRaIndex.hpp:227-235). */
@@ -105,7 +131,8 @@ ibs_status ibs_count_present(ibs_table *t, const uint64_t *codes, uint64_t n, in
 
 /* The same for every k-mer of a KMC 3 database, decoded on the device: the
  * size of its intersection with the table's k-mer set. IBS_ERR_ARG ("K-mer
- * lengths do not match") when the k differs. */
+ * lengths do not match") when the k differs. Takes wide-key tables (k > 32)
+ * too, where KDBIntersect takes its string path (src/KDBIntersect.cpp:386-389). */
 ibs_status ibs_count_present_kmc(ibs_table *t, const char *kmc_prefix, uint64_t *count);
 
 void ibs_close(ibs_table *t);

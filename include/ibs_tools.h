@@ -91,6 +91,11 @@ typedef struct ibs_kmc_spec {
 ibs_status ibs_kmc_write(const char *prefix, const ibs_kmc_spec *spec, const uint64_t *codes,
                          uint64_t n, int on_device, uint64_t *n_written);
 
+/* The same for 33 <= k <= 64: 128-bit canonical codes from host memory
+ * (ibs_code128 of ibs.h); records carry (k - p) / 4 suffix bytes. */
+ibs_status ibs_kmc_write128(const char *prefix, const ibs_kmc_spec *spec, const ibs_code128 *codes,
+                            uint64_t n, uint64_t *n_written);
+
 /* Random 32-byte-sector read rate of this device over a buffer of `bytes`
  * (uniformly random sector indexes, 4 loads in flight per thread): the
  * ceiling of a scan that reads one random sector per probe. */

@@ -228,6 +228,8 @@ void orc_seqfile_free(orc_seqfile *f)
  * loadPre :540-594, loadSuf :596-708, mmerAllowed/buildNorm :712-750) and
  * the probe of src/gpu/ProbeCore.hpp:58-129.
  * ==================================================================== */
+typedef unsigned __int128 u128;
+
 struct orc_index {
     uint32_t k, p, sigLen, suffixBytes, counterBytes;
     uint64_t suffixMask, total, singleLutSize;
@@ -238,6 +240,8 @@ struct orc_index {
     uint32_t *norm;
     uint32_t *suf32;
     uint64_t *suf64;
+    u128 *suf128;     /* k > 32: suffixes of up to 16 bytes */
+    u128 suffixMask128;
 };
 
 static int read_at(FILE *f, long long off, void *dst, size_t n, const char *what)
@@ -358,11 +362,15 @@ orc_index *orc_index_open(const char *prefix)
         set_err("KmcRaIndex: Quake-compatible counters are not supported");
         goto fail;
     }
-    if (ix->k > 32) {
-        set_err("KmcRaIndex: k > 32 is not supported");
+    /* k > 32: the reference's string path reads the same files through the
+     * KMC API (CKMCFile::OpenForRA, KMC/kmc_api/kmc_file.cpp), whose
+     * membership test is the same prefix-LUT bucket plus binary search over
+     * suffixes (CKMCFile::CheckKmer); suffixes are then up to 16 bytes. */
+    if (ix->k == 0 || ix->k > 64) {
+        set_err("KmcRaIndex: k=%u is not supported (k must be 1..64)", ix->k);
         goto fail;
     }
-    if ((ix->k - ix->p) % 4 != 0 || ix->k - ix->p > 32) {
+    if ((ix->k - ix->p) % 4 != 0 || ix->k - ix->p > (ix->k > 32 ? 64u : 32u)) {
         set_err("KmcRaIndex: unexpected suffix geometry");
         goto fail;
     }
@@ -370,7 +378,8 @@ orc_index *orc_index_open(const char *prefix)
     ix->counterBytes = counterSize;
     {
         const uint32_t sym = ix->k - ix->p;
-        ix->suffixMask = sym == 32 ? ~0ull : (1ull << (2 * sym)) - 1;
+        ix->suffixMask = sym >= 32 ? ~0ull : (1ull << (2 * sym)) - 1;
+        ix->suffixMask128 = sym >= 64 ? ~(u128)0 : (((u128)1 << (2 * sym)) - 1);
     }
     ix->singleLutSize = 1ull << (2 * ix->p);
     if (version == 0x200) {
@@ -412,8 +421,10 @@ orc_index *orc_index_open(const char *prefix)
             set_err("KmcRaIndex: suffix file smaller than expected");
             goto fail;
         }
-        const int use32 = ix->suffixBytes <= 4;
-        if (use32)
+        const int use32 = ix->suffixBytes <= 4, use128 = ix->k > 32;
+        if (use128)
+            ix->suf128 = (u128 *)malloc(ix->total * 16 + 16);
+        else if (use32)
             ix->suf32 = (uint32_t *)malloc(ix->total * 4 + 4);
         else
             ix->suf64 = (uint64_t *)malloc(ix->total * 8 + 8);
@@ -430,6 +441,13 @@ orc_index *orc_index_open(const char *prefix)
             }
             const unsigned char *q = buf;
             for (size_t i = 0; i < batch; i++, q += rec) {
+                if (use128) {
+                    u128 w = 0;
+                    for (uint32_t b = 0; b < ix->suffixBytes; b++)
+                        w = (w << 8) | q[b];
+                    ix->suf128[r + i] = w;
+                    continue;
+                }
                 uint64_t v = 0;
                 for (uint32_t b = 0; b < ix->suffixBytes; b++)
                     v = (v << 8) | q[b];
@@ -462,6 +480,7 @@ void orc_index_close(orc_index *ix)
     free(ix->norm);
     free(ix->suf32);
     free(ix->suf64);
+    free(ix->suf128);
     free(ix);
 }
 
@@ -553,6 +572,81 @@ size_t orc_index_list(const orc_index *ix, uint64_t *codes, size_t cap)
     return n;
 }
 
+/* The same three for k > 32 (128-bit codes, first base most significant):
+ * the signature over the code's m-mers, then the LUT bucket and the binary
+ * search, as CKMCFile::CheckKmer does for the string path's
+ * CKMCFile::IsKmer (src/KmerDatabase.hpp:689-693). */
+static uint32_t signature128(const orc_index *ix, u128 code)
+{
+    const uint32_t k = ix->k, s = ix->sigLen;
+    const uint32_t mmask = (1u << (2 * s)) - 1;
+    uint32_t str = 0, best = 0xffffffffu;
+    for (uint32_t i = 0; i < k; ++i) {
+        const uint32_t symb = (uint32_t)(code >> (2 * (k - 1 - i))) & 3;
+        str = ((str << 2) | symb) & mmask;
+        if (i >= s - 1) {
+            const uint32_t v = ix->norm[str];
+            if (v < best)
+                best = v;
+        }
+    }
+    return best;
+}
+
+int orc_probe128(const orc_index *ix, uint64_t lo, uint64_t hi)
+{
+    if (!ix->suf128)
+        return 0;
+    const u128 code = ((u128)hi << 64) | lo;
+    const uint64_t prefix = (uint64_t)(code >> (2 * (ix->k - ix->p)));
+    uint64_t lutBase = 0;
+    if (ix->sigLen)
+        lutBase = (uint64_t)ix->sigMap[signature128(ix, code)] * ix->singleLutSize;
+    const uint64_t entry = lutBase + prefix;
+    long long a = (long long)ix->lut[entry];
+    long long b = (long long)ix->lut[entry + 1] - 1;
+    if (a >= (long long)ix->total)
+        return 0;
+    if (b > (long long)ix->total - 1)
+        b = (long long)ix->total - 1;
+    const u128 target = code & ix->suffixMask128;
+    while (a <= b) {
+        const long long mid = (a + b) >> 1;
+        const u128 v = ix->suf128[mid];
+        if (v == target)
+            return 1;
+        if (v < target)
+            a = mid + 1;
+        else
+            b = mid - 1;
+    }
+    return 0;
+}
+
+size_t orc_index_list128(const orc_index *ix, uint64_t *lo, uint64_t *hi, size_t cap)
+{
+    if (!ix->suf128)
+        return 0;
+    const uint32_t shift = 2 * (ix->k - ix->p);
+    const uint64_t prefixMask = ix->singleLutSize - 1;
+    size_t n = 0;
+    for (size_t j = 0; j + 1 < ix->lutEntries; ++j) {
+        const u128 prefix = (u128)((uint64_t)j & prefixMask) << shift;
+        uint64_t a = ix->lut[j], b = ix->lut[j + 1];
+        if (b > ix->total)
+            b = ix->total;
+        for (uint64_t r = a; r < b; ++r) {
+            if (n < cap) {
+                const u128 c = prefix | ix->suf128[r];
+                lo[n] = (uint64_t)c;
+                hi[n] = (uint64_t)(c >> 64);
+            }
+            n++;
+        }
+    }
+    return n;
+}
+
 /* ======================================================================
  * Codec: KmerCodec::getCanonicalCodes (src/KmerCodec.hpp:38-61) with the
  * table of :105-118 (ACGT and acgt valid, every other byte invalid).
@@ -589,6 +683,40 @@ size_t orc_canonical_codes(const char *seq, size_t len, uint32_t k, uint64_t *co
         rc = (rc >> 2) | ((uint64_t)(3 - c) << rcShift);
         if (validBases >= k)
             codes[n++] = fwd < rc ? fwd : rc;
+    }
+    return n;
+}
+
+/* The string path's k-mers for k > 32: getCanonicalKmersLegacy
+ * (src/Utils.hpp:102-125) upper-cases the window, skips every k-mer with a
+ * byte outside ACGT and keeps the smaller of the k-mer and its reverse
+ * complement as strings; as 2k-bit codes (A<C<G<T) the string order is the
+ * integer order. */
+size_t orc_canonical_codes128(const char *seq, size_t len, uint32_t k, uint64_t *lo, uint64_t *hi)
+{
+    pthread_once(&g_tab_once, init_tab);
+    size_t n = 0;
+    if (len < k || k > 64)
+        return 0;
+    const u128 mask = k == 64 ? ~(u128)0 : (((u128)1 << (2 * k)) - 1);
+    const uint32_t rcShift = 2 * (k - 1);
+    u128 fwd = 0, rc = 0;
+    uint32_t validBases = 0;
+    for (size_t j = 0; j < len; ++j) {
+        unsigned c = g_tab[(unsigned char)seq[j]];
+        if (c > 3) {
+            validBases = 0;
+            c = 0;
+        } else
+            ++validBases;
+        fwd = ((fwd << 2) | c) & mask;
+        rc = (rc >> 2) | ((u128)(3 - c) << rcShift);
+        if (validBases >= k) {
+            const u128 m = fwd < rc ? fwd : rc;
+            lo[n] = (uint64_t)m;
+            hi[n] = (uint64_t)(m >> 64);
+            n++;
+        }
     }
     return n;
 }
@@ -638,6 +766,7 @@ void orc_stats_from_hits(const uint8_t *hits, size_t n, uint32_t k, orc_window *
 
 static int pred_hit(uint64_t code) { return (code * 0x9E3779B97F4A7C15ull >> 61) == 0; }
 
+/* codes holds 2 (W + 1) words: the low words, then (k > 32) the high words. */
 static void scan_window(const orc_index *ix, const char *seq, size_t len, size_t j, uint32_t W,
                         uint32_t k, orc_window *row, uint64_t *codes, uint8_t *hits)
 {
@@ -645,6 +774,15 @@ static void scan_window(const orc_index *ix, const char *seq, size_t len, size_t
     memset(row, 0, sizeof *row);
     row->start = (int32_t)j;
     row->end = (int32_t)end;
+    if (k > 32) {
+        uint64_t *hi = codes + W + 1;
+        const size_t n = orc_canonical_codes128(seq + j, end - j, k, codes, hi);
+        for (size_t i = 0; i < n; i++)
+            hits[i] = (uint8_t)(ix ? orc_probe128(ix, codes[i], hi[i])
+                                   : pred_hit(codes[i] ^ (hi[i] * 0xC2B2AE3D27D4EB4Full)));
+        orc_stats_from_hits(hits, n, k, row);
+        return;
+    }
     const size_t n = orc_canonical_codes(seq + j, end - j, k, codes);
     for (size_t i = 0; i < n; i++)
         hits[i] = (uint8_t)(ix ? orc_probe(ix, codes[i]) : pred_hit(codes[i]));
@@ -658,7 +796,7 @@ int orc_scan_contig(const orc_index *ix, const char *seq, size_t len, uint32_t W
         set_err("window size %u must be larger than k (%u)", W, k);
         return -1;
     }
-    uint64_t *codes = (uint64_t *)malloc(((size_t)W + 1) * 8);
+    uint64_t *codes = (uint64_t *)malloc(((size_t)W + 1) * 16);
     uint8_t *hits = (uint8_t *)malloc((size_t)W + 1);
     size_t w = 0;
     for (size_t j = 0; j < len; j += W - k)
@@ -685,7 +823,7 @@ typedef struct {
 static void *scan_worker(void *arg)
 {
     scan_job *J = (scan_job *)arg;
-    uint64_t *codes = (uint64_t *)malloc(((size_t)J->W + 1) * 8);
+    uint64_t *codes = (uint64_t *)malloc(((size_t)J->W + 1) * 16);
     uint8_t *hits = (uint8_t *)malloc((size_t)J->W + 1);
     for (;;) {
         pthread_mutex_lock(&J->mu);

@@ -49,10 +49,18 @@ void orc_probe_many(const orc_index *ix, const uint64_t *codes, size_t n, uint8_
  * src/gpu/KmcRaIndex.hpp:169-173, :446-460); returns the count written. */
 size_t orc_index_list(const orc_index *ix, uint64_t *codes, size_t cap);
 uint32_t orc_signature(const orc_index *ix, uint64_t code);
+/* k > 32 (the reference's string path, KMC API CKMCFile::IsKmer): membership
+ * of one 128-bit canonical code given as its low and high words, and the
+ * listing as two word arrays. */
+int orc_probe128(const orc_index *ix, uint64_t lo, uint64_t hi);
+size_t orc_index_list128(const orc_index *ix, uint64_t *lo, uint64_t *hi, size_t cap);
 
 /* ---- codec (src/KmerCodec.hpp:38-61) ---------------------------------- */
 /* Canonical codes of all valid positions, in order; returns the count. */
 size_t orc_canonical_codes(const char *seq, size_t len, uint32_t k, uint64_t *codes);
+/* k > 32: canonical k-mers of the string path (src/Utils.hpp:102-125) as
+ * 128-bit codes split into low and high words. */
+size_t orc_canonical_codes128(const char *seq, size_t len, uint32_t k, uint64_t *lo, uint64_t *hi);
 
 /* ---- windows (src/Utils.hpp:296-327) ---------------------------------- */
 /* Number of windows chunkSequences cuts from a contig of `len` bases. */

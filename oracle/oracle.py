@@ -50,6 +50,9 @@ _iparams = _sig("orc_index_params", None, [vp, C.POINTER(C.c_uint32), C.POINTER(
 _probe_many = _sig("orc_probe_many", None, [vp, vp, C.c_size_t, vp])
 _list = _sig("orc_index_list", C.c_size_t, [vp, vp, C.c_size_t])
 _canon = _sig("orc_canonical_codes", C.c_size_t, [C.c_char_p, C.c_size_t, C.c_uint32, vp])
+_canon128 = _sig("orc_canonical_codes128", C.c_size_t, [C.c_char_p, C.c_size_t, C.c_uint32, vp, vp])
+_probe128 = _sig("orc_probe128", C.c_int, [vp, C.c_uint64, C.c_uint64])
+_list128 = _sig("orc_index_list128", C.c_size_t, [vp, vp, vp, C.c_size_t])
 _wcount = _sig("orc_window_count", C.c_size_t, [C.c_size_t, C.c_uint32, C.c_uint32])
 _scan_contigs = _sig("orc_scan_contigs", C.c_int,
                      [vp, C.POINTER(C.c_char_p), vp, C.c_size_t, C.c_uint32, C.c_uint32, C.c_int, vp])
@@ -108,6 +111,19 @@ class Index:
         n = _list(self._h, out.ctypes.data, len(out))
         return out[:n]
 
+    def probe128(self, lo, hi) -> np.ndarray:
+        """k > 32: membership of codes given as low / high word arrays."""
+        lo = np.ascontiguousarray(lo, dtype=np.uint64)
+        hi = np.ascontiguousarray(hi, dtype=np.uint64)
+        return np.array([_probe128(self._h, int(a), int(b)) for a, b in zip(lo, hi)], dtype=np.uint8)
+
+    def list_codes128(self):
+        """k > 32: every k-mer as (low words, high words)."""
+        lo = np.zeros(max(self.total, 1), dtype=np.uint64)
+        hi = np.zeros(max(self.total, 1), dtype=np.uint64)
+        n = _list128(self._h, lo.ctypes.data, hi.ctypes.data, len(lo))
+        return lo[:n], hi[:n]
+
     def close(self):
         if self._h:
             _iclose(self._h)
@@ -124,6 +140,14 @@ def canonical_codes(seq: bytes, k: int) -> np.ndarray:
     out = np.zeros(max(len(seq), 1), dtype=np.uint64)
     n = _canon(seq, len(seq), k, out.ctypes.data)
     return out[:n]
+
+
+def canonical_codes128(seq: bytes, k: int):
+    """k > 32: the string path's canonical k-mers as (low words, high words)."""
+    lo = np.zeros(max(len(seq), 1), dtype=np.uint64)
+    hi = np.zeros(max(len(seq), 1), dtype=np.uint64)
+    n = _canon128(seq, len(seq), k, lo.ctypes.data, hi.ctypes.data)
+    return lo[:n], hi[:n]
 
 
 def window_count(length: int, W: int, k: int) -> int:
@@ -187,14 +211,52 @@ def position_codes(seq: bytes, k: int):
     return np.minimum(fwd, rc), valid
 
 
+def position_codes128(seq: bytes, k: int):
+    """k > 32: (low words, high words, valid) of every k-mer start of seq, the
+    string path's canonical k-mers (src/Utils.hpp:102-125) by position."""
+    s = np.frombuffer(seq, dtype=np.uint8)
+    n = len(s) - k + 1
+    if n <= 0:
+        return np.zeros(0, np.uint64), np.zeros(0, np.uint64), np.zeros(0, bool)
+    lut = np.full(256, 4, dtype=np.uint8)
+    for i, c in enumerate(b"ACGT"):
+        lut[c] = lut[c + 32] = i
+    v = lut[s]
+    cb = np.concatenate([[0], np.cumsum(v > 3)])
+    valid = (cb[k:] - cb[:-k])[:n] == 0
+    v = np.where(v > 3, 0, v).astype(np.uint64)
+    flo, fhi, rlo, rhi = (np.zeros(n, np.uint64) for _ in range(4))
+    for t in range(k):
+        b = v[t:t + n]
+        fb = 2 * (k - 1 - t)
+        if fb >= 64:
+            fhi |= b << np.uint64(fb - 64)
+        else:
+            flo |= b << np.uint64(fb)
+        c = np.uint64(3) - b
+        if 2 * t >= 64:
+            rhi |= c << np.uint64(2 * t - 64)
+        else:
+            rlo |= c << np.uint64(2 * t)
+    fwd = (fhi < rhi) | ((fhi == rhi) & (flo <= rlo))
+    return np.where(fwd, flo, rlo), np.where(fwd, fhi, rhi), valid
+
+
 def coverage(index: Index, seq: bytes, k: int) -> np.ndarray:
     """Per-base k-mer coverage of one contig: the reference's difference array
     (+1 at a hit start, -1 k bases on) and its prefix sum
-    (KmerDatabase::getMappingFromSequence, src/KmerDatabase.hpp:774-801)."""
-    codes, valid = position_codes(seq, k)
+    (KmerDatabase::getMappingFromSequence, src/KmerDatabase.hpp:774-801;
+    for k > 32 its string path, getMappingFromSequenceLegacy, :803-848)."""
+    if k > 32:
+        lo, hi, valid = position_codes128(seq, k)
+        codes = lo
+        probe = lambda: index.probe128(lo, hi)  # noqa: E731
+    else:
+        codes, valid = position_codes(seq, k)
+        probe = lambda: index.probe(codes)  # noqa: E731
     diff = np.zeros(len(seq) + 1, np.int64)
     if len(codes):
-        hit = valid & (index.probe(codes).astype(bool))
+        hit = valid & (probe().astype(bool))
         idx = np.nonzero(hit)[0]
         np.add.at(diff, idx, 1)
         np.add.at(diff, idx + k, -1)

@@ -52,13 +52,15 @@ def build_case(case_root):
 @pytest.fixture(scope="session")
 def native_shim():
     """tests/native/fold_shim.so: the window-statistics fold of
-    gpu-ibs_b200/csrc/ibs_core.cuh and the minimizer key map of mz_core.cuh
-    compiled for the host."""
+    gpu-ibs_b200/csrc/ibs_core.cuh, the minimizer key map of mz_core.cuh and
+    the wide-code reader of wide_core.cuh compiled for the host."""
     src = REPO / "tests" / "native" / "fold_shim.cpp"
     out = REPO / "tests" / "native" / "fold_shim.so"
-    deps = [src, REPO / "gpu-ibs_b200/csrc/ibs_core.cuh", REPO / "gpu-ibs_b200/csrc/mz_core.cuh"]
+    deps = [src, REPO / "gpu-ibs_b200/csrc/ibs_core.cuh", REPO / "gpu-ibs_b200/csrc/mz_core.cuh",
+            REPO / "gpu-ibs_b200/csrc/wide_core.cuh"]
     if not out.exists() or out.stat().st_mtime < max(d.stat().st_mtime for d in deps):
+        cuda_inc = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "include"
         subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-o", str(out), str(src),
-                        f"-I{REPO / 'gpu-ibs_b200' / 'csrc'}"], check=True)
+                        f"-I{REPO / 'gpu-ibs_b200' / 'csrc'}", f"-I{cuda_inc}"], check=True)
     import ctypes
     return ctypes.CDLL(str(out))

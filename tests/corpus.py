@@ -127,6 +127,70 @@ def canonical_codes_np(seq: bytes, k: int) -> np.ndarray:
     return can[ok[:n]]
 
 
+def _split_codes(v: np.ndarray, k: int):
+    """Forward and reverse-complement codes of every k-mer start of the base
+    values v (0..3) as (fwd_lo, fwd_hi, rc_lo, rc_hi), k > 32: base t of a
+    k-mer sits at bit 2 (k - 1 - t) of the forward code and, complemented,
+    at bit 2 t of the reverse complement."""
+    n = len(v) - k + 1
+    z = lambda: np.zeros(max(n, 0), dtype=np.uint64)  # noqa: E731
+    flo, fhi, rlo, rhi = z(), z(), z(), z()
+    for t in range(k):
+        b = v[t:t + n]
+        fb = 2 * (k - 1 - t)
+        if fb >= 64:
+            fhi |= b << np.uint64(fb - 64)
+        else:
+            flo |= b << np.uint64(fb)
+        c = np.uint64(3) - b
+        if 2 * t >= 64:
+            rhi |= c << np.uint64(2 * t - 64)
+        else:
+            rlo |= c << np.uint64(2 * t)
+    return flo, fhi, rlo, rhi
+
+
+def min128(alo, ahi, blo, bhi):
+    a_first = (ahi < bhi) | ((ahi == bhi) & (alo <= blo))
+    return np.where(a_first, alo, blo), np.where(a_first, ahi, bhi)
+
+
+def canonical_codes128_np(seq: bytes, k: int):
+    """k > 32: (lo, hi) words of the canonical codes of the ACGT-only k-mers
+    of seq (case-folded), in order."""
+    s = np.frombuffer(seq.upper(), dtype=np.uint8)
+    lut = np.full(256, 4, dtype=np.uint8)
+    for i, c in enumerate(b"ACGT"):
+        lut[c] = i
+    v = lut[s]
+    n = len(v) - k + 1
+    if n <= 0:
+        return np.zeros(0, dtype=np.uint64), np.zeros(0, dtype=np.uint64)
+    cb = np.concatenate([[0], np.cumsum(v > 3)])
+    ok = ((cb[k:] - cb[:-k]) == 0)[:n]
+    v = np.where(v > 3, 0, v).astype(np.uint64)
+    lo, hi = min128(*_split_codes(v, k))
+    return lo[ok], hi[ok]
+
+
+def random_codes128(rng, n, k):
+    """n random canonical k-mers (k > 32) as (lo, hi)."""
+    v = rng.integers(0, 4, (n, k)).astype(np.uint64)
+    flo, fhi, rlo, rhi = (np.zeros(n, dtype=np.uint64) for _ in range(4))
+    for t in range(k):
+        fb = 2 * (k - 1 - t)
+        if fb >= 64:
+            fhi |= v[:, t] << np.uint64(fb - 64)
+        else:
+            flo |= v[:, t] << np.uint64(fb)
+        c = np.uint64(3) - v[:, t]
+        if 2 * t >= 64:
+            rhi |= c << np.uint64(2 * t - 64)
+        else:
+            rlo |= c << np.uint64(2 * t)
+    return min128(flo, fhi, rlo, rhi)
+
+
 def random_codes(rng, n, k) -> np.ndarray:
     mask = (1 << (2 * k)) - 1 if k < 32 else (1 << 64) - 1
     x = rng.integers(0, 1 << 63, n, dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, n, dtype=np.uint64)
@@ -153,6 +217,10 @@ EDGE_CASES = {
     "edge_k25_crlf": dict(k=25, p=9, version=0x200, counter_size=1, windows=[5000], fmt="crlf"),
     "edge_k25_fastq": dict(k=25, p=5, version=0x200, counter_size=1, windows=[5000], fmt="fastq"),
     "edge_k25_gz": dict(k=25, p=5, version=0x200, counter_size=1, windows=[5000], fmt="gz"),
+    # k > 32: the reference's string path (two-word codes here)
+    "edge_k33": dict(k=33, p=9, version=0x200, counter_size=1, windows=[5000], fmt="fasta"),
+    "edge_k41": dict(k=41, p=5, version=0x200, counter_size=2, windows=[1000, 5000], fmt="fasta"),
+    "edge_k64": dict(k=64, p=8, version=0, counter_size=0, windows=[5000], fmt="fasta"),
 }
 
 
@@ -183,14 +251,22 @@ def build_edge_case(name: str, root: Path):
         data = gzip.compress(fasta_bytes(refs), mtime=0)
     ref_path.write_bytes(data)
     rng = np.random.default_rng(seed + 1)
-    codes = [canonical_codes_np(c, k) for _, _, c in recs]
-    total = sum(len(c) for c in codes)
-    codes.append(random_codes(rng, total // 20, k))
-    allc = np.concatenate(codes)
     prefix = d / "db" / "sample"
-    ib.kmc_write(str(prefix), allc, len(allc), k=k, p=spec["p"], sig_len=9, n_bins=64,
-                 counter_size=spec["counter_size"], version=spec["version"],
-                 min_count=2 if spec["counter_size"] else 0, max_count=255 if spec["counter_size"] == 1 else 65535)
+    kmc = dict(k=k, p=spec["p"], sig_len=9, n_bins=64, counter_size=spec["counter_size"], version=spec["version"],
+               min_count=2 if spec["counter_size"] else 0, max_count=255 if spec["counter_size"] == 1 else 65535)
+    if k > 32:
+        parts = [canonical_codes128_np(c, k) for _, _, c in recs]
+        total = sum(len(lo) for lo, _ in parts)
+        parts.append(random_codes128(rng, total // 20, k))
+        lo = np.concatenate([a for a, _ in parts])
+        hi = np.concatenate([b for _, b in parts])
+        ib.kmc_write128(str(prefix), lo, hi, **kmc)
+    else:
+        codes = [canonical_codes_np(c, k) for _, _, c in recs]
+        total = sum(len(c) for c in codes)
+        codes.append(random_codes(rng, total // 20, k))
+        allc = np.concatenate(codes)
+        ib.kmc_write(str(prefix), allc, len(allc), **kmc)
     return dict(db=d / "db", prefix=prefix, refs=d / "refs", ref=ref_path, k=k, windows=spec["windows"])
 
 
@@ -241,7 +317,28 @@ INTERSECT_CASES = {
     "x_k31": dict(k=31, a=dict(p=7, version=0x200, counter_size=1), b=dict(p=3, version=0x200, counter_size=0)),
     "x_k15": dict(k=15, a=dict(p=7, version=0, counter_size=1), b=dict(p=3, version=0x200, counter_size=1)),
     "x_k32": dict(k=32, a=dict(p=8, version=0x200, counter_size=1), b=dict(p=4, version=0x200, counter_size=1)),
+    # k > 32 (two-word codes; the reference's string path)
+    "x_k41": dict(k=41, a=dict(p=5, version=0x200, counter_size=1), b=dict(p=9, version=0, counter_size=2)),
 }
+
+
+def _wide_sample_codes(seqs, k: int, seed: int, rate: float, present: float, extra: float):
+    """k > 32 samples for the intersection cases: the canonical k-mers of a
+    copy of the reference with SNPs at `rate`, keeping each 20 kbp block with
+    probability `present`, plus random k-mers (`extra` per reference base)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = [], []
+    for s in seqs:
+        a = np.frombuffer(s.upper(), dtype=np.uint8).copy()
+        snp = rng.random(len(a)) < rate
+        a[snp] = BASES[rng.integers(0, 4, int(snp.sum()))]
+        for b0 in range(0, len(a), 20_000):
+            if rng.random() < present:
+                x, y = canonical_codes128_np(bytes(a[b0:b0 + 20_000]), k)
+                lo.append(x)
+                hi.append(y)
+    x, y = random_codes128(rng, int(extra * sum(len(s) for s in seqs)), k)
+    return np.concatenate(lo + [x]), np.concatenate(hi + [y])
 
 
 def build_intersect_case(name: str, root: Path):
@@ -254,6 +351,20 @@ def build_intersect_case(name: str, root: Path):
     ref = ib.RefSpec(seed=seed, lens=[300_000, 100_000], n_frac=0.002, n_run=(1, 200))
     seq, mask = ref.reference_host()
     out = dict(k=k)
+    if k > 32:
+        seqs = [ref.contig_ascii(c) for c in range(len(ref.lens))]
+        for side, rate, present, extra in (("a", 0.01, 1.0, 0.05), ("b", 0.03, 0.6, 0.10)):
+            lo, hi = _wide_sample_codes(seqs, k, seed * 10 + ord(side), rate, present, extra)
+            lay = spec[side]
+            d = root / name / side
+            d.mkdir(parents=True, exist_ok=True)
+            ib.kmc_write128(str(d / "sample"), lo, hi, k=k, p=lay["p"], sig_len=9, n_bins=64,
+                            counter_size=lay["counter_size"], version=lay["version"],
+                            min_count=2 if lay["counter_size"] else 0,
+                            max_count=255 if lay["counter_size"] == 1 else 65535)
+            out[side] = d
+            out["prefix_" + side] = d / "sample"
+        return out
     for side, rate, present, extra in (("a", 0.01, 1.0, 0.05), ("b", 0.03, 0.6, 0.10)):
         smp = ib.SampleSpec(seed=seed * 10 + ord(side), k=k, class_rate=(rate,), class_prob=(1.0,),
                             block_len=20_000, present_frac=present, random_frac=extra)

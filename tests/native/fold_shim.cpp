@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cstdint>
 #include "ibs_core.cuh"
+#include "wide_core.cuh"
 
 using namespace ibs;
 
@@ -175,4 +176,27 @@ extern "C" void span_fold(const uint8_t *valid, const uint8_t *hit, uint64_t n, 
     out[1] = row.observed_kmers;
     out[2] = row.variations;
     out[3] = row.kmer_distance;
+}
+
+// Wide codes (wide_core.cuh): the canonical code and ACGT flag of the k-mer
+// at each packed base G0 .. G0 + n - 1 of a packed reference (33 <= k <= 64),
+// as the wide scan kernel reads them; lo / hi / ok get n entries.
+extern "C" void wide_codes_packed(const uint64_t *seq, const uint64_t *mask, uint64_t G0, uint64_t n, uint32_t k,
+                                  uint64_t *lo, uint64_t *hi, uint8_t *ok)
+{
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t G = G0 + i;
+        bool acgt = false;
+        const uint64_t wi = G >> 5, mi = G >> 6;
+        ibs::wide::canonical_from_words(seq[wi], seq[wi + 1], seq[wi + 2], mask[mi], mask[mi + 1], G, k, acgt,
+                                        lo[i], hi[i]);
+        ok[i] = acgt ? 1 : 0;
+    }
+}
+
+// The wide table's line of a key in a level (wide_core.cuh), for the host
+// tests of the level layout.
+extern "C" uint64_t wide_line_of(uint64_t lo, uint64_t hi, uint32_t level, uint64_t lines)
+{
+    return ibs::wide::line_of(lo, hi, level, lines);
 }

@@ -106,14 +106,15 @@ def test_open_errors_are_reported_without_a_device(tmp_path):
     assert e.value.status == 3  # IBS_ERR_FORMAT
 
 
-def test_open_rejects_k_above_32(tmp_path):
+def test_open_rejects_k_above_64(tmp_path):
     codes = np.arange(10, dtype=np.uint64)
     ib.kmc_write(str(tmp_path / "s"), codes, 10, k=32, p=8)
     pre = (tmp_path / "s.kmc_pre").read_bytes()
-    # patch the header's k (first field of the 64-byte header block) to 40
+    # patch the header's k (first field of the 64-byte header block) to 72:
+    # 33 <= k <= 64 builds a wide-key table, anything longer is refused
     hoff = pre[-8]
     pos = len(pre) - (hoff + 8)
-    patched = pre[:pos] + (40).to_bytes(4, "little") + pre[pos + 4:]
+    patched = pre[:pos] + (72).to_bytes(4, "little") + pre[pos + 4:]
     (tmp_path / "s.kmc_pre").write_bytes(patched)
     with pytest.raises(ib.IbsError) as e:
         ib.Table.open(str(tmp_path / "s"))

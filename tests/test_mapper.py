@@ -49,8 +49,9 @@ def test_device_mapping_matches_reference(name, build_case):
     ref = ib.Reference(seq, mask, lens)
     ix = orc.Index(str(case["prefix"]))
     want_cov = np.concatenate([orc.coverage(ix, s, case["k"]) for s in seqs])
-    formats = ([0, 2] + ([1] if case["k"] <= 25 else []) + ([4] if 16 <= case["k"] <= 27 else [])
-               + ([6] if 16 <= case["k"] <= 31 else []))
+    # k > 32 has one layout, the wide-key table
+    formats = ([0] if case["k"] > 32 else [0, 2] + ([1] if case["k"] <= 25 else [])
+               + ([4] if 16 <= case["k"] <= 27 else []) + ([6] if 16 <= case["k"] <= 31 else []))
     for fmt in formats:
         t = ib.Table.open(str(case["prefix"]), force_format=fmt)
         assert np.array_equal(ib.map_coverage(t, ref).astype(np.int64), want_cov), (name, fmt)
@@ -61,7 +62,8 @@ def test_device_mapping_matches_reference(name, build_case):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["edge_k25", "edge_k25_crlf", "edge_k25_fastq", "edge_k25_gz", "plain_1mbp"])
+@pytest.mark.parametrize("name", ["edge_k25", "edge_k25_crlf", "edge_k25_fastq", "edge_k25_gz", "edge_k41",
+                                  "plain_1mbp"])
 def test_cli_writes_the_reference_file(name, build_case, tmp_path):
     case = build_case(name)
     out = tmp_path / "out"
