@@ -48,6 +48,7 @@ sys.path.insert(0, str(REPO / "gpu-ibs_b200" / "python"))
 
 BYTES_PER_PROBE = 32.0 + 0.375  # one 32-byte bucket sector + 2-bit base + N-mask bit
 METRIC = "ref k-mer probes/s"
+STARTED = time.time()
 
 
 def log(*a):
@@ -1302,6 +1303,9 @@ def main():
     ap.add_argument("--admit-rate", type=float, default=100.0)
     ap.add_argument("--serve-workload", choices=["served_2gbp", "panel_4gbp"], default="served_2gbp",
                     help="the pool: the 2 Gbp reference with 16 samples, or the 4.2 Gbp panel's")
+    ap.add_argument("--arm-start-limit", type=float, default=900.0,
+                    help="seconds after start past which the batched, served and admitted arms are not "
+                         "started (reported as skipped), so that the whole run stays bounded")
     ap.add_argument("--serve-sample-scale", type=float, default=0.5,
                     help="panel_4gbp pool: sample size scale (its 16 full-size samples do not fit "
                          "on one GPU together)")
@@ -1355,6 +1359,11 @@ def main():
         for key, skip, fn in (("panel", args.no_panel, panel_arm), ("served", args.no_serve, served_arm),
                               ("admitted", args.no_admitted, admitted_arm)):
             if skip:
+                continue
+            if time.time() - STARTED > args.arm_start_limit:
+                out[key] = {"skipped": f"not started: {time.time() - STARTED:.0f} s after start is past "
+                                       f"--arm-start-limit {args.arm_start_limit:.0f} s"}
+                log(f"[bench] {key} arm skipped ({out[key]['skipped']})")
                 continue
             torch.cuda.empty_cache()
             t0 = time.time()
