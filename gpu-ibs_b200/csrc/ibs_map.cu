@@ -85,15 +85,16 @@ __global__ void __launch_bounds__(256) k_map_spans(TableView t, const uint64_t *
 // it (starts p - 64 .. p + 31). The reference's string-path mapper
 // (getMappingFromSequenceLegacy, src/KmerDatabase.hpp:803-848) adds 1 to the
 // k bases of every start whose canonical k-mer string the database holds.
+// Every lane of the warp calls it (the lookup is warp-cooperative).
 __device__ __forceinline__ bool hit_at_wide(const wide::View &t, const uint64_t *__restrict__ seq,
-                                            const uint64_t *__restrict__ mask, const Span &sp, uint32_t s, uint32_t k)
+                                            const uint64_t *__restrict__ mask, const Span &sp, uint32_t s, uint32_t k,
+                                            uint32_t lane)
 {
-    if (s >= sp.nPos)
-        return false;
-    bool acgt;
-    uint64_t lo, hi;
-    wide::canonical_at(seq, mask, sp.base + s, k, acgt, lo, hi);
-    return acgt && wide::lookup(t, lo, hi);
+    bool acgt = false;
+    uint64_t lo = 0, hi = 0;
+    if (s < sp.nPos)
+        wide::canonical_at(seq, mask, sp.base + s, k, acgt, lo, hi);
+    return wide::lookup_warp(t, lo, hi, s < sp.nPos && acgt, lane);
 }
 
 __global__ void __launch_bounds__(256) k_map_spans_wide(wide::View t, const uint64_t *__restrict__ seq,
@@ -112,11 +113,11 @@ __global__ void __launch_bounds__(256) k_map_spans_wide(wide::View t, const uint
         // multiple of kSpan >= 64)
         uint32_t prev1 = 0, prev2 = 0; // starts p - 32 .. p - 1 and p - 64 .. p - 33
         if (sp.a >= 64) {
-            prev2 = __ballot_sync(dev::FULL_MASK, hit_at_wide(t, seq, mask, sp, sp.a - 64 + lane, k));
-            prev1 = __ballot_sync(dev::FULL_MASK, hit_at_wide(t, seq, mask, sp, sp.a - 32 + lane, k));
+            prev2 = __ballot_sync(dev::FULL_MASK, hit_at_wide(t, seq, mask, sp, sp.a - 64 + lane, k, lane));
+            prev1 = __ballot_sync(dev::FULL_MASK, hit_at_wide(t, seq, mask, sp, sp.a - 32 + lane, k, lane));
         }
         for (uint32_t p = sp.a; p < sp.b; p += 32) {
-            const uint32_t H = __ballot_sync(dev::FULL_MASK, hit_at_wide(t, seq, mask, sp, p + lane, k));
+            const uint32_t H = __ballot_sync(dev::FULL_MASK, hit_at_wide(t, seq, mask, sp, p + lane, k, lane));
             // bit j of (H : prev1 : prev2) is start p - 64 + j; base p + lane
             // is covered by bits 65 + lane - k .. 64 + lane (1 <= low <= 96)
             const uint64_t lowWord = ((uint64_t)prev1 << 32) | prev2;

@@ -133,7 +133,8 @@ __global__ void __launch_bounds__(512) k_scan_spans(TableView t, const uint64_t 
 
 // The scan over a wide-key table (33 <= k <= 64, format FMT_WIDE): the span
 // loop of k_scan_spans with each lane's k-mer read as a 128-bit canonical
-// code from three packed words and looked up level by level (wide_core.cuh).
+// code from three packed words and the warp's 32 codes looked up together,
+// 8 lanes reading each 128-byte line (wide::lookup_warp).
 // Restates the reference's string path for these k: canonical k-mer strings
 // of the window (getCanonicalKmersLegacy, src/Utils.hpp:102-125: toupper,
 // k-mers with a non-ACGT byte skipped, the smaller of the k-mer and its
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(256) k_scan_spans_wide(wide::View t, const uin
             uint64_t lo, hi;
             wide::canonical_at(seq, mask, G, k, acgt, lo, hi);
             const bool valid = inSpan && acgt;
-            const bool hit = valid && wide::lookup(t, lo, hi);
+            const bool hit = wide::lookup_warp(t, lo, hi, valid, lane);
             fold.push(__ballot_sync(FULL, valid), __ballot_sync(FULL, hit), lane, (int)k);
         }
         const SegStats acc = fold.finish((int)k);
@@ -324,13 +325,17 @@ static void launch_spans_fmt(const ibs_table *t, const uint64_t *dSeq, const uin
     }
 }
 
-// The wide-key scan: 256 threads, enough CTAs for 64 warps per SM.
+// The wide-key scan: 256 threads, as many CTAs as are resident at once.
 static void launch_spans_wide(const ibs_table *t, const uint64_t *dSeq, const uint64_t *dMask, const ScanPlan &p,
                               uint64_t s0, uint64_t s1, SegStats *dSpans, cudaStream_t st)
 {
     const int threads = 256;
+    int perSm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_scan_spans_wide, threads, 0) != cudaSuccess ||
+        perSm < 1)
+        perSm = 1;
     const uint64_t want = (s1 - s0 + 7) / 8;
-    const uint64_t cap = (uint64_t)sm_count() * 8;
+    const uint64_t cap = (uint64_t)sm_count() * perSm;
     const int grid = (int)std::max<uint64_t>(1, std::min(want, cap));
     k_scan_spans_wide<<<grid, threads, 0, st>>>(t->wide, dSeq, dMask, p.dWin, p.dSpan0, (uint32_t)p.nWin, s0, s1,
                                                 p.spanLen, dSpans);

@@ -106,10 +106,10 @@ __device__ __forceinline__ void canonical_at(const uint64_t *__restrict__ seq, c
                          __ldg(mask + mi + 1), G, k, acgt, clo, chi);
 }
 
-// Membership of one wide key.
-__device__ __forceinline__ bool lookup(const View &t, uint64_t lo, uint64_t hi)
+// Membership of one wide key, from level L0 on.
+__device__ __forceinline__ bool lookup(const View &t, uint64_t lo, uint64_t hi, uint32_t L0 = 0)
 {
-    for (uint32_t L = 0; L < t.nLevels; ++L) {
+    for (uint32_t L = L0; L < t.nLevels; ++L) {
         const ulonglong2 *p = t.slots[L] + line_of(lo, hi, L, t.lines[L]) * kSlots;
         bool hit = false, room = false;
 #pragma unroll
@@ -124,6 +124,43 @@ __device__ __forceinline__ bool lookup(const View &t, uint64_t lo, uint64_t hi)
             return false;
     }
     return false;
+}
+
+// Membership of the warp's 32 keys (one per lane; lanes with want == false
+// take part and get false). Level 0 is read cooperatively: in each of 8
+// steps, the four 8-lane groups read four keys' lines, lane i of a group
+// slot i, so one 16-byte load per lane covers four whole 128-byte lines
+// (instead of 32 lines touched per load when every lane reads its own
+// line); each group's 8-bit ballot slices say hit and empty slot to the key's
+// lane. A key whose level-0 line is full without it goes on to level 1 alone.
+// Every lane of the warp must call it.
+__device__ __forceinline__ bool lookup_warp(const View &t, uint64_t lo, uint64_t hi, bool want, uint32_t lane)
+{
+    const uint64_t line = want ? line_of(lo, hi, 0, t.lines[0]) : 0; // line 0 exists in every table
+    const ulonglong2 *base = t.slots[0] + (lane & 7);
+    const uint32_t group = lane >> 3;
+    uint32_t hitBits = 0, roomBits = 0;
+#pragma unroll
+    for (uint32_t g = 0; g < 8; ++g) {
+        const uint32_t owner = 4 * g + group; // the key this lane's group reads in step g
+        const uint64_t l = __shfl_sync(0xffffffffu, line, owner);
+        const uint64_t klo = __shfl_sync(0xffffffffu, lo, owner);
+        const uint64_t khi = __shfl_sync(0xffffffffu, hi, owner);
+        const ulonglong2 v = __ldg(base + l * kSlots);
+        const uint32_t m = __ballot_sync(0xffffffffu, (v.x == klo) & (v.y == khi));
+        const uint32_t e = __ballot_sync(0xffffffffu, (v.x == kEmpty) & (v.y == kEmpty));
+        if ((lane >> 2) == g) { // this lane's key is 4 g + (lane & 3), read by group lane & 3
+            hitBits = (m >> (8 * (lane & 3))) & 0xffu;
+            roomBits = (e >> (8 * (lane & 3))) & 0xffu;
+        }
+    }
+    if (!want)
+        return false;
+    if (hitBits)
+        return true;
+    if (roomBits)
+        return false;
+    return lookup(t, lo, hi, 1);
 }
 #endif
 
