@@ -994,6 +994,67 @@ def served_arm(args, rank: int):
     return out
 
 
+def wide_arm(args, rank: int):
+    """k > 32 (wide-key tables, the reference's string-path k): the 2 Gbp
+    reference scanned against a table of random 128-bit k = 41 keys (4 keys
+    per 128-byte line), timed with CUDA events over --steps scans after
+    --warmup. Throughput only: the rows of the k > 32 golden cases are
+    checked by the tests; here every row's total is checked against the
+    valid positions of its window."""
+    import ctypes as C
+    import torch
+    import ibs_b200 as ib
+    from ibs_b200 import configs
+    w = configs.plain_2gbp(scale=args.scale) if args.scale != 1.0 else configs.plain_2gbp()
+    k, W = 41, w.window
+    lens = w.ref.lens
+    sw, mw = w.ref.packed_words()
+    dseq = torch.empty(sw, dtype=torch.int64, device="cuda")
+    dmask = torch.empty(mw, dtype=torch.int64, device="cuda")
+    w.ref.reference_device(dseq.data_ptr(), dmask.data_ptr())
+    ref = ib.Reference(dseq.data_ptr(), dmask.data_ptr(), lens, on_device=True)
+    n = int(args.wide_keys)
+    g = torch.Generator(device="cuda").manual_seed(41)
+    lo = torch.randint(-2**63, 2**63 - 1, (n,), device="cuda", dtype=torch.int64, generator=g)
+    hi = torch.randint(0, 2**(2 * k - 64), (n,), device="cuda", dtype=torch.int64, generator=g)
+    codes = torch.stack([lo, hi], 1).contiguous()
+    del lo, hi
+    opts = ib.TableOpts(0, 0.0, 0)
+    h = C.c_void_p()
+    t0 = time.time()
+    ib._check(ib._ibs_from_codes128(codes.data_ptr(), n, k, 1, C.byref(opts), C.byref(h)))
+    build_s = time.time() - t0
+    del codes
+    torch.cuda.empty_cache()
+    t = ib.Table(h.value)
+    info = t.info()
+    nwin = ib.window_count(lens, W, k)
+    rows = torch.zeros(nwin * 6, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        ib.scan_async(t, ref, W, rows.data_ptr(), nwin, s.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(args.steps):
+        ib.scan_async(t, ref, W, rows.data_ptr(), nwin, s.cuda_stream)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    got = rows.cpu().numpy().view(ib.WINDOW_DTYPE)
+    bounds = ib.window_bounds(lens, W, k)
+    probes = valid_positions(lens, k, w.ref.n_runs())
+    t.close()
+    ref.free()
+    return {"k": k, "keys": n, "table_gb": info.device_bytes / 1e9, "later_level_keys": int(info.stash_keys),
+            "build_s": build_s, "ms_per_scan": ms, "probes_per_scan": probes, "probes_per_s": probes / ms * 1e3,
+            "bytes_per_probe": 128.375, "windows": int(nwin),
+            "rows_consistent": bool(np.array_equal(got["start"], bounds["start"]) and
+                                    np.array_equal(got["end"], bounds["end"]) and
+                                    int(got["total_kmers"].sum()) >= probes),
+            "table": "random keys (the throughput of one 128-byte line per probe; hits do not change it)"}
+
+
 def admitted_arm(args, rank: int):
     """Memory-admitted serving beyond the device's share: 48 samples whose
     tables total about 3x the server's byte budget, Zipf(1.1) popularity,
@@ -1303,6 +1364,9 @@ def main():
     ap.add_argument("--admit-rate", type=float, default=100.0)
     ap.add_argument("--serve-workload", choices=["served_2gbp", "panel_4gbp"], default="served_2gbp",
                     help="the pool: the 2 Gbp reference with 16 samples, or the 4.2 Gbp panel's")
+    ap.add_argument("--no-wide", action="store_true",
+                    help="skip the k = 41 wide-key scan (measured by default at N=1)")
+    ap.add_argument("--wide-keys", type=float, default=1e8, help="keys of the wide-key table")
     ap.add_argument("--arm-start-limit", type=float, default=900.0,
                     help="seconds after start past which the batched, served and admitted arms are not "
                          "started (reported as skipped), so that the whole run stays bounded")
@@ -1356,7 +1420,8 @@ def main():
     # the line, not fatal to it
     if world == 1:
         import torch
-        for key, skip, fn in (("panel", args.no_panel, panel_arm), ("served", args.no_serve, served_arm),
+        for key, skip, fn in (("wide", args.no_wide, wide_arm),
+                              ("panel", args.no_panel, panel_arm), ("served", args.no_serve, served_arm),
                               ("admitted", args.no_admitted, admitted_arm)):
             if skip:
                 continue
