@@ -59,7 +59,8 @@ typedef struct ibs_reference ibs_reference; /* a device-resident 2-bit packed re
 typedef struct ibs_table_opts {
     int device;             /* CUDA device ordinal (default 0) */
     double keys_per_bucket; /* target mean keys per 32 B bucket (0 = ibs_tuning.keys_per_bucket,
-                               or 4.0 for a hash table while the tuned format is minimizer lines) */
+                               or 4.0 for a hash table while the tuned format is minimizer lines);
+                               for format 8, keys per 128 B line of 8 slots (0 = 4.0) */
     uint32_t force_format;  /* 0 = the tuned default (ibs_tuning.table_format), 1 = B8x32,
                                2 = B6x40, 4 = minimizer lines of B8x32 sectors (16 <= k <= 27),
                                5 = hash buckets, B8x32 or B6x40 by size,
@@ -86,8 +87,9 @@ typedef struct ibs_table_info {
  * k <= 32, and for 33 <= k <= 64 the KMC API random-access view that the
  * reference's string path probes (CKMCFile::IsKmer via
  * getStatsFromSequenceLegacy, src/KmerDatabase.hpp:675-708): such a table
- * holds whole 128-bit keys (format 8) and every scan entry point except the
- * joint-table, serving, mapper and no-alloc ones takes it. */
+ * holds whole 128-bit keys (format 8); the scans (ibs_scan, _async, _packed,
+ * _panel), the mapper and ibs_count_present_kmc take it, the joint-table,
+ * serving and no-alloc entry points do not (IBS_ERR_ARG / _UNSUPPORTED). */
 ibs_status ibs_open(const char *kmc_prefix, const ibs_table_opts *opts, ibs_table **out);
 
 /* Build a table from canonical codes (host or device pointer; duplicates
