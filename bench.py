@@ -1367,7 +1367,7 @@ def main():
     ap.add_argument("--no-wide", action="store_true",
                     help="skip the k = 41 wide-key scan (measured by default at N=1)")
     ap.add_argument("--wide-keys", type=float, default=1e8, help="keys of the wide-key table")
-    ap.add_argument("--arm-start-limit", type=float, default=900.0,
+    ap.add_argument("--arm-start-limit", type=float, default=1080.0,
                     help="seconds after start past which the batched, served and admitted arms are not "
                          "started (reported as skipped), so that the whole run stays bounded")
     ap.add_argument("--serve-sample-scale", type=float, default=0.5,
