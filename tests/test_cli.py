@@ -61,6 +61,26 @@ def test_existing_output_is_skipped(tmp_path, c25):
     assert (out / "db_v_test_5000.tsv").read_text() == "kept\n"
 
 
+def test_k_above_64_is_refused_before_any_device_work(tmp_path):
+    """33 <= k <= 64 builds wide-key tables; a longer k is refused with the
+    reason, from the header alone, as the reference refuses what it cannot
+    open (exit status 1)."""
+    import numpy as np
+    import ibs_b200 as ib
+    db = tmp_path / "db"
+    db.mkdir()
+    ib.kmc_write(str(db / "sample"), np.arange(10, dtype=np.uint64), 10, k=32, p=8)
+    pre = (db / "sample.kmc_pre").read_bytes()
+    pos = len(pre) - (pre[-8] + 8)  # the header's first field is k
+    (db / "sample.kmc_pre").write_bytes(pre[:pos] + (72).to_bytes(4, "little") + pre[pos + 4:])
+    refs = tmp_path / "refs"
+    refs.mkdir()
+    (refs / "x_genome.fasta").write_text(">c\n" + "ACGT" * 100 + "\n")
+    r = run([db, refs, tmp_path / "o", "5000"], tmp_path)
+    assert r.returncode == 1
+    assert "k=72 > 64" in r.stderr
+
+
 def test_without_a_device_the_reference_fails_and_is_logged(tmp_path, c25):
     import ibs_b200
     if ibs_b200.device_count() > 0:
