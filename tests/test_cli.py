@@ -81,6 +81,18 @@ def test_k_above_64_is_refused_before_any_device_work(tmp_path):
     assert "k=72 > 64" in r.stderr
 
 
+def test_panel_of_different_k_is_refused(tmp_path, build_case):
+    """A panel shares one k (src/FastIBS.cpp:155-172): every member's header is
+    read first, so k = 25 and k = 41 databases are refused before any device
+    work, with the reference's message."""
+    a, b = build_case("edge_k25"), build_case("edge_k41")
+    db2 = tmp_path / "db2"
+    shutil.copytree(b["db"], db2)
+    r = run([a["db"], a["refs"], tmp_path / "o", "5000", f"--db={db2}"], tmp_path)
+    assert r.returncode == 1
+    assert "has k=41 but db has k=25; a panel shares one k" in r.stderr
+
+
 def test_without_a_device_the_reference_fails_and_is_logged(tmp_path, c25):
     import ibs_b200
     if ibs_b200.device_count() > 0:
