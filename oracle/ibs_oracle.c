@@ -519,6 +519,8 @@ uint32_t orc_signature(const orc_index *ix, uint64_t code)
  * index: prefix range [0, 0xffffffff). */
 int orc_probe(const orc_index *ix, uint64_t code)
 {
+    if (ix->suf128) /* k > 32 indexes answer orc_probe128 only */
+        return 0;
     const uint64_t prefix = code >> (2 * (ix->k - ix->p));
     if (prefix >= 0xffffffffu)
         return 0;
@@ -555,6 +557,8 @@ void orc_probe_many(const orc_index *ix, const uint64_t *codes, size_t n, uint8_
 /* forEachKmer / walkBuckets (src/gpu/KmcRaIndex.hpp:169-173, :446-460). */
 size_t orc_index_list(const orc_index *ix, uint64_t *codes, size_t cap)
 {
+    if (ix->suf128) /* k > 32 indexes list through orc_index_list128 */
+        return 0;
     const uint32_t shift = 2 * (ix->k - ix->p);
     const uint64_t prefixMask = ix->singleLutSize - 1;
     size_t n = 0;

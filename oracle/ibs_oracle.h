@@ -49,7 +49,8 @@ void orc_probe_many(const orc_index *ix, const uint64_t *codes, size_t n, uint8_
  * src/gpu/KmcRaIndex.hpp:169-173, :446-460); returns the count written. */
 size_t orc_index_list(const orc_index *ix, uint64_t *codes, size_t cap);
 uint32_t orc_signature(const orc_index *ix, uint64_t code);
-/* k > 32 (the reference's string path, KMC API CKMCFile::IsKmer): membership
+/* orc_probe / orc_index_list answer 0 for k > 32 indexes, which take these.
+ * k > 32 (the reference's string path, KMC API CKMCFile::IsKmer): membership
  * of one 128-bit canonical code given as its low and high words, and the
  * listing as two word arrays. */
 int orc_probe128(const orc_index *ix, uint64_t lo, uint64_t hi);
